@@ -1,0 +1,582 @@
+// fm_capi.cu -- the extern "C" boundary of libflashmap_b200.so: table
+// lifetime, host<->device transfers, the round loop of the mutating
+// operations, error mapping and len bookkeeping.  Replaces the reference's
+// src/gpu.rs (bajpainaman/flash-map 0.5.0); see include/flashmap_b200.h.
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/flashmap_b200.h"
+#include "fm_internal.h"
+
+using fm::Ctl;
+using fm::OpScratch;
+
+namespace {
+
+thread_local std::string tl_err;
+
+int fail(int code, const std::string& msg) {
+    tl_err = msg;
+    return code;
+}
+
+int cuda_fail(int code, const char* what, cudaError_t e) {
+    return fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Device chunk of one mutating call: op indices are u32 and 0xFFFFFFFF marks
+// an idle segment slot, so a call is split into sequential chunks (which is
+// exactly the sequential semantics) of at most this many operations.
+constexpr uint64_t OP_CHUNK = 1ull << 30;
+
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+struct GetCtx {
+    cudaStream_t s = nullptr;
+    uint8_t* d_buf = nullptr;
+    size_t cap = 0;
+};
+
+template <class T>
+cudaError_t grow(T*& p, size_t& cap, size_t need) {
+    if (need <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = need + need / 4;
+    cudaError_t e = cudaMalloc((void**)&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+}
+
+bool aligned(const void* p, uintptr_t a) { return ((uintptr_t)p % a) == 0; }
+
+}  // namespace
+
+struct fm_table {
+    int device = 0;
+    uint64_t cap = 0, mask = 0;
+    uint32_t ksz = 0, vsz = 0, mode = 0;
+    fm::Shape shape = fm::SHAPE_GENERIC;
+    uint32_t* d_flags = nullptr;
+    uint8_t* d_keys = nullptr;
+    uint8_t* d_vals = nullptr;
+    uint32_t* d_seg_min = nullptr;
+    uint32_t* d_seg_cnt = nullptr;
+    Ctl* d_ctl = nullptr;
+    Ctl* h_ctl = nullptr;    // pinned mirror for readbacks
+    Ctl* h_reset = nullptr;  // pinned per-round reset template
+    std::atomic<uint64_t> len{0};
+    cudaStream_t stream = nullptr;  // mutating calls
+    std::mutex mu;                  // serialises mutating calls and their scratch
+    OpScratch sc{};
+    size_t sc_bytes = 0;
+    uint8_t* sc_base = nullptr;
+    uint8_t* d_in = nullptr;  // host-API staging for mutating calls
+    size_t d_in_cap = 0;
+    std::mutex pool_mu;
+    std::vector<GetCtx*> pool;
+
+    fm::TableView view() const {
+        fm::TableView v;
+        v.flags = d_flags;
+        v.keys = d_keys;
+        v.vals = d_vals;
+        v.seg_min = d_seg_min;
+        v.seg_cnt = d_seg_cnt;
+        v.mask = mask;
+        v.ksz = ksz;
+        v.vsz = vsz;
+        v.hash_mode = mode;
+        return v;
+    }
+
+    // Shape for a call whose caller-provided buffers are `ptrs`: the
+    // vectorised instantiations need 16-byte aligned record arrays.
+    fm::Shape shape_for(std::initializer_list<const void*> ptrs) const {
+        if (shape == fm::SHAPE_GENERIC) return shape;
+        for (const void* p : ptrs)
+            if (p && !aligned(p, 16)) return fm::SHAPE_GENERIC;
+        return shape;
+    }
+};
+
+namespace {
+
+int ensure_scratch(fm_table* t, uint64_t n) {
+    if (t->sc.cap_ops >= n) return FM_OK;
+    // pend_a, pend_b (u32) | op_slot (u64) | op_word (u32) | op_flag (u8) | op_pt (PT_MAX u32)
+    const uint64_t per_op = 4 + 4 + 8 + 4 + 1 + 4 * fm::PT_MAX;
+    const uint64_t want = n + n / 4 + 1024;
+    const size_t bytes = (size_t)(want * per_op + 6 * 256);
+    if (t->sc_base) cudaFree(t->sc_base);
+    t->sc_base = nullptr;
+    t->sc = OpScratch{};
+    cudaError_t e = cudaMalloc((void**)&t->sc_base, bytes);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_GPU_ALLOC, "scratch allocation", e);
+    uint8_t* p = t->sc_base;
+    auto carve = [&](size_t b) {
+        uint8_t* r = p;
+        p += (b + 255) & ~(size_t)255;
+        return r;
+    };
+    t->sc.op_slot = (uint64_t*)carve(want * 8);
+    t->sc.pend_a = (uint32_t*)carve(want * 4);
+    t->sc.pend_b = (uint32_t*)carve(want * 4);
+    t->sc.op_word = (uint32_t*)carve(want * 4);
+    t->sc.op_pt = (uint32_t*)carve(want * 4 * fm::PT_MAX);
+    t->sc.op_flag = carve(want);
+    t->sc.cap_ops = want;
+    t->sc_bytes = bytes;
+    // op_word doubles as the insert inflow bound: idle value 0xFFFFFFFF.
+    e = cudaMemsetAsync(t->sc.op_word, 0xFF, want * 4, t->stream);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_GPU_ALLOC, "scratch init", e);
+    return FM_OK;
+}
+
+// Reset the per-round fields of the control block (npend_next, gmin, serial).
+cudaError_t reset_round(fm_table* t, cudaStream_t s) {
+    return cudaMemcpyAsync(t->d_ctl, t->h_reset, 12, cudaMemcpyHostToDevice, s);
+}
+
+// After a failed call the segment registrations and the per-op scratch may be
+// left set; put every one of them back to idle.
+void recover(fm_table* t, cudaStream_t s) {
+    cudaMemsetAsync(t->d_seg_min, 0xFF, t->cap * 4, s);
+    cudaMemsetAsync(t->d_seg_cnt, 0, t->cap * 4, s);
+    if (t->sc.op_word) cudaMemsetAsync(t->sc.op_word, 0xFF, t->sc.cap_ops * 4, s);
+    cudaStreamSynchronize(s);
+}
+
+// The round loop shared by insert and remove.  `insert` selects the kernel set.
+int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t* d_v, uint64_t n,
+                     cudaStream_t s, uint64_t* out_count, uint32_t* err_bits) {
+    uint64_t total = 0;
+    *err_bits = 0;
+    const fm::Shape sh = t->shape_for({d_k, d_v});
+    int rc = ensure_scratch(t, n < OP_CHUNK ? n : OP_CHUNK);
+    if (rc) return rc;
+    fm::TableView v = t->view();
+    for (uint64_t base = 0; base < n; base += OP_CHUNK) {
+        const uint64_t m = (n - base) < OP_CHUNK ? (n - base) : OP_CHUNK;
+        const uint8_t* kk = d_k + base * t->ksz;
+        const uint8_t* vv = d_v ? d_v + base * t->vsz : nullptr;
+        cudaError_t e = fm::launch_iota(t->sc.pend_a, m, s);
+        if (e == cudaSuccess) e = reset_round(t, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(&t->d_ctl->err, 0, 4, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(&t->d_ctl->count, 0, sizeof(unsigned long long), s);
+        if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "round setup", e);
+        uint32_t* pend = t->sc.pend_a;
+        uint32_t* next = t->sc.pend_b;
+        uint32_t npend = (uint32_t)m;
+        uint64_t rounds = 0;
+        while (npend > 0) {
+            e = insert ? fm::launch_ins_round(v, sh, kk, vv, pend, npend, (uint32_t)m, next, t->sc, t->d_ctl, s)
+                       : fm::launch_rem_round(v, sh, kk, pend, npend, next, t->sc, t->d_ctl, s);
+            if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, insert ? "insert round" : "remove round", e);
+            e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "round readback", e);
+            const uint32_t left = t->h_ctl->npend_next;
+            if (t->h_ctl->err & fm::ERR_SCRATCH) return fail(FM_ERR_KERNEL_LAUNCH, "stale segment registration");
+            if (left >= npend)  // every round runs at least the lowest pending op
+                return fail(FM_ERR_PROBE_LIMIT, "round made no progress");
+            ++rounds;
+            npend = left;
+            uint32_t* tmp = pend;
+            pend = next;
+            next = tmp;
+            if (npend) {
+                e = reset_round(t, s);
+                if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "round reset", e);
+            }
+        }
+        total += t->h_ctl->count;
+        *err_bits |= t->h_ctl->err;
+    }
+    *out_count = total;
+    return FM_OK;
+}
+
+// Runs a mutating call.  On FM_OK with *limit set, every op ran but at least
+// one insert walk stopped at the full-table step limit (reported to the
+// caller as FM_ERR_PROBE_LIMIT after len is updated).
+int run_rounds(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t* d_v, uint64_t n, cudaStream_t s,
+               uint64_t* out_count, bool* limit) {
+    uint32_t bits = 0;
+    int rc = run_rounds_inner(t, insert, d_k, d_v, n, s, out_count, &bits);
+    if (rc) {
+        std::string msg = tl_err;
+        recover(t, s);
+        tl_err = msg;
+        return rc;
+    }
+    *limit = (bits & fm::ERR_WALK_LIMIT) != 0;
+    return FM_OK;
+}
+
+int limit_error() {
+    return fail(FM_ERR_PROBE_LIMIT,
+                "insert walk passed 2*capacity+2 slots without a free slot (table full; the reference's "
+                "insert loop would not terminate here)");
+}
+
+GetCtx* acquire_ctx(fm_table* t) {
+    {
+        std::lock_guard<std::mutex> g(t->pool_mu);
+        if (!t->pool.empty()) {
+            GetCtx* c = t->pool.back();
+            t->pool.pop_back();
+            return c;
+        }
+    }
+    GetCtx* c = new GetCtx();
+    if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return nullptr;
+    }
+    return c;
+}
+
+void release_ctx(fm_table* t, GetCtx* c) {
+    std::lock_guard<std::mutex> g(t->pool_mu);
+    t->pool.push_back(c);
+}
+
+uint32_t max_dist_of(const uint32_t* flags, uint64_t cap) {
+    uint32_t m = 0;
+    for (uint64_t i = 0; i < cap; i++)
+        if ((flags[i] & 0xFu) == fm::ST_OCC && (flags[i] >> 4) > m) m = flags[i] >> 4;
+    return m;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fm_last_error(void) { return tl_err.c_str(); }
+
+int fm_create(uint64_t capacity, uint32_t key_size, uint32_t value_size, uint32_t hash_mode, int device_id,
+              fm_table** out) {
+    if (!out) return fail(FM_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (capacity == 0) return fail(FM_ERR_ZERO_CAPACITY, "capacity must be positive");  // gpu.rs:50-52
+    if (capacity > (1ull << 32)) return fail(FM_ERR_INVALID_ARG, "capacity above 2^32 slots is not supported");
+    if (hash_mode > 1) return fail(FM_ERR_INVALID_ARG, "unknown hash mode");
+    uint64_t cap = 1;
+    while (cap < capacity) cap <<= 1;  // next_power_of_two (gpu.rs:54)
+    const fm::Shape sh = fm::pick_shape(key_size, value_size);
+    if (sh == fm::SHAPE_GENERIC && (key_size > fm::GENERIC_MAX_KV || value_size > fm::GENERIC_MAX_KV))
+        return fail(FM_ERR_INVALID_ARG, "key or value larger than 256 bytes (FM_MAX_KV_SIZE, kernels.cu:32)");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_CUDA_INIT, "cudaGetDeviceCount", e);
+    if (device_id < 0 || device_id >= ndev) return fail(FM_ERR_CUDA_INIT, "no such CUDA device");
+    DeviceGuard dg(device_id);
+    if (!dg.ok) return fail(FM_ERR_CUDA_INIT, "cudaSetDevice failed");
+    fm_table* t = new fm_table();
+    t->device = device_id;
+    t->cap = cap;
+    t->mask = cap - 1;
+    t->ksz = key_size;
+    t->vsz = value_size;
+    t->mode = hash_mode;
+    t->shape = sh;
+    auto bail = [&](int code, const char* what, cudaError_t err) {
+        int rc = cuda_fail(code, what, err);
+        fm_destroy(t);
+        return rc;
+    };
+    if ((e = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(FM_ERR_CUDA_INIT, "stream", e);
+    const size_t kb = (size_t)cap * (key_size ? key_size : 1);
+    const size_t vb = (size_t)cap * (value_size ? value_size : 1);
+    if ((e = cudaMalloc((void**)&t->d_flags, cap * 4)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "flags", e);
+    if ((e = cudaMalloc((void**)&t->d_keys, kb)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "keys", e);
+    if ((e = cudaMalloc((void**)&t->d_vals, vb)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "values", e);
+    if ((e = cudaMalloc((void**)&t->d_seg_min, cap * 4)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "seg_min", e);
+    if ((e = cudaMalloc((void**)&t->d_seg_cnt, cap * 4)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "seg_cnt", e);
+    if ((e = cudaMalloc((void**)&t->d_ctl, sizeof(Ctl))) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "ctl", e);
+    if ((e = cudaMallocHost((void**)&t->h_ctl, sizeof(Ctl))) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "ctl", e);
+    if ((e = cudaMallocHost((void**)&t->h_reset, sizeof(Ctl))) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "ctl", e);
+    memset(t->h_ctl, 0, sizeof(Ctl));
+    memset(t->h_reset, 0, sizeof(Ctl));
+    t->h_reset->gmin = fm::IDLE;
+    // Zeroed SoA table: all flags EMPTY (gpu.rs:81-92).
+    cudaMemsetAsync(t->d_flags, 0, cap * 4, t->stream);
+    cudaMemsetAsync(t->d_keys, 0, kb, t->stream);
+    cudaMemsetAsync(t->d_vals, 0, vb, t->stream);
+    cudaMemsetAsync(t->d_seg_min, 0xFF, cap * 4, t->stream);
+    cudaMemsetAsync(t->d_seg_cnt, 0, cap * 4, t->stream);
+    cudaMemsetAsync(t->d_ctl, 0, sizeof(Ctl), t->stream);
+    if ((e = cudaStreamSynchronize(t->stream)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "table init", e);
+    *out = t;
+    return FM_OK;
+}
+
+void fm_destroy(fm_table* t) {
+    if (!t) return;
+    DeviceGuard dg(t->device);
+    if (t->stream) cudaStreamSynchronize(t->stream);
+    for (GetCtx* c : t->pool) {
+        cudaStreamSynchronize(c->s);
+        cudaStreamDestroy(c->s);
+        if (c->d_buf) cudaFree(c->d_buf);
+        delete c;
+    }
+    cudaFree(t->d_flags);
+    cudaFree(t->d_keys);
+    cudaFree(t->d_vals);
+    cudaFree(t->d_seg_min);
+    cudaFree(t->d_seg_cnt);
+    cudaFree(t->d_ctl);
+    if (t->h_ctl) cudaFreeHost(t->h_ctl);
+    if (t->h_reset) cudaFreeHost(t->h_reset);
+    if (t->sc_base) cudaFree(t->sc_base);
+    if (t->d_in) cudaFree(t->d_in);
+    if (t->stream) cudaStreamDestroy(t->stream);
+    delete t;
+}
+
+uint64_t fm_len(const fm_table* t) { return t ? t->len.load() : 0; }
+uint64_t fm_capacity(const fm_table* t) { return t ? t->cap : 0; }
+double fm_load_factor(const fm_table* t) { return t ? (double)t->len.load() / (double)t->cap : 0.0; }
+int fm_device(const fm_table* t) { return t ? t->device : -1; }
+
+int fm_bulk_get(fm_table* t, const void* keys, uint64_t n, void* out_values, uint8_t* out_found) {
+    if (!t) return fail(FM_ERR_INVALID_ARG, "table is NULL");
+    if (n == 0) return FM_OK;
+    if (!keys || (!out_values && t->vsz) || !out_found) return fail(FM_ERR_INVALID_ARG, "NULL buffer");
+    DeviceGuard dg(t->device);
+    GetCtx* c = acquire_ctx(t);
+    if (!c) return fail(FM_ERR_CUDA_INIT, "stream creation failed");
+    const size_t kb = (size_t)n * t->ksz, vb = (size_t)n * t->vsz;
+    const size_t off_v = (kb + 255) & ~(size_t)255;
+    const size_t off_f = off_v + ((vb + 255) & ~(size_t)255);
+    cudaError_t e = grow(c->d_buf, c->cap, off_f + n);
+    if (e != cudaSuccess) {
+        release_ctx(t, c);
+        return cuda_fail(FM_ERR_GPU_ALLOC, "get buffers", e);
+    }
+    uint8_t* dq = c->d_buf;
+    uint8_t* dv = c->d_buf + off_v;
+    uint8_t* df = c->d_buf + off_f;
+    int rc = FM_OK;
+    if ((e = cudaMemcpyAsync(dq, keys, kb, cudaMemcpyHostToDevice, c->s)) != cudaSuccess)
+        rc = cuda_fail(FM_ERR_TRANSFER, "htod keys", e);
+    if (!rc && (e = fm::launch_get(t->view(), t->shape, dq, n, dv, df, c->s)) != cudaSuccess)
+        rc = cuda_fail(FM_ERR_KERNEL_LAUNCH, "bulk_get", e);
+    if (!rc && vb && (e = cudaMemcpyAsync(out_values, dv, vb, cudaMemcpyDeviceToHost, c->s)) != cudaSuccess)
+        rc = cuda_fail(FM_ERR_TRANSFER, "dtoh values", e);
+    if (!rc && (e = cudaMemcpyAsync(out_found, df, n, cudaMemcpyDeviceToHost, c->s)) != cudaSuccess)
+        rc = cuda_fail(FM_ERR_TRANSFER, "dtoh found", e);
+    if ((e = cudaStreamSynchronize(c->s)) != cudaSuccess && !rc) rc = cuda_fail(FM_ERR_TRANSFER, "bulk_get sync", e);
+    release_ctx(t, c);
+    return rc;
+}
+
+static int precheck(fm_table* t, uint64_t n) {
+    // len + n > capacity * MAX_LOAD_FACTOR (1.0) -> TableFull (gpu.rs:198-206)
+    const uint64_t len = t->len.load();
+    if (len + n > t->cap) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "table full: %llu occupied of %llu capacity (load factor %.1f%%)",
+                 (unsigned long long)len, (unsigned long long)t->cap, (double)len / (double)t->cap * 100.0);
+        return fail(FM_ERR_TABLE_FULL, buf);
+    }
+    return FM_OK;
+}
+
+int fm_bulk_insert(fm_table* t, const void* keys, const void* values, uint64_t n, uint64_t* num_new) {
+    if (!t || !num_new) return fail(FM_ERR_INVALID_ARG, "NULL argument");
+    *num_new = 0;
+    if (n == 0) return FM_OK;  // gpu.rs:194-196
+    if (!keys || (!values && t->vsz)) return fail(FM_ERR_INVALID_ARG, "NULL buffer");
+    std::lock_guard<std::mutex> g(t->mu);
+    int rc = precheck(t, n);
+    if (rc) return rc;
+    DeviceGuard dg(t->device);
+    const size_t kb = (size_t)n * t->ksz, vb = (size_t)n * t->vsz;
+    const size_t off_v = (kb + 255) & ~(size_t)255;
+    cudaError_t e = grow(t->d_in, t->d_in_cap, off_v + vb + 1);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_GPU_ALLOC, "insert buffers", e);
+    if ((e = cudaMemcpyAsync(t->d_in, keys, kb, cudaMemcpyHostToDevice, t->stream)) != cudaSuccess)
+        return cuda_fail(FM_ERR_TRANSFER, "htod keys", e);
+    if (vb && (e = cudaMemcpyAsync(t->d_in + off_v, values, vb, cudaMemcpyHostToDevice, t->stream)) != cudaSuccess)
+        return cuda_fail(FM_ERR_TRANSFER, "htod values", e);
+    uint64_t added = 0;
+    bool limit = false;
+    rc = run_rounds(t, true, t->d_in, t->d_in + off_v, n, t->stream, &added, &limit);
+    if (rc) return rc;
+    t->len += added;
+    *num_new = added;
+    return limit ? limit_error() : FM_OK;
+}
+
+int fm_bulk_remove(fm_table* t, const void* keys, uint64_t n, uint64_t* num_removed) {
+    if (!t || !num_removed) return fail(FM_ERR_INVALID_ARG, "NULL argument");
+    *num_removed = 0;
+    if (n == 0) return FM_OK;
+    if (!keys) return fail(FM_ERR_INVALID_ARG, "NULL buffer");
+    std::lock_guard<std::mutex> g(t->mu);
+    DeviceGuard dg(t->device);
+    const size_t kb = (size_t)n * t->ksz;
+    cudaError_t e = grow(t->d_in, t->d_in_cap, kb + 1);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_GPU_ALLOC, "remove buffers", e);
+    if ((e = cudaMemcpyAsync(t->d_in, keys, kb, cudaMemcpyHostToDevice, t->stream)) != cudaSuccess)
+        return cuda_fail(FM_ERR_TRANSFER, "htod keys", e);
+    uint64_t removed = 0;
+    bool limit = false;
+    int rc = run_rounds(t, false, t->d_in, nullptr, n, t->stream, &removed, &limit);
+    if (rc) return rc;
+    t->len -= removed;
+    *num_removed = removed;
+    return FM_OK;
+}
+
+int fm_clear(fm_table* t) {
+    if (!t) return fail(FM_ERR_INVALID_ARG, "table is NULL");
+    std::lock_guard<std::mutex> g(t->mu);
+    DeviceGuard dg(t->device);
+    cudaError_t e = cudaMemsetAsync(t->d_flags, 0, t->cap * 4, t->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&t->d_ctl->dmax, 0, 8, t->stream);  // dmax, tomb_claimed
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "clear", e);
+    t->len.store(0);
+    return FM_OK;
+}
+
+int fm_bulk_get_device(fm_table* t, const void* d_keys, uint64_t n, void* d_out_values, uint8_t* d_out_found,
+                       void* stream) {
+    if (!t) return fail(FM_ERR_INVALID_ARG, "table is NULL");
+    if (n == 0) return FM_OK;
+    if (!d_keys || (!d_out_values && t->vsz)) return fail(FM_ERR_INVALID_ARG, "NULL buffer");
+    DeviceGuard dg(t->device);
+    cudaError_t e = fm::launch_get(t->view(), t->shape_for({d_keys, d_out_values}), (const uint8_t*)d_keys, n,
+                                   (uint8_t*)d_out_values, d_out_found, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "bulk_get_device", e);
+    return FM_OK;
+}
+
+int fm_bulk_get_values_device(fm_table* t, const void* d_keys, uint64_t n, void* d_out_values, void* stream) {
+    return fm_bulk_get_device(t, d_keys, n, d_out_values, nullptr, stream);
+}
+
+static int insert_device(fm_table* t, const void* d_keys, const void* d_values, uint64_t n, uint64_t* num_new,
+                         void* stream, bool counted) {
+    if (!t) return fail(FM_ERR_INVALID_ARG, "table is NULL");
+    if (num_new) *num_new = 0;
+    if (n == 0) return FM_OK;
+    if (!d_keys || (!d_values && t->vsz)) return fail(FM_ERR_INVALID_ARG, "NULL buffer");
+    std::lock_guard<std::mutex> g(t->mu);
+    if (counted) {
+        int rc = precheck(t, n);
+        if (rc) return rc;
+    }
+    DeviceGuard dg(t->device);
+    uint64_t added = 0;
+    bool limit = false;
+    int rc = run_rounds(t, true, (const uint8_t*)d_keys, (const uint8_t*)d_values, n, (cudaStream_t)stream, &added,
+                        &limit);
+    if (rc) return rc;
+    if (counted) {
+        t->len += added;
+        if (num_new) *num_new = added;
+    } else {
+        t->len += n;  // gpu.rs:670
+    }
+    return limit ? limit_error() : FM_OK;
+}
+
+int fm_bulk_insert_device(fm_table* t, const void* d_keys, const void* d_values, uint64_t n, uint64_t* num_new,
+                          void* stream) {
+    if (!num_new) return fail(FM_ERR_INVALID_ARG, "num_new is NULL");
+    return insert_device(t, d_keys, d_values, n, num_new, stream, true);
+}
+
+int fm_bulk_insert_device_uncounted(fm_table* t, const void* d_keys, const void* d_values, uint64_t n,
+                                    void* stream) {
+    return insert_device(t, d_keys, d_values, n, nullptr, stream, false);
+}
+
+int fm_bulk_remove_device(fm_table* t, const void* d_keys, uint64_t n, uint64_t* num_removed, void* stream) {
+    if (!t || !num_removed) return fail(FM_ERR_INVALID_ARG, "NULL argument");
+    *num_removed = 0;
+    if (n == 0) return FM_OK;
+    if (!d_keys) return fail(FM_ERR_INVALID_ARG, "NULL buffer");
+    std::lock_guard<std::mutex> g(t->mu);
+    DeviceGuard dg(t->device);
+    uint64_t removed = 0;
+    bool limit = false;
+    int rc = run_rounds(t, false, (const uint8_t*)d_keys, nullptr, n, (cudaStream_t)stream, &removed, &limit);
+    if (rc) return rc;
+    t->len -= removed;
+    *num_removed = removed;
+    return FM_OK;
+}
+
+int fm_recount(fm_table* t, uint64_t* out) {
+    if (!t) return fail(FM_ERR_INVALID_ARG, "table is NULL");
+    std::lock_guard<std::mutex> g(t->mu);
+    DeviceGuard dg(t->device);
+    cudaError_t e = cudaMemsetAsync(&t->d_ctl->occupied, 0, 8, t->stream);
+    if (e == cudaSuccess) e = fm::launch_count(t->view(), t->d_ctl, t->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, t->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "recount", e);
+    const uint64_t c = t->h_ctl->occupied;
+    t->len.store(c);
+    if (out) *out = c;
+    return FM_OK;
+}
+
+int fm_snapshot(fm_table* t, uint32_t* flags, void* keys, void* values) {
+    if (!t) return fail(FM_ERR_INVALID_ARG, "table is NULL");
+    std::lock_guard<std::mutex> g(t->mu);
+    DeviceGuard dg(t->device);
+    cudaError_t e = cudaSuccess;
+    if (flags) e = cudaMemcpyAsync(flags, t->d_flags, t->cap * 4, cudaMemcpyDeviceToHost, t->stream);
+    if (e == cudaSuccess && keys && t->ksz)
+        e = cudaMemcpyAsync(keys, t->d_keys, t->cap * t->ksz, cudaMemcpyDeviceToHost, t->stream);
+    if (e == cudaSuccess && values && t->vsz)
+        e = cudaMemcpyAsync(values, t->d_vals, t->cap * t->vsz, cudaMemcpyDeviceToHost, t->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "snapshot", e);
+    return FM_OK;
+}
+
+int fm_load(fm_table* t, const uint32_t* flags, const void* keys, const void* values, uint64_t len) {
+    if (!t || !flags) return fail(FM_ERR_INVALID_ARG, "NULL argument");
+    std::lock_guard<std::mutex> g(t->mu);
+    DeviceGuard dg(t->device);
+    cudaError_t e = cudaMemcpyAsync(t->d_flags, flags, t->cap * 4, cudaMemcpyHostToDevice, t->stream);
+    if (e == cudaSuccess && keys && t->ksz)
+        e = cudaMemcpyAsync(t->d_keys, keys, t->cap * t->ksz, cudaMemcpyHostToDevice, t->stream);
+    if (e == cudaSuccess && values && t->vsz)
+        e = cudaMemcpyAsync(t->d_vals, values, t->cap * t->vsz, cudaMemcpyHostToDevice, t->stream);
+    // dmax bounds every stored distance; the history of a loaded table is
+    // unknown, so tombstone reuse is assumed.
+    uint32_t persist[2] = {max_dist_of(flags, t->cap), 1u};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&t->d_ctl->dmax, persist, 8, cudaMemcpyHostToDevice, t->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "load", e);
+    t->len.store(len);
+    return FM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,91 @@
+"""ctypes binding of ``libflashmap_b200.so`` (the C ABI in include/flashmap_b200.h).
+
+The shared library is built in-tree (``make -C flash-map_b200``).  There is no
+fallback: if the library is missing or cannot be loaded, every entry point
+raises ``CudaInit``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+from .errors import CudaInit
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "libflashmap_b200.so")
+
+# Every exported symbol of include/flashmap_b200.h.
+EXPORTS = (
+    "fm_create", "fm_destroy", "fm_bulk_get", "fm_bulk_insert", "fm_bulk_remove", "fm_len",
+    "fm_capacity", "fm_load_factor", "fm_clear", "fm_device", "fm_bulk_get_device",
+    "fm_bulk_get_values_device", "fm_bulk_insert_device", "fm_bulk_insert_device_uncounted",
+    "fm_bulk_remove_device", "fm_recount", "fm_last_error", "fm_snapshot", "fm_load",
+)
+
+_lock = threading.Lock()
+_lib = None
+
+
+def _declare(L) -> None:
+    vp, u64, u32, i32 = C.c_void_p, C.c_uint64, C.c_uint32, C.c_int
+    u64p = C.POINTER(C.c_uint64)
+    L.fm_create.restype = i32
+    L.fm_create.argtypes = [u64, u32, u32, u32, i32, C.POINTER(vp)]
+    L.fm_destroy.restype = None
+    L.fm_destroy.argtypes = [vp]
+    L.fm_bulk_get.restype = i32
+    L.fm_bulk_get.argtypes = [vp, vp, u64, vp, vp]
+    L.fm_bulk_insert.restype = i32
+    L.fm_bulk_insert.argtypes = [vp, vp, vp, u64, u64p]
+    L.fm_bulk_remove.restype = i32
+    L.fm_bulk_remove.argtypes = [vp, vp, u64, u64p]
+    L.fm_len.restype = u64
+    L.fm_len.argtypes = [vp]
+    L.fm_capacity.restype = u64
+    L.fm_capacity.argtypes = [vp]
+    L.fm_load_factor.restype = C.c_double
+    L.fm_load_factor.argtypes = [vp]
+    L.fm_clear.restype = i32
+    L.fm_clear.argtypes = [vp]
+    L.fm_device.restype = i32
+    L.fm_device.argtypes = [vp]
+    L.fm_bulk_get_device.restype = i32
+    L.fm_bulk_get_device.argtypes = [vp, vp, u64, vp, vp, vp]
+    L.fm_bulk_get_values_device.restype = i32
+    L.fm_bulk_get_values_device.argtypes = [vp, vp, u64, vp, vp]
+    L.fm_bulk_insert_device.restype = i32
+    L.fm_bulk_insert_device.argtypes = [vp, vp, vp, u64, u64p, vp]
+    L.fm_bulk_insert_device_uncounted.restype = i32
+    L.fm_bulk_insert_device_uncounted.argtypes = [vp, vp, vp, u64, vp]
+    L.fm_bulk_remove_device.restype = i32
+    L.fm_bulk_remove_device.argtypes = [vp, vp, u64, u64p, vp]
+    L.fm_recount.restype = i32
+    L.fm_recount.argtypes = [vp, u64p]
+    L.fm_last_error.restype = C.c_char_p
+    L.fm_last_error.argtypes = []
+    L.fm_snapshot.restype = i32
+    L.fm_snapshot.argtypes = [vp, vp, vp, vp]
+    L.fm_load.restype = i32
+    L.fm_load.argtypes = [vp, vp, vp, vp, u64]
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the shared library (once).  Raises CudaInit when it is absent."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(path):
+                raise CudaInit(f"native library not built: {path} (run `make -C flash-map_b200`)")
+            try:
+                L = C.CDLL(path)
+            except OSError as e:  # pragma: no cover - depends on the host
+                raise CudaInit(f"cannot load {path}: {e}") from e
+            _declare(L)
+            _lib = L
+        return _lib
+
+
+def last_error() -> str:
+    msg = load_library().fm_last_error()
+    return msg.decode() if msg else ""

@@ -1,0 +1,131 @@
+/*
+ * flashmap_b200.h -- C ABI of the FlashMap B200 backend (libflashmap_b200.so).
+ *
+ * This ABI replaces the reference's src/gpu.rs (bajpainaman/flash-map 0.5.0):
+ * each entry point below is what a thin Rust `GpuFlashMap<K, V>` shim binds so
+ * that src/lib.rs (FlashMap / FlashMapBuilder) and src/async_map.rs
+ * (AsyncFlashMap) stay unchanged.  Citations are file:line in the reference.
+ *
+ * Conventions
+ *  - Every call returns an fm_status; 0 is success.  A thread-local message
+ *    for the last failure is available from fm_last_error().
+ *  - Keys and values are fixed-size byte records (K = key_size bytes,
+ *    V = value_size bytes), laid out structure-of-arrays: n keys back to back,
+ *    n values back to back.  A Rust (K, V) tuple has no C layout, so the shim
+ *    splits pairs exactly as gpu.rs:212-217 does.
+ *  - Host-pointer entry points copy inputs to the GPU, run, copy results back
+ *    and return when the results are in place (gpu.rs's synchronous model).
+ *  - *_device entry points take raw device pointers (cudarc CudaSlice device
+ *    pointers) and a CUDA stream (cudaStream_t / CUstream cast to void*; NULL =
+ *    the legacy default stream).  Work is ordered on that stream.
+ *  - Results are bit-exact with the reference's sequential semantics
+ *    (src/rayon_cpu.rs:82-328 applied in batch index order): in-batch
+ *    duplicate keys resolve to the later position, tombstones are reused by
+ *    inserts, and gets stop at the Robin Hood exit.
+ *  - Thread safety: fm_bulk_get* may run concurrently on one table (the
+ *    AsyncFlashMap read lock, async_map.rs:48-61).  Mutating calls (insert,
+ *    remove, clear, recount) must be exclusive on a table (`&mut self`).
+ */
+#ifndef FLASHMAP_B200_H
+#define FLASHMAP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  1-6 map one to one onto FlashMapError (src/error.rs:5-27). */
+typedef enum fm_status {
+    FM_OK = 0,
+    FM_ERR_CUDA_INIT = 1,       /* FlashMapError::CudaInit */
+    FM_ERR_GPU_ALLOC = 2,       /* FlashMapError::GpuAlloc */
+    FM_ERR_KERNEL_LAUNCH = 3,   /* FlashMapError::KernelLaunch */
+    FM_ERR_TRANSFER = 4,        /* FlashMapError::Transfer */
+    FM_ERR_TABLE_FULL = 5,      /* FlashMapError::TableFull: occupied = fm_len(),
+                                   capacity = fm_capacity() */
+    FM_ERR_ZERO_CAPACITY = 6,   /* FlashMapError::ZeroCapacity */
+    FM_ERR_INVALID_ARG = 7,     /* -> KernelLaunch with message (unsupported size, NULL) */
+    FM_ERR_DEVICE_TIMEOUT = 8,  /* -> KernelLaunch with message (bounded device wait ran out) */
+    FM_ERR_PROBE_LIMIT = 9      /* -> KernelLaunch with message (round limit exceeded) */
+} fm_status;
+
+/* HashStrategy::to_mode (src/hash.rs:22-27). */
+#define FM_HASH_IDENTITY 0u
+#define FM_HASH_MURMUR3 1u
+
+typedef struct fm_table fm_table;
+
+/* GpuFlashMap::new (gpu.rs:45-105).  capacity 0 -> FM_ERR_ZERO_CAPACITY;
+ * otherwise rounded up to the next power of two (gpu.rs:54).  Allocates the
+ * zeroed SoA table on `device_id` (the CUDA primary context). */
+int fm_create(uint64_t capacity, uint32_t key_size, uint32_t value_size, uint32_t hash_mode,
+              int device_id, fm_table** out);
+
+/* Drop for GpuFlashMap: frees the table and every buffer the library owns. */
+void fm_destroy(fm_table* t);
+
+/* GpuFlashMap::bulk_get (gpu.rs:111-191).  out_values receives n*V bytes
+ * (zeros for misses), out_found n bytes (1 = found, 0 = miss). */
+int fm_bulk_get(fm_table* t, const void* keys, uint64_t n, void* out_values, uint8_t* out_found);
+
+/* GpuFlashMap::bulk_insert (gpu.rs:193-273).  Precheck len + n > capacity ->
+ * FM_ERR_TABLE_FULL before any mutation (gpu.rs:198-206).  *num_new = number
+ * of keys not present before (updates do not count). */
+int fm_bulk_insert(fm_table* t, const void* keys, const void* values, uint64_t n, uint64_t* num_new);
+
+/* GpuFlashMap::bulk_remove (gpu.rs:275-332).  *num_removed = keys tombstoned. */
+int fm_bulk_remove(fm_table* t, const void* keys, uint64_t n, uint64_t* num_removed);
+
+/* len / capacity / load_factor (gpu.rs:334-348).  len is a host-side count. */
+uint64_t fm_len(const fm_table* t);
+uint64_t fm_capacity(const fm_table* t);
+double fm_load_factor(const fm_table* t);
+
+/* GpuFlashMap::clear (gpu.rs:350-374): every slot EMPTY, len = 0. */
+int fm_clear(fm_table* t);
+
+/* GpuFlashMap::device (gpu.rs:381-383): the CUDA device ordinal. */
+int fm_device(const fm_table* t);
+
+/* GpuFlashMap::bulk_get_device (gpu.rs:422-478).  Outputs are caller-owned
+ * device buffers (n*V and n bytes); misses are written as zeros. */
+int fm_bulk_get_device(fm_table* t, const void* d_keys, uint64_t n, void* d_out_values,
+                       uint8_t* d_out_found, void* stream);
+
+/* GpuFlashMap::bulk_get_values_device (gpu.rs:484-536): no found mask;
+ * misses are written as zeros. */
+int fm_bulk_get_values_device(fm_table* t, const void* d_keys, uint64_t n, void* d_out_values,
+                              void* stream);
+
+/* GpuFlashMap::bulk_insert_device (gpu.rs:541-611): precheck, then a 4-byte
+ * class readback of the new-key count. */
+int fm_bulk_insert_device(fm_table* t, const void* d_keys, const void* d_values, uint64_t n,
+                          uint64_t* num_new, void* stream);
+
+/* GpuFlashMap::bulk_insert_device_uncounted (gpu.rs:618-672): no precheck,
+ * len += n; call fm_recount for the exact count. */
+int fm_bulk_insert_device_uncounted(fm_table* t, const void* d_keys, const void* d_values, uint64_t n,
+                                    void* stream);
+
+/* Device-pointer counterpart of bulk_remove (gpu.rs:275-332) for pipelines
+ * that keep keys on the GPU. */
+int fm_bulk_remove_device(fm_table* t, const void* d_keys, uint64_t n, uint64_t* num_removed,
+                          void* stream);
+
+/* GpuFlashMap::recount (gpu.rs:677-712): counts OCCUPIED slots, len := count. */
+int fm_recount(fm_table* t, uint64_t* out);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* fm_last_error(void);
+
+/* Raw table access for layout checks and for loading a prefilled table:
+ * flags (capacity u32), keys (capacity*K bytes), values (capacity*V bytes),
+ * all host pointers; any may be NULL to skip it. */
+int fm_snapshot(fm_table* t, uint32_t* flags, void* keys, void* values);
+int fm_load(fm_table* t, const uint32_t* flags, const void* keys, const void* values, uint64_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLASHMAP_B200_H */
