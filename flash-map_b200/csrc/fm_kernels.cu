@@ -543,6 +543,8 @@ __global__ void __launch_bounds__(BLOCK) k_rem_reset(TableView t, const uint8_t*
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npend; i += gridDim.x * blockDim.x) {
         const uint32_t j = pend[i];
         const uint32_t npt = sc.op_flag[j];
+        const uint32_t wend = sc.op_word[j];
+        sc.op_word[j] = IDLE;  // the word is the insert's inflow bound between calls
         if (npt == 0) continue;
         RegKey<KB> key;
         key.load(keys + (uint64_t)j * ksz, ksz);
@@ -550,7 +552,6 @@ __global__ void __launch_bounds__(BLOCK) k_rem_reset(TableView t, const uint8_t*
         if (npt <= PT_MAX) {
             for (uint32_t k = 0; k < npt; k++) t.seg_min[(h + sc.op_pt[(uint64_t)j * PT_MAX + k]) & mask] = IDLE;
         } else {
-            const uint32_t wend = sc.op_word[j];
             for (uint64_t q = 0; q <= wend; ++q) {
                 const uint64_t s = (h + q) & mask;
                 if (t.seg_min[s] != IDLE) t.seg_min[s] = IDLE;
