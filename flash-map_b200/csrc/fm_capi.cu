@@ -271,6 +271,8 @@ extern "C" {
 
 const char* fm_last_error(void) { return tl_err.c_str(); }
 
+uint64_t fm_launch_count(void) { return fm::launch_count(); }
+
 int fm_create(uint64_t capacity, uint32_t key_size, uint32_t value_size, uint32_t hash_mode, int device_id,
               fm_table** out) {
     if (!out) return fail(FM_ERR_INVALID_ARG, "out is NULL");

@@ -54,5 +54,6 @@ cudaError_t launch_rem_round(const TableView& t, Shape sh, const uint8_t* keys, 
                              cudaStream_t s);
 cudaError_t launch_count(const TableView& t, Ctl* ctl, cudaStream_t s);
 int num_sms();
+unsigned long long launch_count();
 
 }  // namespace fm

@@ -22,7 +22,7 @@
 //  * remove  (k_rem_scan / k_rem_check / k_rem_reset, in rounds): an op runs
 //            unless an earlier pending op has a possible target inside its
 //            dependency window.  rayon_cpu.rs:273-328.
-#include <cooperative_groups.h>
+#include <atomic>
 
 #include "fm_internal.h"
 
@@ -32,6 +32,7 @@ namespace {
 
 constexpr int BLOCK = 256;
 int g_num_sms = 0;
+std::atomic<unsigned long long> g_launches{0};
 
 __device__ __forceinline__ uint32_t warp_min_u32(uint32_t v) { return __reduce_min_sync(0xFFFFFFFFu, v); }
 
@@ -591,6 +592,7 @@ template <int KB, int VB>
 cudaError_t get_shape(const TableView& t, const uint8_t* q, uint64_t n, uint8_t* ov, uint8_t* of, cudaStream_t s) {
     constexpr int T = 8;
     k_get<KB, VB, T><<<grid_for(n * T, 16), BLOCK, 0, s>>>(t, q, n, ov, of);
+    g_launches += 1;
     return cudaGetLastError();
 }
 
@@ -603,6 +605,7 @@ cudaError_t ins_round_shape(const TableView& t, const uint8_t* keys, const uint8
     k_ins_walk<<<g, BLOCK, 0, s>>>(t, pend, npend, nops, sc.op_slot, sc.op_word, sc.op_flag, ctl);
     k_ins_exec<KB, VB><<<g, BLOCK, 0, s>>>(t, keys, vals, pend, npend, pend_next, sc.op_slot, sc.op_word,
                                            sc.op_flag, ctl);
+    g_launches += 3;
     return cudaGetLastError();
 }
 
@@ -613,10 +616,13 @@ cudaError_t rem_round_shape(const TableView& t, const uint8_t* keys, const uint3
     k_rem_scan<KB><<<g, BLOCK, 0, s>>>(t, keys, pend, npend, sc, ctl);
     k_rem_check<KB><<<g, BLOCK, 0, s>>>(t, keys, pend, npend, pend_next, sc, ctl);
     k_rem_reset<KB><<<g, BLOCK, 0, s>>>(t, keys, pend, npend, sc);
+    g_launches += 3;
     return cudaGetLastError();
 }
 
 }  // namespace
+
+unsigned long long launch_count() { return g_launches.load(); }
 
 int num_sms() {
     if (g_num_sms == 0) {
@@ -653,6 +659,7 @@ cudaError_t launch_get(const TableView& t, Shape sh, const uint8_t* q, uint64_t 
 cudaError_t launch_iota(uint32_t* p, uint64_t n, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     k_iota<<<grid_for(n, 8), BLOCK, 0, s>>>(p, n);
+    g_launches += 1;
     return cudaGetLastError();
 }
 
@@ -683,6 +690,7 @@ cudaError_t launch_rem_round(const TableView& t, Shape sh, const uint8_t* keys, 
 
 cudaError_t launch_count(const TableView& t, Ctl* ctl, cudaStream_t s) {
     k_count<<<grid_for(t.mask + 1, 4), BLOCK, 0, s>>>(t.flags, t.mask + 1, ctl);
+    g_launches += 1;
     return cudaGetLastError();
 }
 

@@ -20,7 +20,7 @@ EXPORTS = (
     "fm_create", "fm_destroy", "fm_bulk_get", "fm_bulk_insert", "fm_bulk_remove", "fm_len",
     "fm_capacity", "fm_load_factor", "fm_clear", "fm_device", "fm_bulk_get_device",
     "fm_bulk_get_values_device", "fm_bulk_insert_device", "fm_bulk_insert_device_uncounted",
-    "fm_bulk_remove_device", "fm_recount", "fm_last_error", "fm_snapshot", "fm_load",
+    "fm_bulk_remove_device", "fm_recount", "fm_last_error", "fm_launch_count", "fm_snapshot", "fm_load",
 )
 
 _lock = threading.Lock()
@@ -62,6 +62,8 @@ def _declare(L) -> None:
     L.fm_bulk_remove_device.argtypes = [vp, vp, u64, u64p, vp]
     L.fm_recount.restype = i32
     L.fm_recount.argtypes = [vp, u64p]
+    L.fm_launch_count.restype = u64
+    L.fm_launch_count.argtypes = []
     L.fm_last_error.restype = C.c_char_p
     L.fm_last_error.argtypes = []
     L.fm_snapshot.restype = i32
@@ -84,6 +86,11 @@ def load_library(path: str = LIB_PATH):
             _declare(L)
             _lib = L
         return _lib
+
+
+def launch_count() -> int:
+    """Kernels launched by the library in this process (instrumentation)."""
+    return load_library().fm_launch_count()
 
 
 def last_error() -> str:

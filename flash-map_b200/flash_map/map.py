@@ -121,17 +121,26 @@ class FlashMap:
         raise_for_status(rc, _native.last_error(), self.len(), self.capacity())
 
     # -- host-facing bulk API (lib.rs:123-162, gpu.rs:111-332) ---------------
-    def bulk_get(self, keys: ArrayLike) -> Tuple[np.ndarray, np.ndarray]:
+    def bulk_get(self, keys: ArrayLike, out_values: Optional[np.ndarray] = None,
+                 out_found: Optional[np.ndarray] = None) -> Tuple[np.ndarray, np.ndarray]:
         """Look up keys.  Returns ``(values, found)``: ``values`` is
         ``(n, value_size)`` uint8 with zeros for misses, ``found`` a bool mask
-        (the ``Vec<Option<V>>`` of the reference, split)."""
+        (the ``Vec<Option<V>>`` of the reference, split).  Preallocated
+        C-contiguous host buffers (``(n, value_size)`` and ``(n,)`` uint8, for
+        example pinned memory) may be passed to avoid per-call allocation; the
+        found mask is then returned as those uint8 bytes."""
         k = as_records(keys, self.key_size, "keys")
         n = len(k)
-        vals = np.zeros((n, self.value_size), np.uint8)
-        found = np.zeros(n, np.uint8)
+        given = out_found is not None
+        vals = np.zeros((n, self.value_size), np.uint8) if out_values is None else out_values
+        found = np.zeros(n, np.uint8) if out_found is None else out_found
+        if vals.shape != (n, self.value_size) or vals.dtype != np.uint8 or not vals.flags.c_contiguous:
+            raise ValueError("out_values must be a C-contiguous (n, value_size) uint8 array")
+        if found.shape != (n,) or found.dtype != np.uint8:
+            raise ValueError("out_found must be an (n,) uint8 array")
         if n:
             self._check(self._L.fm_bulk_get(self._h, _ptr(k), n, _ptr(vals), _ptr(found)))
-        return vals, found.astype(bool)
+        return vals, (found if given else found.astype(bool))
 
     def bulk_get_options(self, keys: ArrayLike) -> List[Optional[bytes]]:
         """``bulk_get`` as a list of ``Optional[bytes]`` (``Vec<Option<V>>``)."""

@@ -119,6 +119,10 @@ int fm_recount(fm_table* t, uint64_t* out);
 /* Message of the last failed call on this thread ("" if none). */
 const char* fm_last_error(void);
 
+/* Instrumentation (no counterpart in gpu.rs): number of kernels this library
+ * has launched in the process so far, across all tables. */
+uint64_t fm_launch_count(void);
+
 /* Raw table access for layout checks and for loading a prefilled table:
  * flags (capacity u32), keys (capacity*K bytes), values (capacity*V bytes),
  * all host pointers; any may be NULL to skip it. */
