@@ -126,15 +126,19 @@ def cpu_baseline_leg():
     import oracle as O
 
     inp = cpu_sample_inputs()
-    dt, _ = cpu_step(O, inp)
+    reps, total = 0, 0.0
+    while reps < 64 and (total < 8.0 or reps < 2):  # ~10 s of CPU work
+        dt, _ = cpu_step(O, inp)
+        total += dt
+        reps += 1
     _, tr = cpu_step(O, inp, traffic=True)
     return {
-        "value": round(sample_ops() / dt / 1e6, 3),
+        "value": round(sample_ops() * reps / total / 1e6, 3),
         "unit": "Mops/s",
         "cores": 1,
         "kind": "port",
         "sample": f"the same step at 1/{SAMPLE_DIV} scale (2^20 slots, 500K pairs in 5x100K inserts, 500K gets, "
-                  f"50K removes; same load factors), sequential C oracle, {dt:.2f} s",
+                  f"50K removes; same load factors), sequential C oracle, {reps} reps in {total:.1f} s",
     }, bytes_per_op(tr)
 
 
@@ -183,7 +187,7 @@ class Clocks:
                  "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh, stderr=subprocess.DEVNULL)
+                 "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
@@ -239,8 +243,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--scale", type=int, default=1,
+                    help="divide the table and batch counts by this power of two (same call size and load "
+                         "factors; for profiling captures on a small case)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.scale > 1:
+        global CAP_REQ, N_PAIRS, N_GET, N_REM
+        CAP_REQ //= args.scale
+        N_PAIRS //= args.scale
+        N_GET //= args.scale
+        N_REM //= args.scale
     if args.impl == "reference":
         return reference_arm(args)
 
@@ -285,19 +299,18 @@ def main():
             ev[1].record(stream)
         m.bulk_remove_device(rem, N_REM, stream)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    # correctness guard on the timed workload (not a parity test)
-    assert m.len() == N_PAIRS - N_REM, m.len()
-    assert int(out_f.sum().item()) == N_GET // 2
-
     phase = [(Ev(enable_timing=True), Ev(enable_timing=True)) for _ in range(args.steps)]
     starts = [Ev(enable_timing=True) for _ in range(args.steps)]
     ends = [Ev(enable_timing=True) for _ in range(args.steps)]
     t_all0, t_all1 = Ev(enable_timing=True), Ev(enable_timing=True)
-    l0 = _native.launch_count()
-    with Clocks(local) as clk:
+    with Clocks(local) as clk:  # sampled from the warm-up on, through the timed steps
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        # correctness guard on the timed workload (not a parity test)
+        assert m.len() == N_PAIRS - N_REM, m.len()
+        assert int(out_f.sum().item()) == N_GET // 2
+        l0 = _native.launch_count()
         barrier()
         torch.cuda.synchronize()
         t_all0.record(stream)
@@ -322,39 +335,43 @@ def main():
     value = ops_step * world / (ms_step / 1e3) / 1e6
 
     # ---- end to end through the host API (pinned host buffers) ----------
-    hk = keys.cpu().pin_memory().numpy()
-    hv = vals.cpu().pin_memory().numpy()
-    hq = q.cpu().pin_memory().numpy()
-    hr = rem.cpu().pin_memory().numpy()
-    ho = torch.empty((N_GET, VB), dtype=torch.uint8).pin_memory().numpy()
-    hf = torch.empty((N_GET,), dtype=torch.uint8).pin_memory().numpy()
+    def run_e2e():
+        hk = keys.cpu().pin_memory().numpy()
+        hv = vals.cpu().pin_memory().numpy()
+        hq = q.cpu().pin_memory().numpy()
+        hr = rem.cpu().pin_memory().numpy()
+        ho = torch.empty((N_GET, VB), dtype=torch.uint8).pin_memory().numpy()
+        hf = torch.empty((N_GET,), dtype=torch.uint8).pin_memory().numpy()
 
-    def step_host():
-        m.clear()
-        for b in range(0, N_PAIRS, CALL):
-            m.bulk_insert(hk[b:b + CALL], hv[b:b + CALL])
-        m.bulk_get(hq, out_values=ho, out_found=hf)
-        m.bulk_remove(hr)
+        def step_host():
+            m.clear()
+            for b in range(0, N_PAIRS, CALL):
+                m.bulk_insert(hk[b:b + CALL], hv[b:b + CALL])
+            m.bulk_get(hq, out_values=ho, out_found=hf)
+            m.bulk_remove(hr)
 
-    for _ in range(1):
-        step_host()
-    assert int(hf.sum()) == N_GET // 2
-    e2e_steps = max(1, min(args.steps, 3))
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        step_host()
-    torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": round(ops_step * world / e2e_s / 1e6, 3), "unit": "Mops/s",
-           "h2d_bytes_per_step": N_PAIRS * (KB + VB) + N_GET * KB + N_REM * KB,
-           "d2h_bytes_per_step": N_GET * (VB + 1) + 8 * (N_PAIRS // CALL + 1),
-           "ms_per_step": round(e2e_s * 1e3, 3)}
+        for _ in range(1):
+            step_host()
+        assert int(hf.sum()) == N_GET // 2
+        e2e_steps = max(1, min(args.steps, 3))
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            step_host()
+        torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        if dist is not None:
+            t = torch.tensor([e2e_s], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": round(ops_step * world / e2e_s / 1e6, 3), "unit": "Mops/s",
+               "h2d_bytes_per_step": N_PAIRS * (KB + VB) + N_GET * KB + N_REM * KB,
+               "d2h_bytes_per_step": N_GET * (VB + 1) + 8 * (N_PAIRS // CALL + 1),
+               "ms_per_step": round(e2e_s * 1e3, 3)}
+        return e2e
+
+    e2e = None if args.no_e2e else run_e2e()
 
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Mops/s", "n_gpus": world, "steps": args.steps,
@@ -364,9 +381,10 @@ def main():
         "ops": {"insert_mops": round(N_PAIRS / ins_ms / 1e3, 3), "get_mops": round(N_GET / get_ms / 1e3, 3),
                 "remove_mops": round(N_REM / rem_ms / 1e3, 3), "insert_ms": round(ins_ms, 3),
                 "get_ms": round(get_ms, 3), "remove_ms": round(rem_ms, 3)},
-        "e2e": e2e,
         "gpu_launches": int(launches),
     }
+    if e2e:
+        line["e2e"] = e2e
     clk_sum = clk.summary()
     if clk_sum:
         line["clocks"] = clk_sum

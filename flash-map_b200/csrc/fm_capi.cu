@@ -80,7 +80,7 @@ struct fm_table {
     uint32_t* d_seg_cnt = nullptr;
     Ctl* d_ctl = nullptr;
     Ctl* h_ctl = nullptr;    // pinned mirror for readbacks
-    Ctl* h_reset = nullptr;  // pinned per-round reset template
+    uint32_t last_rounds = 0;  // rounds of the last mutating call (statistics)
     std::atomic<uint64_t> len{0};
     cudaStream_t stream = nullptr;  // mutating calls
     std::mutex mu;                  // serialises mutating calls and their scratch
@@ -120,7 +120,7 @@ namespace {
 
 int ensure_scratch(fm_table* t, uint64_t n) {
     if (t->sc.cap_ops >= n) return FM_OK;
-    // pend_a, pend_b (u32) | op_slot (u64) | op_word (u32) | op_flag (u8) | op_pt (PT_MAX u32)
+    // pend[0], pend[1] (u32) | op_slot (u64) | op_word (u32) | op_flag (u8) | op_pt (PT_MAX u32)
     const uint64_t per_op = 4 + 4 + 8 + 4 + 1 + 4 * fm::PT_MAX;
     const uint64_t want = n + n / 4 + 1024;
     const size_t bytes = (size_t)(want * per_op + 6 * 256);
@@ -136,8 +136,8 @@ int ensure_scratch(fm_table* t, uint64_t n) {
         return r;
     };
     t->sc.op_slot = (uint64_t*)carve(want * 8);
-    t->sc.pend_a = (uint32_t*)carve(want * 4);
-    t->sc.pend_b = (uint32_t*)carve(want * 4);
+    t->sc.pend[0] = (uint32_t*)carve(want * 4);
+    t->sc.pend[1] = (uint32_t*)carve(want * 4);
     t->sc.op_word = (uint32_t*)carve(want * 4);
     t->sc.op_pt = (uint32_t*)carve(want * 4 * fm::PT_MAX);
     t->sc.op_flag = carve(want);
@@ -145,13 +145,9 @@ int ensure_scratch(fm_table* t, uint64_t n) {
     t->sc_bytes = bytes;
     // op_word doubles as the insert inflow bound: idle value 0xFFFFFFFF.
     e = cudaMemsetAsync(t->sc.op_word, 0xFF, want * 4, t->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_GPU_ALLOC, "scratch init", e);
     return FM_OK;
-}
-
-// Reset the per-round fields of the control block (npend_next, gmin, serial).
-cudaError_t reset_round(fm_table* t, cudaStream_t s) {
-    return cudaMemcpyAsync(t->d_ctl, t->h_reset, 12, cudaMemcpyHostToDevice, s);
 }
 
 // After a failed call the segment registrations and the per-op scratch may be
@@ -163,7 +159,10 @@ void recover(fm_table* t, cudaStream_t s) {
     cudaStreamSynchronize(s);
 }
 
-// The round loop shared by insert and remove.  `insert` selects the kernel set.
+// The round driver shared by insert and remove.  Each pass launches two
+// grid-wide rounds and the single-block tail back to back, then reads the
+// control block once: a zero pending count for the next round means done.
+// Counts, lists and per-round flags stay in device memory between rounds.
 int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t* d_v, uint64_t n,
                      cudaStream_t s, uint64_t* out_count, uint32_t* err_bits) {
     uint64_t total = 0;
@@ -173,41 +172,43 @@ int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t
     if (rc) return rc;
     fm::TableView v = t->view();
     for (uint64_t base = 0; base < n; base += OP_CHUNK) {
-        const uint64_t m = (n - base) < OP_CHUNK ? (n - base) : OP_CHUNK;
+        const uint32_t m = (uint32_t)((n - base) < OP_CHUNK ? (n - base) : OP_CHUNK);
         const uint8_t* kk = d_k + base * t->ksz;
         const uint8_t* vv = d_v ? d_v + base * t->vsz : nullptr;
-        cudaError_t e = fm::launch_iota(t->sc.pend_a, m, s);
-        if (e == cudaSuccess) e = reset_round(t, s);
-        if (e == cudaSuccess) e = cudaMemsetAsync(&t->d_ctl->err, 0, 4, s);
-        if (e == cudaSuccess) e = cudaMemsetAsync(&t->d_ctl->count, 0, sizeof(unsigned long long), s);
+        cudaError_t e = cudaMemsetAsync(t->d_ctl, 0, fm::CTL_CALL_BYTES, s);
         if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "round setup", e);
-        uint32_t* pend = t->sc.pend_a;
-        uint32_t* next = t->sc.pend_b;
-        uint32_t npend = (uint32_t)m;
-        uint64_t rounds = 0;
-        while (npend > 0) {
-            e = insert ? fm::launch_ins_round(v, sh, kk, vv, pend, npend, (uint32_t)m, next, t->sc, t->d_ctl, s)
-                       : fm::launch_rem_round(v, sh, kk, pend, npend, next, t->sc, t->d_ctl, s);
-            if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, insert ? "insert round" : "remove round", e);
+        uint32_t r = 0;
+        uint32_t left = m;
+        for (;;) {
+            e = insert ? fm::launch_ins_rounds(v, sh, kk, vv, m, r, 2, left, t->sc, t->d_ctl, s)
+                       : fm::launch_rem_rounds(v, sh, kk, m, r, 2, left, t->sc, t->d_ctl, s);
+            r += 2;
+            if (e == cudaSuccess)
+                e = insert ? fm::launch_ins_tail(v, sh, kk, vv, m, r, t->sc, t->d_ctl, s)
+                           : fm::launch_rem_tail(v, sh, kk, m, r, t->sc, t->d_ctl, s);
+            if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, insert ? "insert rounds" : "remove rounds", e);
             e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
             if (e == cudaSuccess) e = cudaStreamSynchronize(s);
             if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "round readback", e);
-            const uint32_t left = t->h_ctl->npend_next;
             if (t->h_ctl->err & fm::ERR_SCRATCH) return fail(FM_ERR_KERNEL_LAUNCH, "stale segment registration");
-            if (left >= npend)  // every round runs at least the lowest pending op
-                return fail(FM_ERR_PROBE_LIMIT, "round made no progress");
-            ++rounds;
-            npend = left;
-            uint32_t* tmp = pend;
-            pend = next;
-            next = tmp;
-            if (npend) {
-                e = reset_round(t, s);
-                if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "round reset", e);
+            if (t->h_ctl->err & fm::ERR_NO_PROGRESS) return fail(FM_ERR_PROBE_LIMIT, "round made no progress");
+            uint32_t now = t->h_ctl->npend[r & 1];
+            if (insert && now > 0 && t->h_ctl->serial[(r - 1) & 1]) {
+                // the table is full: the remaining ops run one at a time in index order
+                e = fm::launch_ins_serial(v, sh, kk, vv, m, r, t->sc, t->d_ctl, s);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "serial insert", e);
+                now = t->h_ctl->npend[r & 1];
             }
+            if (now == 0) break;
+            if (now >= left)  // every round runs at least the lowest pending op
+                return fail(FM_ERR_PROBE_LIMIT, "round made no progress");
+            left = now;
         }
-        total += t->h_ctl->count;
+        total += t->h_ctl->total_count();
         *err_bits |= t->h_ctl->err;
+        t->last_rounds = t->h_ctl->rounds;
     }
     *out_count = total;
     return FM_OK;
@@ -315,10 +316,7 @@ int fm_create(uint64_t capacity, uint32_t key_size, uint32_t value_size, uint32_
     if ((e = cudaMalloc((void**)&t->d_seg_cnt, cap * 4)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "seg_cnt", e);
     if ((e = cudaMalloc((void**)&t->d_ctl, sizeof(Ctl))) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "ctl", e);
     if ((e = cudaMallocHost((void**)&t->h_ctl, sizeof(Ctl))) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "ctl", e);
-    if ((e = cudaMallocHost((void**)&t->h_reset, sizeof(Ctl))) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "ctl", e);
     memset(t->h_ctl, 0, sizeof(Ctl));
-    memset(t->h_reset, 0, sizeof(Ctl));
-    t->h_reset->gmin = fm::IDLE;
     // Zeroed SoA table: all flags EMPTY (gpu.rs:81-92).
     cudaMemsetAsync(t->d_flags, 0, cap * 4, t->stream);
     cudaMemsetAsync(t->d_keys, 0, kb, t->stream);
@@ -348,7 +346,6 @@ void fm_destroy(fm_table* t) {
     cudaFree(t->d_seg_cnt);
     cudaFree(t->d_ctl);
     if (t->h_ctl) cudaFreeHost(t->h_ctl);
-    if (t->h_reset) cudaFreeHost(t->h_reset);
     if (t->sc_base) cudaFree(t->sc_base);
     if (t->d_in) cudaFree(t->d_in);
     if (t->stream) cudaStreamDestroy(t->stream);

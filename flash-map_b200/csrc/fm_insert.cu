@@ -1,0 +1,834 @@
+// fm_insert.cu -- deterministic bulk insert for sm_100a.
+//
+// Semantics: the reference's sequential insert (src/rayon_cpu.rs:153-264; the
+// same walk as src/kernels.cu:224-313 run one key at a time) applied to the
+// batch in index order: Robin Hood eviction, update of an equal key in place,
+// claim of the first EMPTY or TOMBSTONE slot, drop past the capacity, and
+// in-batch duplicate keys resolved to the later position.
+//
+// Why rounds: an insert only reads and writes slots in [home, F], where F is
+// the first free (EMPTY or TOMBSTONE) slot at or after its home, so ops whose
+// segments end at different free slots touch disjoint slots and commute.  A
+// round runs the lowest-index pending op of every segment ("leader") unless an
+// earlier op could still reach that segment: a segment holding c >= 2 pending
+// ops can push up to c-1 of them past its free slot once it is consumed, so a
+// forward walk from every such segment carries that flow over the following
+// segments (each absorbs one op at its free slot and adds its own) and marks
+// the leaders it reaches with a lower bound on the op indices that could
+// arrive.  The lowest pending op is never blocked, so every round makes
+// progress.  When a round finds an op with no free slot anywhere (only an
+// uncounted insert can overfill a table) or a flow that wraps the whole
+// table, it runs nothing and the remaining ops are applied one at a time in
+// index order by a single thread (serial_process).
+//
+// Control: two grid-wide rounds are launched back to back (counts and lists
+// live in device memory, double-buffered by round parity), then one block
+// runs every remaining round with block barriers between phases when at most
+// TAIL_MAX ops are left.  The host reads the control block once per pass.
+// Grid kernels aggregate list appends and counts per block so no address
+// takes more than one atomic per block.
+#include <type_traits>
+
+#include "fm_rounds.cuh"
+
+namespace fm {
+namespace {
+
+template <int KB>
+__device__ __forceinline__ uint64_t find_free(const TableView& t, const uint8_t* keys, uint32_t j) {
+    const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
+    RegKey<KB> key;
+    key.load(keys + (uint64_t)j * ksz, ksz);
+    const uint64_t h = key.hash(ksz, t.hash_mode) & t.mask;
+    for (uint64_t p = 0; p <= t.mask; ++p) {
+        const uint64_t s = (h + p) & t.mask;
+        if (is_free(t.flags[s])) return s;
+    }
+    return NONE64;
+}
+
+__device__ __forceinline__ void register_op(const TableView& t, uint32_t j, uint64_t F, uint64_t* op_slot) {
+    op_slot[j] = F;
+    if (F != NONE64) {
+        atomicMin(&t.seg_min[F], j);
+        atomicAdd(&t.seg_cnt[F], 1u);
+    }
+}
+
+// Phase 2 for op j: records whether j leads its segment and, for a crowded
+// segment, walks the flow forward.  Returns bit 0 when the flow wraps the
+// whole table (serial round), bit 1 on a registration from another call.
+__device__ __forceinline__ uint32_t walk_op(const TableView& t, uint32_t j, uint32_t nops, const uint64_t* op_slot,
+                                            uint32_t* op_block, uint8_t* op_leader) {
+    const uint64_t mask = t.mask;
+    const uint64_t F = op_slot[j];
+    const bool leader = F != NONE64 && t.seg_min[F] == j;
+    op_leader[j] = leader ? 1 : 0;
+    if (!leader) return 0;
+    const uint32_t c = t.seg_cnt[F];
+    if (c < 2) return 0;
+    uint64_t flow = c - 1;
+    uint32_t L = j;
+    uint64_t pos = F + 1;
+    uint64_t walked = 0;
+    for (;;) {
+        // At most the capacity-1 slots after F; coming back to F means the
+        // flow wraps the whole table.
+        uint64_t F2 = NONE64;
+        while (walked < mask) {
+            const uint64_t s = pos & mask;
+            ++pos;
+            ++walked;
+            if (is_free(t.flags[s])) {
+                F2 = s;
+                break;
+            }
+        }
+        if (F2 == NONE64) return 1u;
+        const uint32_t c2 = t.seg_cnt[F2];
+        if (c2) {
+            const uint32_t l2 = t.seg_min[F2];
+            if (l2 >= nops) return 2u;  // registrations come only from this call's ops
+            atomicMin(&op_block[l2], L);
+            L = min(L, l2);
+        }
+        flow = flow + c2 - 1;
+        if (flow == 0) return 0;
+    }
+}
+
+struct ExecAcc {
+    uint32_t claimed = 0;
+    uint32_t maxd = 0;
+    bool tomb = false;
+    bool limit = false;
+};
+
+// The sequential insert of one key, run by one thread on the segment it owns
+// this round.  Returns 1 when a free slot was claimed.
+template <int KB, int VB>
+__device__ __noinline__ int exec_insert(const TableView& t, const uint8_t* kin, const uint8_t* vin, ExecAcc& a) {
+    const uint64_t mask = t.mask;
+    RegKey<KB> ck;
+    ck.load(kin, KB);
+    RegVal<VB> cv;
+    cv.load(vin, VB);
+    uint64_t h = ck.hash(KB, t.hash_mode) & mask;
+    uint64_t p = 0;
+    const uint64_t step_limit = 2 * (mask + 1) + 2;
+    for (uint64_t step = 0;; ++step) {
+        if (p > mask) return 0;  // drop (rayon_cpu.rs:167-169)
+        if (step > step_limit) {  // no free slot: the reference's loop may never end
+            a.limit = true;
+            return 0;
+        }
+        const uint64_t idx = (h + p) & mask;
+        const uint32_t f = t.flags[idx];
+        const uint32_t s = st_of(f);
+        if (s == ST_OCC) {
+            if (dist_matches(f, p) && ck.eq(t.keys + idx * KB, KB)) {
+                cv.store(t.vals + idx * VB, VB);  // update in place (rayon_cpu.rs:178-182)
+                return 0;
+            }
+            const uint64_t d = dist_of(f);
+            if (p > d) {  // Robin Hood eviction (rayon_cpu.rs:184-217)
+                RegKey<KB> tk;
+                tk.load_table(t.keys + idx * KB, KB);
+                RegVal<VB> tv;
+                tv.load(t.vals + idx * VB, VB);
+                ck.store(t.keys + idx * KB, KB);
+                cv.store(t.vals + idx * VB, VB);
+                t.flags[idx] = mk_flag(ST_OCC, p);
+                a.maxd = max(a.maxd, (uint32_t)min(p, (uint64_t)DIST_MASK));
+                ck = tk;
+                cv = tv;
+                h = ck.hash(KB, t.hash_mode) & mask;
+                p = d + 1;
+                continue;
+            }
+            ++p;
+            continue;
+        }
+        if (s == ST_EMPTY || s == ST_TOMB) {  // claim (rayon_cpu.rs:228-251)
+            ck.store(t.keys + idx * KB, KB);
+            cv.store(t.vals + idx * VB, VB);
+            t.flags[idx] = mk_flag(ST_OCC, p);
+            a.maxd = max(a.maxd, (uint32_t)min(p, (uint64_t)DIST_MASK));
+            a.tomb = a.tomb || s == ST_TOMB;
+            return 1;
+        }
+        ++p;
+    }
+}
+
+// Run-time sizes (up to GENERIC_MAX_KV bytes each): the carried entry lives in
+// a local buffer and is swapped with the slot byte by byte.
+__device__ __forceinline__ int exec_insert_generic(const TableView& t, const uint8_t* kin, const uint8_t* vin,
+                                                   ExecAcc& a) {
+    const uint64_t mask = t.mask;
+    const uint32_t ksz = t.ksz, vsz = t.vsz;
+    uint8_t ck[GENERIC_MAX_KV];
+    uint8_t cv[GENERIC_MAX_KV];
+    copy_bytes(ck, kin, ksz);
+    copy_bytes(cv, vin, vsz);
+    uint64_t h = hash_bytes(ck, ksz, t.hash_mode) & mask;
+    uint64_t p = 0;
+    const uint64_t step_limit = 2 * (mask + 1) + 2;
+    for (uint64_t step = 0;; ++step) {
+        if (p > mask) return 0;
+        if (step > step_limit) {
+            a.limit = true;
+            return 0;
+        }
+        const uint64_t idx = (h + p) & mask;
+        const uint32_t f = t.flags[idx];
+        const uint32_t s = st_of(f);
+        uint8_t* sk = t.keys + idx * ksz;
+        uint8_t* sv = t.vals + idx * vsz;
+        if (s == ST_OCC) {
+            bool eq = dist_matches(f, p);
+            for (uint32_t i = 0; eq && i < ksz; i++) eq = sk[i] == ck[i];
+            if (eq) {
+                copy_bytes(sv, cv, vsz);
+                return 0;
+            }
+            const uint64_t d = dist_of(f);
+            if (p > d) {
+                for (uint32_t i = 0; i < ksz; i++) {
+                    const uint8_t x = sk[i];
+                    sk[i] = ck[i];
+                    ck[i] = x;
+                }
+                for (uint32_t i = 0; i < vsz; i++) {
+                    const uint8_t x = sv[i];
+                    sv[i] = cv[i];
+                    cv[i] = x;
+                }
+                t.flags[idx] = mk_flag(ST_OCC, p);
+                a.maxd = max(a.maxd, (uint32_t)min(p, (uint64_t)DIST_MASK));
+                h = hash_bytes(ck, ksz, t.hash_mode) & mask;
+                p = d + 1;
+                continue;
+            }
+            ++p;
+            continue;
+        }
+        if (s == ST_EMPTY || s == ST_TOMB) {
+            copy_bytes(sk, ck, ksz);
+            copy_bytes(sv, cv, vsz);
+            t.flags[idx] = mk_flag(ST_OCC, p);
+            a.maxd = max(a.maxd, (uint32_t)min(p, (uint64_t)DIST_MASK));
+            a.tomb = a.tomb || s == ST_TOMB;
+            return 1;
+        }
+        ++p;
+    }
+}
+
+// Phase 3 for op j (scalar path): run it if it leads an unblocked segment of a
+// non-serial round, then clear its registration.  Returns whether it ran.
+template <int KB, int VB>
+__device__ __forceinline__ bool finish_op(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t j,
+                                          bool serial, const OpScratch& sc, ExecAcc& a) {
+    const bool run = !serial && sc.op_flag[j] != 0 && sc.op_word[j] > j;
+    if (run) {
+        const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
+        const uint32_t vsz = VB ? (uint32_t)VB : t.vsz;
+        if constexpr (KB == 0 || VB == 0)
+            a.claimed += exec_insert_generic(t, keys + (uint64_t)j * ksz, vals + (uint64_t)j * vsz, a);
+        else
+            a.claimed += exec_insert<KB, VB>(t, keys + (uint64_t)j * ksz, vals + (uint64_t)j * vsz, a);
+    }
+    const uint64_t F = sc.op_slot[j];
+    if (F != NONE64) {
+        t.seg_min[F] = IDLE;
+        t.seg_cnt[F] = 0;
+    }
+    sc.op_word[j] = IDLE;
+    return run;
+}
+
+// Rare facts, once per warp: the largest stored distance, tombstone reuse and
+// the full-table walk limit.
+__device__ __forceinline__ void publish_rare(Ctl* ctl, uint32_t maxd, bool tomb, bool limit) {
+    maxd = __reduce_max_sync(0xFFFFFFFFu, maxd);
+    tomb = __any_sync(0xFFFFFFFFu, tomb);
+    limit = __any_sync(0xFFFFFFFFu, limit);
+    if ((threadIdx.x & 31u) == 0) {
+        if (maxd > *(volatile uint32_t*)&ctl->dmax) atomicMax(&ctl->dmax, maxd);
+        if (tomb && !*(volatile uint32_t*)&ctl->tomb_claimed) ctl->tomb_claimed = 1u;
+        if (limit) atomicOr(&ctl->err, ERR_WALK_LIMIT);
+    }
+}
+
+// Applies the ops of `list` (n ops; nullptr = the identity over n ops) one at a
+// time in index order on thread 0 of one block -- the sequential semantics,
+// for rounds that found the table full.  Their registrations must already be
+// clear.  Block-uniform call; s_buf holds blockDim.x words, s_woff 33.
+template <int KB, int VB>
+__device__ void serial_process(const TableView& t, const uint8_t* keys, const uint8_t* vals, const uint32_t* list,
+                               uint32_t n, uint32_t n0, const OpScratch& sc, ExecAcc& a, uint32_t* s_buf,
+                               uint32_t* s_woff) {
+    const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
+    const uint32_t vsz = VB ? (uint32_t)VB : t.vsz;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sc.op_flag[list ? list[i] : i] = 3;
+    __syncthreads();
+    for (uint32_t base = 0; base < n0; base += blockDim.x) {
+        const uint32_t j = base + threadIdx.x;
+        const bool take = j < n0 && sc.op_flag[j] == 3;
+        const uint32_t c = block_compact(j, take, s_buf, s_woff);
+        if (threadIdx.x == 0) {
+            for (uint32_t k = 0; k < c; k++) {
+                const uint32_t jj = s_buf[k];
+                sc.op_flag[jj] = 0;
+                if constexpr (KB == 0 || VB == 0)
+                    a.claimed += exec_insert_generic(t, keys + (uint64_t)jj * ksz, vals + (uint64_t)jj * vsz, a);
+                else
+                    a.claimed += exec_insert<KB, VB>(t, keys + (uint64_t)jj * ksz, vals + (uint64_t)jj * vsz, a);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+
+// ---- tile-cooperative probe and execute (compile-time shapes) -------------
+//
+// A tile of T lanes reads T consecutive metadata words per step (T = 8: one
+// 32-byte sector).  The walk of an insert is decided by the metadata alone
+// except for key equality, so the tile computes the whole Robin Hood chain
+// (eviction slots P_0 < P_1 < ... and the end: claim, update or drop) with
+// ballots over the window, checks the possible updates (slots whose stored
+// distance equals the carried entry's probe depth) with parallel key
+// compares, and only then moves data: slot P_i receives the entry evicted at
+// P_(i-1) (P_0 the new entry), the end slot the last evicted one.  Sources are
+// read before destinations are written, highest move first, so the moves are
+// the sequential walk's writes in one pass.
+
+constexpr int MAXCH = 48;  // eviction chain kept per tile; longer chains run the scalar walk
+
+template <int T>
+__device__ __forceinline__ uint64_t find_free_tile(const TableView& t, uint64_t h, const Tile<T>& tl) {
+    const uint64_t mask = t.mask;
+    uint64_t wb = h & ~(uint64_t)(T - 1);
+    for (;;) {
+        const uint64_t pos = wb + tl.lane;
+        const bool before = pos < h;
+        const uint64_t p = pos - h;
+        const uint32_t f = t.flags[pos & mask];
+        const bool past = !before && p > mask;
+        const uint32_t fm = tl.ballot(!before && !past && is_free(f));
+        if (fm) return (wb + __ffs(fm) - 1) & mask;
+        if (tl.ballot(past)) return NONE64;
+        wb += T;
+    }
+}
+
+// Chunk type for moving KB/VB-byte records.
+template <int KB, int VB>
+struct ChunkOf {
+    static constexpr int CK = (KB % 16 == 0 && VB % 16 == 0) ? 16 : ((KB % 8 == 0 && VB % 8 == 0) ? 8 : 4);
+    using type = typename std::conditional<CK == 16, uint4, typename std::conditional<CK == 8, uint2, uint32_t>::type>::type;
+    static constexpr int NK = KB / CK;
+    static constexpr int NV = VB / CK;
+    static constexpr int NC = NK + NV;
+};
+
+template <int KB, int VB, int T>
+__device__ __forceinline__ void exec_tile(const TableView& t, const uint8_t* __restrict__ keys_in,
+                                          const uint8_t* __restrict__ vals_in, uint32_t j, const Tile<T>& tl,
+                                          uint64_t* s_pos, uint32_t* s_p, ExecAcc& a) {
+    using CO = ChunkOf<KB, VB>;
+    using Ch = typename CO::type;
+    constexpr int CK = CO::CK, NK = CO::NK, NC = CO::NC;
+    constexpr int MB = (4 * T) / NC > 0 ? (4 * T) / NC : 1;  // moves per batch (<= 4 chunks per lane)
+    constexpr int CPL = (MB * NC + T - 1) / T;
+    const uint64_t mask = t.mask;
+    const uint32_t lane = tl.lane;
+    RegKey<KB> key;
+    key.load(keys_in + (uint64_t)j * KB, KB);
+    const uint64_t h = key.hash(KB, t.hash_mode) & mask;
+
+    // -- walk: metadata only, plus key compares at possible updates ----------
+    uint64_t sstart = h, pstart = 0;
+    uint32_t stage = 0;
+    int kind = 0;  // 1 claim, 2 update, 3 drop, 4 chain too long
+    uint64_t end_pos = 0, end_p = 0;
+    bool end_tomb = false;
+    uint64_t wb = h & ~(uint64_t)(T - 1);
+    while (kind == 0) {
+        const uint64_t pos = wb + lane;
+        const uint32_t f = t.flags[pos & mask];
+        for (;;) {
+            const bool in = pos >= sstart;
+            const uint64_t q = pstart + (pos - sstart);
+            const uint32_t st = st_of(f);
+            const bool drop = in && q > mask;
+            const bool occ = in && !drop && st == ST_OCC;
+            const bool ev_l = drop || (in && !drop && (st == ST_EMPTY || st == ST_TOMB)) || (occ && q > dist_of(f));
+            const uint32_t em = tl.ballot(ev_l);
+            const uint32_t elane = em ? (uint32_t)(__ffs(em) - 1) : (uint32_t)T;
+            bool match = false;
+            if (occ && lane < elane && dist_matches(f, q)) {
+                const uint8_t* sk = t.keys + (pos & mask) * KB;
+                if (stage == 0) {
+                    match = key.eq(sk, KB);
+                } else {
+                    RegKey<KB> ck;  // the carried entry's key, still at its old slot
+                    ck.load_table(t.keys + (s_pos[stage - 1] & mask) * KB, KB);
+                    match = ck.eq(sk, KB);
+                }
+            }
+            const uint32_t mm = tl.ballot(match);
+            if (mm) {
+                kind = 2;
+                end_pos = wb + __ffs(mm) - 1;
+                break;
+            }
+            if (!em) break;
+            const uint64_t epos = wb + elane;
+            const uint32_t ef = tl.shfl(f, elane);
+            const uint64_t eq = pstart + (epos - sstart);
+            if (eq > mask) {
+                kind = 3;
+                break;
+            }
+            if (st_of(ef) == ST_EMPTY || st_of(ef) == ST_TOMB) {
+                kind = 1;
+                end_pos = epos;
+                end_p = eq;
+                end_tomb = st_of(ef) == ST_TOMB;
+                break;
+            }
+            if (stage >= (uint32_t)MAXCH) {
+                kind = 4;
+                break;
+            }
+            if (lane == 0) {
+                s_pos[stage] = epos;
+                s_p[stage] = (uint32_t)min(eq, (uint64_t)0xFFFFFFFFu);
+            }
+            tl.sync();
+            ++stage;
+            sstart = epos + 1;
+            pstart = dist_of(ef) + 1;
+        }
+        wb += T;
+    }
+    if (kind == 4) {  // very long chain: the sequential walk, on lane 0
+        if (lane == 0) a.claimed += exec_insert<KB, VB>(t, keys_in + (uint64_t)j * KB, vals_in + (uint64_t)j * VB, a);
+        tl.sync();
+        return;
+    }
+    tl.sync();
+
+    // -- moves: move m puts the entry of source(m) into dest(m) ---------------
+    // m < stage: dest P_m; m == stage: dest = end slot (claim: whole entry;
+    // update: value only; drop: no such move).  source(0) = the new entry,
+    // source(m) = P_(m-1).
+    const uint32_t k = stage;
+    const int M = (kind == 3) ? (int)k : (int)k + 1;
+    for (int hi = M - 1; hi >= 0; hi -= MB) {
+        const int lo = hi - MB + 1 > 0 ? hi - MB + 1 : 0;
+        const int nchunks = (hi - lo + 1) * NC;
+        Ch buf[CPL];
+#pragma unroll
+        for (int u = 0; u < CPL; u++) {
+            const int g = (int)lane + u * T;
+            if (g < nchunks) {
+                const int m = lo + g / NC, c = g % NC;
+                const bool value_only = (m == (int)k) && kind == 2;
+                if (value_only && c < NK) continue;
+                const uint8_t* src;
+                if (m == 0) src = c < NK ? keys_in + (uint64_t)j * KB + c * CK : vals_in + (uint64_t)j * VB + (c - NK) * CK;
+                else {
+                    const uint64_t ss = s_pos[m - 1] & mask;
+                    src = c < NK ? t.keys + ss * KB + c * CK : t.vals + ss * VB + (c - NK) * CK;
+                }
+                buf[u] = *reinterpret_cast<const Ch*>(src);
+            }
+        }
+        tl.sync();
+#pragma unroll
+        for (int u = 0; u < CPL; u++) {
+            const int g = (int)lane + u * T;
+            if (g < nchunks) {
+                const int m = lo + g / NC, c = g % NC;
+                const bool value_only = (m == (int)k) && kind == 2;
+                if (value_only && c < NK) continue;
+                const uint64_t ds = ((m < (int)k) ? s_pos[m] : end_pos) & mask;
+                uint8_t* dst = c < NK ? t.keys + ds * KB + c * CK : t.vals + ds * VB + (c - NK) * CK;
+                *reinterpret_cast<Ch*>(dst) = buf[u];
+            }
+        }
+        tl.sync();
+    }
+    // metadata of every moved entry
+    uint32_t md = 0;
+    for (uint32_t m = lane; m < k; m += T) {
+        t.flags[s_pos[m] & mask] = mk_flag(ST_OCC, s_p[m]);
+        md = max(md, min(s_p[m], DIST_MASK));
+    }
+    if (lane == 0) {
+        if (kind == 1) {
+            t.flags[end_pos & mask] = mk_flag(ST_OCC, end_p);
+            md = max(md, (uint32_t)min(end_p, (uint64_t)DIST_MASK));
+            a.claimed += 1;
+            a.tomb = a.tomb || end_tomb;
+        }
+    }
+    a.maxd = max(a.maxd, md);
+}
+
+
+// ---- grid-wide round phases ---------------------------------------------
+
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_ins_p1(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
+                                                   uint32_t r, OpScratch sc, Ctl* ctl) {
+    const RoundOps ops = round_ops(sc, ctl, r, n0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) reset_next_round(ctl, r);
+    bool no_free = false;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ops.n; i += gridDim.x * blockDim.x) {
+        const uint32_t j = ops.op(i);
+        const uint64_t F = find_free<KB>(t, keys, j);
+        register_op(t, j, F, sc.op_slot);
+        no_free = no_free || F == NONE64;
+    }
+    if (no_free) ctl->serial[r & 1] = 1u;
+}
+
+__global__ void __launch_bounds__(RBLOCK) k_ins_p2(TableView t, uint32_t n0, uint32_t r, uint32_t nops,
+                                                   OpScratch sc, Ctl* ctl) {
+    const RoundOps ops = round_ops(sc, ctl, r, n0);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ops.n; i += gridDim.x * blockDim.x) {
+        const uint32_t bits = walk_op(t, ops.op(i), nops, sc.op_slot, sc.op_word, sc.op_flag);
+        if (bits & 1u) ctl->serial[r & 1] = 1u;
+        if (bits & 2u) atomicOr(&ctl->err, ERR_SCRATCH);
+    }
+}
+
+template <int KB, int VB>
+__global__ void __launch_bounds__(RBLOCK) k_ins_p3(TableView t, const uint8_t* __restrict__ keys,
+                                                   const uint8_t* __restrict__ vals, uint32_t n0, uint32_t r,
+                                                   OpScratch sc, Ctl* ctl) {
+    __shared__ AppendSmem s_app;
+    __shared__ uint32_t s_tmp[RBLOCK / 32];
+    const RoundOps ops = round_ops(sc, ctl, r, n0);
+    const bool serial = *(volatile uint32_t*)&ctl->serial[r & 1] != 0;
+    uint32_t* out = pend_of(sc, r + 1);
+    uint32_t* out_n = &ctl->npend[(r + 1) & 1];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t iters = grid_iters(ops.n);
+    ExecAcc a;
+    for (uint32_t it = 0; it < iters; it++) {
+        const uint32_t i = i0 + it * stride;
+        const bool valid = i < ops.n;
+        uint32_t j = 0;
+        bool ran = false;
+        if (valid) {
+            j = ops.op(i);
+            ran = finish_op<KB, VB>(t, keys, vals, j, serial, sc, a);
+        }
+        block_append(out, out_n, j, valid && !ran, s_app);
+    }
+    block_add_count(ctl, a.claimed, s_tmp);
+    publish_rare(ctl, a.maxd, a.tomb, a.limit);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && ops.n) atomicAdd(&ctl->rounds, 1u);
+}
+
+// ---- tile-cooperative round phases (compile-time shapes) -----------------
+
+template <int KB, int T>
+__global__ void __launch_bounds__(RBLOCK) k_ins_p1t(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
+                                                    uint32_t r, OpScratch sc, Ctl* ctl) {
+    const RoundOps ops = round_ops(sc, ctl, r, n0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) reset_next_round(ctl, r);
+    const Tile<T> tl;
+    const uint32_t ntiles = gridDim.x * (blockDim.x / T);
+    bool no_free = false;
+    for (uint32_t i = blockIdx.x * (blockDim.x / T) + threadIdx.x / T; i < ops.n; i += ntiles) {
+        const uint32_t j = ops.op(i);
+        RegKey<KB> key;
+        key.load(keys + (uint64_t)j * KB, KB);
+        const uint64_t F = find_free_tile<T>(t, key.hash(KB, t.hash_mode) & t.mask, tl);
+        if (tl.lane == 0) register_op(t, j, F, sc.op_slot);
+        no_free = no_free || F == NONE64;
+    }
+    if (no_free && (threadIdx.x & (T - 1)) == 0) ctl->serial[r & 1] = 1u;
+}
+
+// Phase 3 for op j on a tile: run the tile walk if j leads an unblocked
+// segment of a non-serial round; clear the registration.  Returns whether it ran.
+template <int KB, int VB, int T>
+__device__ __forceinline__ bool finish_tile(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t j,
+                                            bool serial, const OpScratch& sc, const Tile<T>& tl, uint64_t* s_pos,
+                                            uint32_t* s_p, ExecAcc& a) {
+    const bool run = !serial && sc.op_flag[j] != 0 && sc.op_word[j] > j;
+    if (run) exec_tile<KB, VB, T>(t, keys, vals, j, tl, s_pos, s_p, a);
+    tl.sync();
+    if (tl.lane == 0) {
+        const uint64_t F = sc.op_slot[j];
+        if (F != NONE64) {
+            t.seg_min[F] = IDLE;
+            t.seg_cnt[F] = 0;
+        }
+        sc.op_word[j] = IDLE;
+    }
+    return run;
+}
+
+template <int KB, int VB, int T>
+__global__ void __launch_bounds__(RBLOCK, 3) k_ins_p3t(TableView t, const uint8_t* __restrict__ keys,
+                                                       const uint8_t* __restrict__ vals, uint32_t n0, uint32_t r,
+                                                       OpScratch sc, Ctl* ctl) {
+    __shared__ uint64_t s_pos[RBLOCK / T][MAXCH];
+    __shared__ uint32_t s_p[RBLOCK / T][MAXCH];
+    __shared__ AppendSmem s_app;
+    __shared__ uint32_t s_tmp[RBLOCK / 32];
+    const RoundOps ops = round_ops(sc, ctl, r, n0);
+    const bool serial = *(volatile uint32_t*)&ctl->serial[r & 1] != 0;
+    uint32_t* out = pend_of(sc, r + 1);
+    uint32_t* out_n = &ctl->npend[(r + 1) & 1];
+    const Tile<T> tl;
+    const uint32_t tix = threadIdx.x / T;
+    const uint32_t ntiles = gridDim.x * (blockDim.x / T);
+    const uint32_t t0 = blockIdx.x * (blockDim.x / T) + tix;
+    const uint32_t iters = (ops.n + ntiles - 1) / ntiles;
+    ExecAcc a;
+    for (uint32_t it = 0; it < iters; it++) {
+        const uint32_t i = t0 + it * ntiles;
+        const bool valid = i < ops.n;
+        uint32_t j = 0;
+        bool ran = false;
+        if (valid) {
+            j = ops.op(i);
+            ran = finish_tile<KB, VB, T>(t, keys, vals, j, serial, sc, tl, s_pos[tix], s_p[tix], a);
+        }
+        block_append(out, out_n, j, valid && !ran && tl.lane == 0, s_app);
+    }
+    block_add_count(ctl, a.claimed, s_tmp);
+    publish_rare(ctl, a.maxd, a.tomb, a.limit);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && ops.n) atomicAdd(&ctl->rounds, 1u);
+}
+
+// ---- single-block tails ----------------------------------------------------
+//
+// One block runs every remaining round of the call (phases separated by block
+// barriers) when at most TAIL_MAX ops are pending, or returns at once.  A
+// serial round hands its ops to serial_process.  On completion both pending
+// counts are zero (the host's done marker).
+
+template <int KB, int VB, int T>
+__global__ void __launch_bounds__(TAIL_THREADS) k_ins_tail(TableView t, const uint8_t* __restrict__ keys,
+                                                           const uint8_t* __restrict__ vals, uint32_t n0,
+                                                           uint32_t r0, uint32_t nops, OpScratch sc, Ctl* ctl) {
+    constexpr int NT = T > 1 ? TAIL_THREADS / T : 1;
+    __shared__ uint32_t s_n, s_next, s_serial, s_err;
+    __shared__ uint64_t s_pos[NT][T > 1 ? MAXCH : 1];
+    __shared__ uint32_t s_p[NT][T > 1 ? MAXCH : 1];
+    __shared__ uint32_t s_buf[TAIL_THREADS];
+    __shared__ uint32_t s_woff[33];
+    if (threadIdx.x == 0) {
+        s_n = (r0 == 0) ? n0 : *(volatile uint32_t*)&ctl->npend[r0 & 1];
+        s_err = 0;
+    }
+    __syncthreads();
+    uint32_t n = s_n;
+    if (n == 0 || n > TAIL_MAX) return;
+    ExecAcc a;
+    uint32_t r = r0;
+    uint32_t rounds = 0;
+    // tiles (T > 1) or single threads (T == 1) as the unit of work
+    const uint32_t unit = T > 1 ? threadIdx.x / T : threadIdx.x;
+    const uint32_t nunits = T > 1 ? blockDim.x / T : blockDim.x;
+    const bool leader_lane = T > 1 ? (threadIdx.x & (T - 1)) == 0 : true;
+    for (;;) {
+        const uint32_t* in = (r == 0) ? nullptr : pend_of(sc, r);
+        uint32_t* out = pend_of(sc, r + 1);
+        if (threadIdx.x == 0) {
+            s_next = 0;
+            s_serial = 0;
+        }
+        __syncthreads();
+        for (uint32_t i = unit; i < n; i += nunits) {
+            const uint32_t j = in ? in[i] : i;
+            uint64_t F;
+            if constexpr (T > 1) {
+                const Tile<(T > 1 ? T : 8)> tl;
+                RegKey<KB> key;
+                key.load(keys + (uint64_t)j * KB, KB);
+                F = find_free_tile<(T > 1 ? T : 8)>(t, key.hash(KB, t.hash_mode) & t.mask, tl);
+            } else {
+                F = find_free<KB>(t, keys, j);
+            }
+            if (leader_lane) {
+                register_op(t, j, F, sc.op_slot);
+                if (F == NONE64) s_serial = 1u;
+            }
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint32_t bits = walk_op(t, in ? in[i] : i, nops, sc.op_slot, sc.op_word, sc.op_flag);
+            if (bits & 1u) s_serial = 1u;
+            if (bits & 2u) atomicOr(&s_err, ERR_SCRATCH);
+        }
+        __syncthreads();
+        const bool serial = s_serial != 0;
+        if (s_err) break;
+        if (serial) {
+            // clear the round's registrations, then apply its ops in index order
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+                const uint32_t j = in ? in[i] : i;
+                const uint64_t F = sc.op_slot[j];
+                if (F != NONE64) {
+                    t.seg_min[F] = IDLE;
+                    t.seg_cnt[F] = 0;
+                }
+                sc.op_word[j] = IDLE;
+            }
+            __syncthreads();
+            serial_process<KB, VB>(t, keys, vals, in, n, n0, sc, a, s_buf, s_woff);
+            ++rounds;
+            break;
+        }
+        for (uint32_t i = unit; i < n; i += nunits) {
+            const uint32_t j = in ? in[i] : i;
+            bool ran;
+            if constexpr (T > 1) {
+                const Tile<(T > 1 ? T : 8)> tl;
+                ran = finish_tile<KB, VB, (T > 1 ? T : 8)>(t, keys, vals, j, false, sc, tl, s_pos[unit], s_p[unit], a);
+            } else {
+                ran = finish_op<KB, VB>(t, keys, vals, j, false, sc, a);
+            }
+            if (!ran && leader_lane) out[atomicAdd(&s_next, 1u)] = j;
+        }
+        __syncthreads();
+        const uint32_t nn = s_next;
+        ++r;
+        ++rounds;
+        if (nn == 0) break;
+        if (nn >= n) {  // every non-serial round runs its smallest op
+            if (threadIdx.x == 0) atomicOr(&s_err, ERR_NO_PROGRESS);
+            break;
+        }
+        n = nn;
+        __syncthreads();  // everyone has read s_next before it is reset
+    }
+    __syncthreads();
+    if (a.claimed) atomicAdd(&ctl->count, (unsigned long long)a.claimed);
+    if (a.maxd > *(volatile uint32_t*)&ctl->dmax) atomicMax(&ctl->dmax, a.maxd);
+    if (a.tomb) ctl->tomb_claimed = 1u;
+    if (a.limit) atomicOr(&ctl->err, ERR_WALK_LIMIT);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_err) {
+            atomicOr(&ctl->err, s_err);
+        } else {
+            ctl->npend[r0 & 1] = 0;  // done marker read by the host
+            ctl->npend[(r0 + 1) & 1] = 0;
+        }
+        atomicAdd(&ctl->rounds, rounds);
+    }
+}
+
+// Host-launched fallback for a serial round whose pending count is above
+// TAIL_MAX: applies round r's ops in index order.
+template <int KB, int VB>
+__global__ void __launch_bounds__(1024) k_ins_serial(TableView t, const uint8_t* __restrict__ keys,
+                                                     const uint8_t* __restrict__ vals, uint32_t n0, uint32_t r,
+                                                     OpScratch sc, Ctl* ctl) {
+    __shared__ uint32_t s_buf[1024];
+    __shared__ uint32_t s_woff[33];
+    const RoundOps ops = round_ops(sc, ctl, r, n0);
+    ExecAcc a;
+    serial_process<KB, VB>(t, keys, vals, ops.list, ops.n, n0, sc, a, s_buf, s_woff);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (a.claimed) atomicAdd(&ctl->count, (unsigned long long)a.claimed);
+        if (a.maxd > ctl->dmax) ctl->dmax = a.maxd;
+        if (a.tomb) ctl->tomb_claimed = 1u;
+        if (a.limit) atomicOr(&ctl->err, ERR_WALK_LIMIT);
+        ctl->npend[r & 1] = 0;
+        ctl->npend[(r + 1) & 1] = 0;
+        atomicAdd(&ctl->rounds, 1u);
+    }
+}
+
+constexpr int INS_T = 8;  // lanes per insert in the tile kernels
+
+template <int KB, int VB>
+void rounds_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, uint32_t r0,
+                  uint32_t nrounds, uint32_t grid_ops, uint32_t nops, const OpScratch& sc, Ctl* ctl,
+                  cudaStream_t s) {
+    for (uint32_t r = r0; r < r0 + nrounds; r++) {
+        if constexpr (KB != 0 && VB != 0) {
+            const unsigned gt = grid_for((uint64_t)grid_ops * INS_T, 8);
+            const unsigned g = grid_for(grid_ops, 8);
+            k_ins_p1t<KB, INS_T><<<gt, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
+            k_ins_p2<<<g, RBLOCK, 0, s>>>(t, n0, r, nops, sc, ctl);
+            k_ins_p3t<KB, VB, INS_T><<<gt, RBLOCK, 0, s>>>(t, keys, vals, n0, r, sc, ctl);
+        } else {
+            const unsigned g = grid_for(grid_ops, 8);
+            k_ins_p1<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
+            k_ins_p2<<<g, RBLOCK, 0, s>>>(t, n0, r, nops, sc, ctl);
+            k_ins_p3<KB, VB><<<g, RBLOCK, 0, s>>>(t, keys, vals, n0, r, sc, ctl);
+        }
+    }
+    count_launches(3 * nrounds);
+}
+
+template <int KB, int VB>
+void tail_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, uint32_t r,
+                uint32_t nops, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+    constexpr int T = (KB != 0 && VB != 0) ? INS_T : 1;
+    k_ins_tail<KB, VB, T><<<1, TAIL_THREADS, 0, s>>>(t, keys, vals, n0, r, nops, sc, ctl);
+    count_launches(1);
+}
+
+template <int KB, int VB>
+void serial_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, uint32_t r,
+                  const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+    k_ins_serial<KB, VB><<<1, 1024, 0, s>>>(t, keys, vals, n0, r, sc, ctl);
+    count_launches(1);
+}
+
+}  // namespace
+
+#define FM_SHAPE_SWITCH(sh, CALL)                 \
+    switch (sh) {                                 \
+        case SHAPE_8_8: CALL(8, 8); break;        \
+        case SHAPE_32_128: CALL(32, 128); break;  \
+        case SHAPE_32_64: CALL(32, 64); break;    \
+        case SHAPE_32_32: CALL(32, 32); break;    \
+        case SHAPE_8_32: CALL(8, 32); break;      \
+        default: CALL(0, 0); break;               \
+    }
+
+cudaError_t launch_ins_rounds(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
+                              uint32_t r0, uint32_t nrounds, uint32_t grid_ops, const OpScratch& sc, Ctl* ctl,
+                              cudaStream_t s) {
+#define FM_CALL(K, V) rounds_shape<K, V>(t, keys, vals, n0, r0, nrounds, grid_ops, n0, sc, ctl, s)
+    FM_SHAPE_SWITCH(sh, FM_CALL)
+#undef FM_CALL
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ins_tail(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
+                            uint32_t r, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+#define FM_CALL(K, V) tail_shape<K, V>(t, keys, vals, n0, r, n0, sc, ctl, s)
+    FM_SHAPE_SWITCH(sh, FM_CALL)
+#undef FM_CALL
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ins_serial(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
+                              uint32_t r, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+#define FM_CALL(K, V) serial_shape<K, V>(t, keys, vals, n0, r, sc, ctl, s)
+    FM_SHAPE_SWITCH(sh, FM_CALL)
+#undef FM_CALL
+    return cudaGetLastError();
+}
+
+}  // namespace fm

@@ -1,6 +1,8 @@
 // fm_internal.h -- host-side interface between the C ABI layer (fm_capi.cu)
-// and the kernel launchers (fm_kernels.cu).  Not part of the public ABI.
+// and the kernel launchers (fm_get.cu, fm_insert.cu, fm_remove.cu).  Not part
+// of the public ABI.
 #pragma once
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -8,30 +10,47 @@
 
 namespace fm {
 
-// Per-call control block in device memory (one per table, reused by every
-// mutating call, which are exclusive per table).
+// Control block in device memory, one per table, reused by every mutating
+// call (mutating calls are exclusive per table).  Round r reads its pending
+// count from npend[r & 1] (round 0: the call size) and its op list from
+// OpScratch::pend[r & 1] (round 0: the identity), and appends the ops that
+// did not run to pend[(r + 1) & 1].  The first CTL_CALL_BYTES bytes are
+// zeroed at the start of every call.
+// Counters that every block of a grid adds to are spread over COUNT_PARTS
+// slots, each in its own 32-byte sector, so the atomics do not queue on one
+// address; the host sums them.
+constexpr int COUNT_PARTS = 32;
+
 struct Ctl {
-    uint32_t npend_next;     // ops still pending after this round
-    uint32_t gmin;           // smallest pending op index (serial mode)
-    uint32_t serial;         // 1: this round runs only the smallest pending op
+    uint32_t npend[2];       // pending ops per round parity
+    uint32_t serial[2];      // 1: a round found no free slot / a flow wrapping the table
     uint32_t err;            // device-side error bits
-    unsigned long long count;  // new keys (insert) / removed keys (remove)
+    uint32_t rounds;         // rounds run by the call (statistics)
+    unsigned long long count;  // new keys (insert) / removed keys (remove), single-block kernels
+    unsigned long long count_part[COUNT_PARTS][4];  // the same from grid kernels, [i][0] used
     // Persistent table facts (survive across calls, reset by clear):
     uint32_t dmax;           // largest probe distance ever stored since clear
     uint32_t tomb_claimed;   // 1 once an insert reused a tombstone since clear
     unsigned long long occupied;  // recount result
+    unsigned long long total_count() const {
+        unsigned long long s = count;
+        for (int i = 0; i < COUNT_PARTS; i++) s += count_part[i][0];
+        return s;
+    }
 };
+constexpr size_t CTL_CALL_BYTES = 32 + 32 * COUNT_PARTS;  // npend .. count_part
+static_assert(offsetof(Ctl, dmax) == CTL_CALL_BYTES, "Ctl layout");
 
 // Device-side error bits (Ctl::err).
-constexpr uint32_t ERR_WALK_LIMIT = 1u;  // an insert walk passed 2*capacity+2 slots (full table)
-constexpr uint32_t ERR_SCRATCH = 2u;     // a segment registration did not belong to this call
+constexpr uint32_t ERR_WALK_LIMIT = 1u;   // an insert walk passed 2*capacity+2 slots (full table)
+constexpr uint32_t ERR_SCRATCH = 2u;      // a segment registration did not belong to this call
+constexpr uint32_t ERR_NO_PROGRESS = 4u;  // a tail round ran no op (never expected)
 
 // Per-op scratch for the round-based insert and remove (op index space).
 struct OpScratch {
-    uint32_t* pend_a;    // pending op indices (this round)
-    uint32_t* pend_b;    // pending op indices (next round)
+    uint32_t* pend[2];   // pending op indices, by round parity
     uint64_t* op_slot;   // insert: terminating free slot F; remove: target slot
-    uint32_t* op_word;   // insert: inflow lower bound; remove: window length
+    uint32_t* op_word;   // insert: inflow lower bound; remove: window length (idle 0xFFFFFFFF)
     uint8_t* op_flag;    // insert: leader bit; remove: potential-target count
     uint32_t* op_pt;     // remove: up to PT_MAX potential-target distances per op
     uint64_t cap_ops;
@@ -42,18 +61,35 @@ enum Shape { SHAPE_8_8 = 0, SHAPE_32_128, SHAPE_32_64, SHAPE_32_32, SHAPE_8_32, 
 Shape pick_shape(uint32_t ksz, uint32_t vsz);
 constexpr uint32_t GENERIC_MAX_KV = 256;  // byte limit of the run-time-size path (kernels.cu:32)
 
+// Single-CTA tail: rounds with at most this many pending ops run inside one
+// block with block-level barriers between phases.
+constexpr uint32_t TAIL_MAX = 256;
+constexpr int TAIL_THREADS = 512;
+
 // Launchers.  All are stream-ordered and return the launch error.
 cudaError_t launch_get(const TableView& t, Shape sh, const uint8_t* qkeys, uint64_t n, uint8_t* out_vals,
                        uint8_t* out_found, cudaStream_t s);
-cudaError_t launch_iota(uint32_t* p, uint64_t n, cudaStream_t s);
-cudaError_t launch_ins_round(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals,
-                             const uint32_t* pend, uint32_t npend, uint32_t nops, uint32_t* pend_next,
-                             const OpScratch& sc, Ctl* ctl, cudaStream_t s);
-cudaError_t launch_rem_round(const TableView& t, Shape sh, const uint8_t* keys, const uint32_t* pend,
-                             uint32_t npend, uint32_t* pend_next, const OpScratch& sc, Ctl* ctl,
-                             cudaStream_t s);
+// Grid-wide rounds r0 .. r0+nrounds-1 of an insert call of n0 ops; `grid_ops`
+// bounds the pending count of every launched round (sizes the grids).
+cudaError_t launch_ins_rounds(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
+                              uint32_t r0, uint32_t nrounds, uint32_t grid_ops, const OpScratch& sc, Ctl* ctl,
+                              cudaStream_t s);
+// Runs every remaining round starting at r in one block if the pending count
+// is at most TAIL_MAX; otherwise returns without touching anything.
+cudaError_t launch_ins_tail(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
+                            uint32_t r, const OpScratch& sc, Ctl* ctl, cudaStream_t s);
+// Applies round r's pending ops one at a time in index order (a round that
+// found the table full, with more than TAIL_MAX ops pending).
+cudaError_t launch_ins_serial(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
+                              uint32_t r, const OpScratch& sc, Ctl* ctl, cudaStream_t s);
+cudaError_t launch_rem_rounds(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, uint32_t r0,
+                              uint32_t nrounds, uint32_t grid_ops, const OpScratch& sc, Ctl* ctl, cudaStream_t s);
+cudaError_t launch_rem_tail(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, uint32_t r,
+                            const OpScratch& sc, Ctl* ctl, cudaStream_t s);
 cudaError_t launch_count(const TableView& t, Ctl* ctl, cudaStream_t s);
 int num_sms();
 unsigned long long launch_count();
+void count_launches(unsigned n);
+unsigned grid_for(uint64_t threads, unsigned per_sm);
 
 }  // namespace fm

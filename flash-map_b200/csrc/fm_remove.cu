@@ -1,0 +1,262 @@
+// fm_remove.cu -- deterministic bulk remove for sm_100a.
+//
+// Semantics: the reference's sequential remove (src/rayon_cpu.rs:273-328;
+// the probe of src/kernels.cu:565-644 run one key at a time) in batch index
+// order: the first OCCUPIED slot holding the key before the first EMPTY slot
+// or Robin Hood exit (p > dist) becomes the whole word TOMBSTONE (dist 0).
+//
+// Why rounds: removes of different keys interact only through slots one of
+// them tombstones.  Every pending op marks each slot that holds its key
+// within [home, min(first EMPTY - 1, X + dmax)] (X = its current target, or
+// home on a miss; dmax bounds every stored distance, so no copy of a key lies
+// further) with its index.  An op runs in a round unless an earlier pending
+// op marked a slot of its own window (the same range), which covers both
+// directions of interference: an earlier op's tombstone changing this op's
+// probe, and this op's tombstone letting an earlier op's probe run on past a
+// former terminator.  The lowest pending op is never blocked.
+//
+// Control: as fm_insert.cu (two grid rounds, then a single-block tail).
+#include "fm_rounds.cuh"
+
+namespace fm {
+namespace {
+
+template <int KB>
+__device__ __forceinline__ uint64_t home_of(const TableView& t, const uint8_t* keys, uint32_t j, RegKey<KB>& key) {
+    const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
+    key.load(keys + (uint64_t)j * ksz, ksz);
+    return key.hash(ksz, t.hash_mode) & t.mask;
+}
+
+// Phase 1 for op j: probe, then mark every possible target.
+template <int KB>
+__device__ __forceinline__ void scan_op(const TableView& t, const uint8_t* keys, uint32_t j, uint64_t dmax,
+                                        const OpScratch& sc) {
+    const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
+    const uint64_t mask = t.mask;
+    RegKey<KB> key;
+    const uint64_t h = home_of<KB>(t, keys, j, key);
+    uint64_t tp = NONE64;  // probe depth of the current target
+    uint64_t p = 0;
+    bool empty_hit = false;
+    for (; p <= mask; ++p) {
+        const uint64_t s = (h + p) & mask;
+        const uint32_t f = t.flags[s];
+        const uint32_t st = st_of(f);
+        if (st == ST_EMPTY) {
+            empty_hit = true;
+            break;
+        }
+        if (st == ST_OCC) {
+            if (p > dist_of(f)) break;  // Robin Hood exit (rayon_cpu.rs:298-302)
+            if (dist_matches(f, p) && key.eq(t.keys + s * ksz, ksz)) {
+                tp = p;
+                break;
+            }
+        }
+    }
+    uint64_t lim = (tp != NONE64 ? tp : 0) + dmax;
+    if (lim > mask) lim = mask;
+    uint32_t npt = 0;
+    uint64_t wend;
+    auto mark = [&](uint64_t q) {
+        atomicMin(&t.seg_min[(h + q) & mask], j);
+        if (npt < PT_MAX) sc.op_pt[(uint64_t)j * PT_MAX + npt] = (uint32_t)q;
+        ++npt;
+    };
+    if (empty_hit) {
+        wend = p == 0 ? NONE64 : min(p - 1, lim);  // home slot EMPTY: nothing to watch
+    } else {
+        if (tp != NONE64) mark(tp);
+        wend = min(p, lim);
+        for (uint64_t q = (tp != NONE64 ? tp : p) + 1; q <= lim; ++q) {
+            const uint64_t s = (h + q) & mask;
+            const uint32_t f = t.flags[s];
+            const uint32_t st = st_of(f);
+            if (st == ST_EMPTY) break;
+            wend = q;
+            if (st == ST_OCC && dist_matches(f, q) && key.eq(t.keys + s * ksz, ksz)) mark(q);
+        }
+    }
+    sc.op_slot[j] = tp != NONE64 ? ((h + tp) & mask) : NONE64;
+    sc.op_word[j] = wend == NONE64 ? IDLE : (uint32_t)wend;
+    sc.op_flag[j] = (uint8_t)min(npt, 255u);
+}
+
+// Phase 2 for op j: run unless an earlier op marked its window.
+template <int KB>
+__device__ __forceinline__ bool check_op(const TableView& t, const uint8_t* keys, uint32_t j, const OpScratch& sc,
+                                         uint32_t& removed) {
+    const uint64_t mask = t.mask;
+    const uint32_t wend = sc.op_word[j];
+    if (wend != IDLE) {
+        RegKey<KB> key;
+        const uint64_t h = home_of<KB>(t, keys, j, key);
+        for (uint64_t q = 0; q <= wend; ++q)
+            if (t.seg_min[(h + q) & mask] < j) return false;
+    }
+    const uint64_t ts = sc.op_slot[j];
+    if (ts != NONE64) {
+        t.flags[ts] = ST_TOMB;  // whole word 2: TOMBSTONE, dist 0 (rayon_cpu.rs:306-313)
+        ++removed;
+    }
+    return true;
+}
+
+// Phase 3 for op j: clear its marks and its window word.
+template <int KB>
+__device__ __forceinline__ void reset_op(const TableView& t, const uint8_t* keys, uint32_t j, const OpScratch& sc) {
+    const uint64_t mask = t.mask;
+    const uint32_t npt = sc.op_flag[j];
+    const uint32_t wend = sc.op_word[j];
+    sc.op_word[j] = IDLE;  // the word is the insert's inflow bound between calls
+    if (npt == 0) return;
+    RegKey<KB> key;
+    const uint64_t h = home_of<KB>(t, keys, j, key);
+    if (npt <= PT_MAX) {
+        for (uint32_t k = 0; k < npt; k++) t.seg_min[(h + sc.op_pt[(uint64_t)j * PT_MAX + k]) & mask] = IDLE;
+    } else {
+        for (uint64_t q = 0; q <= wend; ++q) {
+            const uint64_t s = (h + q) & mask;
+            if (t.seg_min[s] != IDLE) t.seg_min[s] = IDLE;
+        }
+    }
+}
+
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_rem_p1(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
+                                                   uint32_t r, OpScratch sc, Ctl* ctl) {
+    const RoundOps ops = round_ops(sc, ctl, r, n0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) reset_next_round(ctl, r);
+    const uint64_t dmax = *(volatile uint32_t*)&ctl->dmax;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ops.n; i += gridDim.x * blockDim.x)
+        scan_op<KB>(t, keys, ops.op(i), dmax, sc);
+}
+
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_rem_p2(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
+                                                   uint32_t r, OpScratch sc, Ctl* ctl) {
+    __shared__ AppendSmem s_app;
+    __shared__ uint32_t s_tmp[RBLOCK / 32];
+    const RoundOps ops = round_ops(sc, ctl, r, n0);
+    uint32_t* out = pend_of(sc, r + 1);
+    uint32_t* out_n = &ctl->npend[(r + 1) & 1];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t iters = grid_iters(ops.n);
+    uint32_t removed = 0;
+    for (uint32_t it = 0; it < iters; it++) {
+        const uint32_t i = i0 + it * stride;
+        const bool valid = i < ops.n;
+        uint32_t j = 0;
+        bool ran = false;
+        if (valid) {
+            j = ops.op(i);
+            ran = check_op<KB>(t, keys, j, sc, removed);
+        }
+        block_append(out, out_n, j, valid && !ran, s_app);
+    }
+    block_add_count(ctl, removed, s_tmp);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && ops.n) atomicAdd(&ctl->rounds, 1u);
+}
+
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_rem_p3(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
+                                                   uint32_t r, OpScratch sc, Ctl* ctl) {
+    const RoundOps ops = round_ops(sc, ctl, r, n0);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ops.n; i += gridDim.x * blockDim.x)
+        reset_op<KB>(t, keys, ops.op(i), sc);
+}
+
+template <int KB>
+__global__ void __launch_bounds__(TAIL_THREADS) k_rem_tail(TableView t, const uint8_t* __restrict__ keys,
+                                                           uint32_t n0, uint32_t r0, OpScratch sc, Ctl* ctl) {
+    __shared__ uint32_t s_n, s_next;
+    if (threadIdx.x == 0) s_n = (r0 == 0) ? n0 : *(volatile uint32_t*)&ctl->npend[r0 & 1];
+    __syncthreads();
+    uint32_t n = s_n;
+    if (n == 0 || n > TAIL_MAX) return;
+    const uint64_t dmax = *(volatile uint32_t*)&ctl->dmax;
+    uint32_t removed = 0, rounds = 0;
+    uint32_t r = r0;
+    bool stuck = false;
+    for (;;) {
+        const uint32_t* in = (r == 0) ? nullptr : pend_of(sc, r);
+        uint32_t* out = pend_of(sc, r + 1);
+        if (threadIdx.x == 0) s_next = 0;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) scan_op<KB>(t, keys, in ? in[i] : i, dmax, sc);
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const uint32_t j = in ? in[i] : i;
+            if (!check_op<KB>(t, keys, j, sc, removed)) out[atomicAdd(&s_next, 1u)] = j;
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) reset_op<KB>(t, keys, in ? in[i] : i, sc);
+        __syncthreads();
+        const uint32_t nn = s_next;
+        ++r;
+        ++rounds;
+        if (nn == 0) break;
+        if (nn >= n) {
+            stuck = true;
+            break;
+        }
+        n = nn;
+        __syncthreads();
+    }
+    if (removed) atomicAdd(&ctl->count, (unsigned long long)removed);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (stuck) {
+            atomicOr(&ctl->err, ERR_NO_PROGRESS);
+        } else {
+            ctl->npend[r0 & 1] = 0;
+            ctl->npend[(r0 + 1) & 1] = 0;
+        }
+        atomicAdd(&ctl->rounds, rounds);
+    }
+}
+
+template <int KB>
+void rounds_shape(const TableView& t, const uint8_t* keys, uint32_t n0, uint32_t r0, uint32_t nrounds,
+                  uint32_t grid_ops, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+    const unsigned g = grid_for(grid_ops, 8);
+    for (uint32_t r = r0; r < r0 + nrounds; r++) {
+        k_rem_p1<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
+        k_rem_p2<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
+        k_rem_p3<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
+    }
+    count_launches(3 * nrounds);
+}
+
+}  // namespace
+
+cudaError_t launch_rem_rounds(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, uint32_t r0,
+                              uint32_t nrounds, uint32_t grid_ops, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+    switch (sh) {
+        case SHAPE_8_8:
+        case SHAPE_8_32: rounds_shape<8>(t, keys, n0, r0, nrounds, grid_ops, sc, ctl, s); break;
+        case SHAPE_32_128:
+        case SHAPE_32_64:
+        case SHAPE_32_32: rounds_shape<32>(t, keys, n0, r0, nrounds, grid_ops, sc, ctl, s); break;
+        default: rounds_shape<0>(t, keys, n0, r0, nrounds, grid_ops, sc, ctl, s); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rem_tail(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, uint32_t r,
+                            const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+    switch (sh) {
+        case SHAPE_8_8:
+        case SHAPE_8_32: k_rem_tail<8><<<1, TAIL_THREADS, 0, s>>>(t, keys, n0, r, sc, ctl); break;
+        case SHAPE_32_128:
+        case SHAPE_32_64:
+        case SHAPE_32_32: k_rem_tail<32><<<1, TAIL_THREADS, 0, s>>>(t, keys, n0, r, sc, ctl); break;
+        default: k_rem_tail<0><<<1, TAIL_THREADS, 0, s>>>(t, keys, n0, r, sc, ctl); break;
+    }
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace fm

@@ -316,3 +316,68 @@ def test_skewed_duplicate_heavy_scaled():
         rm = present[rng.integers(0, len(present), 3000)]
         assert g.bulk_remove(rm) == o.bulk_remove(rm)
     assert_same_layout(g, o)
+
+
+@pytest.mark.parametrize("shape", [(8, 8), (32, 128)])
+@pytest.mark.parametrize("chain", [5, 30, 47, 48, 49, 70])
+def test_long_eviction_chains(shape, chain):
+    """An insert whose Robin Hood walk evicts `chain` entries in a row (homes
+    1..chain each at dist 0 behind a home-0 entry): exercises chains spanning
+    several metadata windows and the scalar walk past the per-tile chain
+    buffer."""
+    ks, vs = shape
+    cap = 256
+    g = gpu_map(cap, ks, vs)
+    o = OracleAdapter(cap, ks, vs)
+    homes = np.arange(0, chain + 1, dtype=np.uint64)
+    keys = le(homes, ks)
+    vals = le(homes * 3 + 1, vs)
+    assert g.bulk_insert(keys, vals) == o.bulk_insert(keys, vals)
+    k2 = le([np.uint64(cap)], ks)  # home 0 again: evicts homes 1..chain
+    v2 = le([np.uint64(999)], vs)
+    assert g.bulk_insert(k2, v2) == o.bulk_insert(k2, v2) == 1
+    assert_same_layout(g, o)
+    # the same as several ops in one batch (segments merge as free slots fill)
+    g2 = gpu_map(cap, ks, vs)
+    o2 = OracleAdapter(cap, ks, vs)
+    batch = np.concatenate([keys, le(np.arange(1, 6, dtype=np.uint64) * cap, ks)])
+    bv = le(np.arange(len(batch), dtype=np.uint64), vs)
+    assert g2.bulk_insert(batch, bv) == o2.bulk_insert(batch, bv)
+    assert_same_layout(g2, o2)
+
+
+@pytest.mark.parametrize("extra_n", [100, 300])
+def test_overfull_table_serial_path(extra_n):
+    """Uncounted inserts into a completely full table: every round finds no
+    free slot, so the ops run one at a time in index order (inside the tail
+    block for small counts, in the host-launched sequential kernel above the
+    tail limit).  Layout, len and the limit report match the oracle."""
+    import torch
+
+    import flash_map as F
+    import oracle as O
+
+    cap = 512
+    rng = np.random.default_rng(extra_n)
+    g = gpu_map(cap, 8, 8)
+    o = OracleAdapter(cap, 8, 8)
+    k = le(rng.permutation(np.arange(cap, dtype=np.uint64) * 7 + 3))
+    assert g.bulk_insert(k, k) == o.bulk_insert(k, k) == cap
+    extra = le(rng.integers(0, 1 << 40, extra_n).astype(np.uint64))
+    o_limit = False
+    try:
+        o.bulk_insert_uncounted(extra, extra)
+    except O.ProbeLimit:
+        o_limit = True
+    dk = torch.from_numpy(extra.copy()).cuda()
+    g_limit = False
+    try:
+        g.bulk_insert_device_uncounted(dk, dk, extra_n)
+    except F.KernelLaunch as e:
+        assert "2*capacity" in str(e)
+        g_limit = True
+    torch.cuda.synchronize()
+    assert g_limit == o_limit
+    assert g.len() == o.len() == cap + extra_n
+    assert_same_layout(g, o)
+    assert g.recount() == o.recount()
