@@ -579,3 +579,153 @@ int fm_load(fm_table* t, const uint32_t* flags, const void* keys, const void* va
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free insert (no counterpart in the reference).
+//
+// Some callers cannot allocate GPU memory at the point where they insert: a
+// pipeline stage inside a captured or long-lived stream, a process that runs
+// with its device memory pre-reserved under a fixed budget, or code running
+// from a CUDA host callback, where cudaMalloc is not allowed.  For them,
+// fm_bulk_insert_device_noalloc runs the same insert kernels as
+// fm_bulk_insert_device, but every per-call buffer (round control block,
+// pending lists, per-op words) comes from the file-scope device array below,
+// sized for FM_NOALLOC_MAX_OPS operations (about 2.5 MB, held by every GPU
+// that loads the library until the process exits).
+//
+// The first call on a device sets the array up (looks up its device address
+// and marks the per-op words idle) and synchronizes; make that first call
+// before any stream capture.  Later calls only launch kernels and copy small
+// control words.  All calls share the one array: calls whose GPU work
+// overlaps -- on any table of the same device -- race on it, so serialize them
+// (one stream, or an event between calls).
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t na_align(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr uint64_t NA_OPS = FM_NOALLOC_MAX_OPS;
+constexpr size_t NA_CTL = 0;
+constexpr size_t NA_PEND0 = na_align(sizeof(Ctl));
+constexpr size_t NA_PEND1 = NA_PEND0 + na_align(NA_OPS * 4);
+constexpr size_t NA_SLOT = NA_PEND1 + na_align(NA_OPS * 4);
+constexpr size_t NA_WORD = NA_SLOT + na_align(NA_OPS * 8);
+constexpr size_t NA_PT = NA_WORD + na_align(NA_OPS * 4);
+constexpr size_t NA_FLAG = NA_PT + na_align(NA_OPS * 4 * fm::PT_MAX);
+constexpr size_t NA_BYTES = NA_FLAG + na_align(NA_OPS);
+
+}  // namespace
+
+// The scratch of fm_bulk_insert_device_noalloc.  In host code this name is
+// not a device address; na_setup() looks the address up per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+namespace {
+
+constexpr int NA_MAX_DEVICES = 64;
+std::mutex na_mu;
+uint8_t* na_base[NA_MAX_DEVICES] = {};
+
+// Once per device, with that device current: the array's device address, and
+// the per-op words set idle (the insert kernels leave them idle after use).
+int na_setup(int dev, uint8_t** out) {
+    if (dev < 0 || dev >= NA_MAX_DEVICES) return fail(FM_ERR_INVALID_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> g(na_mu);
+    if (!na_base[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(FM_ERR_CUDA_INIT, "cudaGetSymbolAddress(noalloc scratch)", e);
+        e = cudaMemset((uint8_t*)p + NA_WORD, 0xFF, NA_OPS * 4);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) return cuda_fail(FM_ERR_CUDA_INIT, "noalloc scratch init", e);
+        na_base[dev] = (uint8_t*)p;
+    }
+    *out = na_base[dev];
+    return FM_OK;
+}
+
+int noalloc_rounds(fm_table* t, const uint8_t* d_k, const uint8_t* d_v, uint32_t m, cudaStream_t s, uint8_t* base,
+                   uint64_t* out_count, bool* limit) {
+    Ctl* ctl = (Ctl*)(base + NA_CTL);
+    OpScratch sc{};
+    sc.pend[0] = (uint32_t*)(base + NA_PEND0);
+    sc.pend[1] = (uint32_t*)(base + NA_PEND1);
+    sc.op_slot = (uint64_t*)(base + NA_SLOT);
+    sc.op_word = (uint32_t*)(base + NA_WORD);
+    sc.op_pt = (uint32_t*)(base + NA_PT);
+    sc.op_flag = base + NA_FLAG;
+    sc.cap_ops = NA_OPS;
+    const fm::Shape sh = t->shape_for({d_k, d_v});
+    const fm::TableView v = t->view();
+    // per-call fields start at zero; the table's persistent facts (largest
+    // stored distance, tombstone reuse) travel in and back out
+    cudaError_t e = cudaMemsetAsync(ctl, 0, fm::CTL_CALL_BYTES, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&ctl->dmax, &t->d_ctl->dmax, 8, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "noalloc setup", e);
+    uint32_t r = 0, left = m;
+    for (;;) {
+        e = fm::launch_ins_rounds(v, sh, d_k, d_v, m, r, 2, left, sc, ctl, s);
+        r += 2;
+        if (e == cudaSuccess) e = fm::launch_ins_tail(v, sh, d_k, d_v, m, r, sc, ctl, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(t->h_ctl, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "noalloc insert rounds", e);
+        if (t->h_ctl->err & fm::ERR_SCRATCH) return fail(FM_ERR_KERNEL_LAUNCH, "stale segment registration");
+        if (t->h_ctl->err & fm::ERR_NO_PROGRESS) return fail(FM_ERR_PROBE_LIMIT, "round made no progress");
+        uint32_t now = t->h_ctl->npend[r & 1];
+        if (now > 0 && t->h_ctl->serial[(r - 1) & 1]) {
+            e = fm::launch_ins_serial(v, sh, d_k, d_v, m, r, sc, ctl, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(t->h_ctl, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "noalloc serial insert", e);
+            now = t->h_ctl->npend[r & 1];
+        }
+        if (now == 0) break;
+        if (now >= left) return fail(FM_ERR_PROBE_LIMIT, "round made no progress");
+        left = now;
+    }
+    e = cudaMemcpyAsync(&t->d_ctl->dmax, &ctl->dmax, 8, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "noalloc finish", e);
+    *out_count = t->h_ctl->total_count();
+    *limit = (t->h_ctl->err & fm::ERR_WALK_LIMIT) != 0;
+    return FM_OK;
+}
+
+}  // namespace
+
+extern "C" int fm_bulk_insert_device_noalloc(fm_table* t, const void* d_keys, const void* d_values, uint64_t n,
+                                             uint64_t* num_new, void* stream) {
+    if (!t || !num_new) return fail(FM_ERR_INVALID_ARG, "NULL argument");
+    *num_new = 0;
+    if (n == 0) return FM_OK;
+    if (n > NA_OPS) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "fm_bulk_insert_device_noalloc: %llu ops exceed FM_NOALLOC_MAX_OPS (%llu); "
+                 "split the batch or use fm_bulk_insert_device", (unsigned long long)n, (unsigned long long)NA_OPS);
+        return fail(FM_ERR_INVALID_ARG, buf);
+    }
+    if (!d_keys || (!d_values && t->vsz)) return fail(FM_ERR_INVALID_ARG, "NULL buffer");
+    std::lock_guard<std::mutex> g(t->mu);
+    int rc = precheck(t, n);
+    if (rc) return rc;
+    DeviceGuard dg(t->device);
+    uint8_t* base = nullptr;
+    rc = na_setup(t->device, &base);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    uint64_t added = 0;
+    bool limit = false;
+    rc = noalloc_rounds(t, (const uint8_t*)d_keys, (const uint8_t*)d_values, (uint32_t)n, s, base, &added, &limit);
+    if (rc) {
+        const std::string msg = tl_err;
+        cudaMemsetAsync(t->d_seg_min, 0xFF, t->cap * 4, s);
+        cudaMemsetAsync(t->d_seg_cnt, 0, t->cap * 4, s);
+        cudaMemsetAsync(base + NA_WORD, 0xFF, NA_OPS * 4, s);
+        cudaStreamSynchronize(s);
+        tl_err = msg;
+        return rc;
+    }
+    t->len += added;
+    *num_new = added;
+    return limit ? limit_error() : FM_OK;
+}

@@ -21,6 +21,7 @@ EXPORTS = (
     "fm_capacity", "fm_load_factor", "fm_clear", "fm_device", "fm_bulk_get_device",
     "fm_bulk_get_values_device", "fm_bulk_insert_device", "fm_bulk_insert_device_uncounted",
     "fm_bulk_remove_device", "fm_recount", "fm_last_error", "fm_launch_count", "fm_snapshot", "fm_load",
+    "fm_bulk_insert_device_noalloc",
 )
 
 _lock = threading.Lock()
@@ -60,6 +61,8 @@ def _declare(L) -> None:
     L.fm_bulk_insert_device_uncounted.argtypes = [vp, vp, vp, u64, vp]
     L.fm_bulk_remove_device.restype = i32
     L.fm_bulk_remove_device.argtypes = [vp, vp, u64, u64p, vp]
+    L.fm_bulk_insert_device_noalloc.restype = i32
+    L.fm_bulk_insert_device_noalloc.argtypes = [vp, vp, vp, u64, u64p, vp]
     L.fm_recount.restype = i32
     L.fm_recount.argtypes = [vp, u64p]
     L.fm_launch_count.restype = u64

@@ -113,6 +113,21 @@ int fm_bulk_insert_device_uncounted(fm_table* t, const void* d_keys, const void*
 int fm_bulk_remove_device(fm_table* t, const void* d_keys, uint64_t n, uint64_t* num_removed,
                           void* stream);
 
+/* Allocation-free insert.  No counterpart in the reference: an addition for
+ * callers that cannot allocate GPU memory when they insert (work issued from
+ * a CUDA host callback, where cudaMalloc is not allowed; a pipeline stage on
+ * a long-lived stream; a process whose device memory is reserved up front).
+ * Same semantics and arguments as fm_bulk_insert_device, but it calls no
+ * cudaMalloc/cudaFree: its per-call scratch is a fixed device array inside
+ * the library, so a call takes at most FM_NOALLOC_MAX_OPS keys (larger
+ * batches fail with FM_ERR_INVALID_ARG; split them).  The first call on a
+ * device sets that array up and synchronizes -- make it before any stream
+ * capture.  All calls share the array: calls whose GPU work overlaps (on any
+ * table of the same device) race, so keep them ordered on one stream. */
+#define FM_NOALLOC_MAX_OPS 65536u
+int fm_bulk_insert_device_noalloc(fm_table* t, const void* d_keys, const void* d_values, uint64_t n,
+                                  uint64_t* num_new, void* stream);
+
 /* GpuFlashMap::recount (gpu.rs:677-712): counts OCCUPIED slots, len := count. */
 int fm_recount(fm_table* t, uint64_t* out);
 
