@@ -121,9 +121,9 @@ namespace {
 int ensure_scratch(fm_table* t, uint64_t n) {
     if (t->sc.cap_ops >= n) return FM_OK;
     // pend[0], pend[1] (u32) | op_slot (u64) | op_word (u32) | op_flag (u8) | op_pt (PT_MAX u32)
-    const uint64_t per_op = 4 + 4 + 8 + 4 + 1 + 4 * fm::PT_MAX;
+    const uint64_t per_op = 4 + 4 + 8 + 4 + 1 + 4 * fm::PT_MAX + 4;
     const uint64_t want = n + n / 4 + 1024;
-    const size_t bytes = (size_t)(want * per_op + 6 * 256);
+    const size_t bytes = (size_t)(want * per_op + 7 * 256);
     if (t->sc_base) cudaFree(t->sc_base);
     t->sc_base = nullptr;
     t->sc = OpScratch{};
@@ -141,6 +141,7 @@ int ensure_scratch(fm_table* t, uint64_t n) {
     t->sc.op_word = (uint32_t*)carve(want * 4);
     t->sc.op_pt = (uint32_t*)carve(want * 4 * fm::PT_MAX);
     t->sc.op_flag = carve(want);
+    t->sc.long_list = (uint32_t*)carve(want * 4);
     t->sc.cap_ops = want;
     t->sc_bytes = bytes;
     // op_word doubles as the insert inflow bound: idle value 0xFFFFFFFF.
@@ -611,7 +612,8 @@ constexpr size_t NA_SLOT = NA_PEND1 + na_align(NA_OPS * 4);
 constexpr size_t NA_WORD = NA_SLOT + na_align(NA_OPS * 8);
 constexpr size_t NA_PT = NA_WORD + na_align(NA_OPS * 4);
 constexpr size_t NA_FLAG = NA_PT + na_align(NA_OPS * 4 * fm::PT_MAX);
-constexpr size_t NA_BYTES = NA_FLAG + na_align(NA_OPS);
+constexpr size_t NA_LONG = NA_FLAG + na_align(NA_OPS);
+constexpr size_t NA_BYTES = NA_LONG + na_align(NA_OPS * 4);
 
 }  // namespace
 
@@ -653,6 +655,7 @@ int noalloc_rounds(fm_table* t, const uint8_t* d_k, const uint8_t* d_v, uint32_t
     sc.op_word = (uint32_t*)(base + NA_WORD);
     sc.op_pt = (uint32_t*)(base + NA_PT);
     sc.op_flag = base + NA_FLAG;
+    sc.long_list = (uint32_t*)(base + NA_LONG);
     sc.cap_ops = NA_OPS;
     const fm::Shape sh = t->shape_for({d_k, d_v});
     const fm::TableView v = t->view();

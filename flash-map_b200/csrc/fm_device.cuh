@@ -204,6 +204,12 @@ struct RegKey {
         }
         return diff == 0;
     }
+    __device__ __forceinline__ bool same(const RegKey& o) const {
+        uint32_t diff = 0;
+#pragma unroll
+        for (int i = 0; i < NW; i++) diff |= w[i] ^ o.w[i];
+        return diff == 0;
+    }
     __device__ __forceinline__ void store(uint8_t* p, uint32_t) const {
         if constexpr (KB % 16 == 0) {
 #pragma unroll
@@ -281,6 +287,29 @@ struct RegVal {
 #pragma unroll
             for (int i = 0; i < NW; i++) reinterpret_cast<uint32_t*>(p)[i] = w[i];
         }
+    }
+    // Load through the read-only path (the table is not written concurrently).
+    __device__ __forceinline__ void load_ro(const uint8_t* p) {
+        if constexpr (VB % 16 == 0) {
+#pragma unroll
+            for (int i = 0; i < VB / 16; i++) {
+                const uint4 v = __ldg(reinterpret_cast<const uint4*>(p) + i);
+                w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w;
+            }
+        } else if constexpr (VB % 8 == 0) {
+#pragma unroll
+            for (int i = 0; i < VB / 8; i++) {
+                const uint2 v = __ldg(reinterpret_cast<const uint2*>(p) + i);
+                w[2 * i] = v.x; w[2 * i + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < NW; i++) w[i] = __ldg(reinterpret_cast<const uint32_t*>(p) + i);
+        }
+    }
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < (NW > 0 ? NW : 1); i++) w[i] = 0u;
     }
 };
 

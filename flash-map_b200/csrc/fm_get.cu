@@ -130,8 +130,66 @@ __global__ void __launch_bounds__(BLOCK) k_count(const uint32_t* __restrict__ fl
     }
 }
 
+// bulk_get with one thread per query (compile-time shapes, capacity >= 8).
+// Each step reads the 8-slot metadata window that holds the probe position as
+// two 16-byte loads (one 32-byte sector, aligned), walks it in registers, and
+// compares keys only where the stored distance equals the probe depth.  With
+// one query per thread about eight times as many queries are in flight per SM
+// as with one query per 8-lane tile, which is what a chain of dependent
+// random reads (key -> metadata -> key -> value) needs.
+template <int KB, int VB>
+__global__ void __launch_bounds__(BLOCK) k_get_thread(TableView t, const uint8_t* __restrict__ qkeys, uint64_t n,
+                                                      uint8_t* __restrict__ out_vals,
+                                                      uint8_t* __restrict__ out_found) {
+    const uint64_t mask = t.mask;
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (uint64_t)gridDim.x * blockDim.x) {
+        RegKey<KB> key;
+        key.load(qkeys + q * KB, KB);
+        const uint64_t h = key.hash(KB, t.hash_mode) & mask;
+        uint64_t wb = h & ~7ull;
+        uint64_t hit = NONE64;
+        bool done = false;
+        while (!done) {
+            const uint4* fp = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
+            const uint4 a = __ldg(fp), b = __ldg(fp + 1);
+            const uint32_t f8[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int l = 0; l < 8; l++) {
+                const uint64_t pos = wb + l;
+                if (done || pos < h) continue;
+                const uint64_t p = pos - h;
+                const uint32_t f = f8[l];
+                const uint32_t s = st_of(f);
+                // Terminators: probe past the capacity, EMPTY, or OCCUPIED with
+                // p > dist (rayon_cpu.rs:91-111); tombstones are skipped.
+                if (p > mask || s == ST_EMPTY || (s == ST_OCC && p > dist_of(f))) {
+                    done = true;
+                } else if (s == ST_OCC && dist_matches(f, p) && key.eq(t.keys + (pos & mask) * KB, KB)) {
+                    hit = pos & mask;
+                    done = true;
+                }
+            }
+            wb += 8;
+        }
+        if (out_vals) {
+            RegVal<VB> v;
+            if (hit != NONE64) v.load_ro(t.vals + hit * VB);
+            else v.zero();
+            v.store(out_vals + q * VB, VB);
+        }
+        if (out_found) out_found[q] = hit != NONE64 ? 1 : 0;
+    }
+}
+
 template <int KB, int VB>
 cudaError_t get_shape(const TableView& t, const uint8_t* q, uint64_t n, uint8_t* ov, uint8_t* of, cudaStream_t s) {
+    if constexpr (KB != 0 && VB != 0) {
+        if (t.mask >= 7) {
+            k_get_thread<KB, VB><<<grid_for(n, 64), BLOCK, 0, s>>>(t, q, n, ov, of);
+            g_launches += 1;
+            return cudaGetLastError();
+        }
+    }
     constexpr int T = 8;
     k_get<KB, VB, T><<<grid_for(n * T, 16), BLOCK, 0, s>>>(t, q, n, ov, of);
     g_launches += 1;

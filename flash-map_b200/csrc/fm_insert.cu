@@ -34,12 +34,33 @@
 namespace fm {
 namespace {
 
+// First free (EMPTY or TOMBSTONE) slot at or after home, NONE64 if the table
+// has none.  With capacity >= 8 the metadata is read in aligned 8-slot
+// windows (one 32-byte sector as two 16-byte loads) and scanned in registers.
 template <int KB>
 __device__ __forceinline__ uint64_t find_free(const TableView& t, const uint8_t* keys, uint32_t j) {
     const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
     RegKey<KB> key;
     key.load(keys + (uint64_t)j * ksz, ksz);
     const uint64_t h = key.hash(ksz, t.hash_mode) & t.mask;
+    if (t.mask >= 7) {
+        // two windows per round trip
+        uint64_t wb = h & ~7ull;
+        for (uint64_t w = 0; w <= (t.mask >> 4) + 1; ++w, wb += 16) {
+            const uint4* p0 = reinterpret_cast<const uint4*>(t.flags + (wb & t.mask));
+            const uint4* p1 = reinterpret_cast<const uint4*>(t.flags + ((wb + 8) & t.mask));
+            const uint4 a = p0[0], b = p0[1], c = p1[0], d = p1[1];
+            const uint32_t f16[16] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w};
+#pragma unroll
+            for (int l = 0; l < 16; l++) {
+                const uint64_t pos = wb + l;
+                if (pos < h) continue;
+                if (pos - h > t.mask) return NONE64;
+                if (is_free(f16[l])) return pos & t.mask;
+            }
+        }
+        return NONE64;
+    }
     for (uint64_t p = 0; p <= t.mask; ++p) {
         const uint64_t s = (h + p) & t.mask;
         if (is_free(t.flags[s])) return s;
@@ -104,13 +125,14 @@ struct ExecAcc {
     bool limit = false;
 };
 
+template <int VB>
+__device__ __forceinline__ void swap_value(uint8_t* p, RegVal<VB>& cv);
+
 // The sequential insert of one key, run by one thread on the segment it owns
 // this round.  Returns 1 when a free slot was claimed.
 template <int KB, int VB>
-__device__ __noinline__ int exec_insert(const TableView& t, const uint8_t* kin, const uint8_t* vin, ExecAcc& a) {
+__device__ __noinline__ int exec_insert_key(const TableView& t, RegKey<KB> ck, const uint8_t* vin, ExecAcc& a) {
     const uint64_t mask = t.mask;
-    RegKey<KB> ck;
-    ck.load(kin, KB);
     RegVal<VB> cv;
     cv.load(vin, VB);
     uint64_t h = ck.hash(KB, t.hash_mode) & mask;
@@ -134,14 +156,11 @@ __device__ __noinline__ int exec_insert(const TableView& t, const uint8_t* kin, 
             if (p > d) {  // Robin Hood eviction (rayon_cpu.rs:184-217)
                 RegKey<KB> tk;
                 tk.load_table(t.keys + idx * KB, KB);
-                RegVal<VB> tv;
-                tv.load(t.vals + idx * VB, VB);
                 ck.store(t.keys + idx * KB, KB);
-                cv.store(t.vals + idx * VB, VB);
+                swap_value<VB>(t.vals + idx * VB, cv);
                 t.flags[idx] = mk_flag(ST_OCC, p);
                 a.maxd = max(a.maxd, (uint32_t)min(p, (uint64_t)DIST_MASK));
                 ck = tk;
-                cv = tv;
                 h = ck.hash(KB, t.hash_mode) & mask;
                 p = d + 1;
                 continue;
@@ -159,6 +178,236 @@ __device__ __noinline__ int exec_insert(const TableView& t, const uint8_t* kin, 
         }
         ++p;
     }
+}
+
+template <int KB, int VB>
+__device__ __forceinline__ int exec_insert(const TableView& t, const uint8_t* kin, const uint8_t* vin, ExecAcc& a) {
+    RegKey<KB> ck;
+    ck.load(kin, KB);
+    return exec_insert_key<KB, VB>(t, ck, vin, a);
+}
+
+// Swap a value held in registers with the value at p (in halves of at most
+// 64 bytes, so the temporary stays small).
+template <int VB>
+__device__ __forceinline__ void swap_value(uint8_t* p, RegVal<VB>& cv) {
+    constexpr int CW = (VB % 16 == 0) ? 4 : ((VB % 8 == 0) ? 2 : 1);  // words per chunk
+    constexpr int NCH = VB / (4 * CW);
+    constexpr int HALF = NCH > 4 ? 4 : NCH;
+#pragma unroll
+    for (int c0 = 0; c0 < NCH; c0 += HALF) {
+        uint32_t tmp[HALF * CW];
+#pragma unroll
+        for (int c = 0; c < HALF && c0 + c < NCH; c++) {
+            if constexpr (CW == 4) {
+                const uint4 v = reinterpret_cast<const uint4*>(p)[c0 + c];
+                tmp[4 * c] = v.x; tmp[4 * c + 1] = v.y; tmp[4 * c + 2] = v.z; tmp[4 * c + 3] = v.w;
+            } else if constexpr (CW == 2) {
+                const uint2 v = reinterpret_cast<const uint2*>(p)[c0 + c];
+                tmp[2 * c] = v.x; tmp[2 * c + 1] = v.y;
+            } else {
+                tmp[c] = reinterpret_cast<const uint32_t*>(p)[c0 + c];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < HALF && c0 + c < NCH; c++) {
+            const int w = (c0 + c) * CW;
+            if constexpr (CW == 4)
+                reinterpret_cast<uint4*>(p)[c0 + c] = make_uint4(cv.w[w], cv.w[w + 1], cv.w[w + 2], cv.w[w + 3]);
+            else if constexpr (CW == 2)
+                reinterpret_cast<uint2*>(p)[c0 + c] = make_uint2(cv.w[w], cv.w[w + 1]);
+            else
+                reinterpret_cast<uint32_t*>(p)[c0 + c] = cv.w[w];
+#pragma unroll
+            for (int i = 0; i < CW; i++) cv.w[w + i] = tmp[c * CW + i];
+        }
+    }
+}
+
+// One move of a whole entry (or just its value) from a source to a slot, in
+// groups of at most 64 bytes so the temporary stays small.  Every thread of a
+// warp runs the same loop, so their loads issue together.
+template <int KB, int VB>
+__device__ __forceinline__ void move_entry(const TableView& t, const uint8_t* ksrc, const uint8_t* vsrc, uint64_t dst,
+                                           bool value_only, bool src_ro) {
+    constexpr int CW = (KB % 16 == 0 && VB % 16 == 0) ? 16 : ((KB % 8 == 0 && VB % 8 == 0) ? 8 : 4);
+    using Ch = typename std::conditional<CW == 16, uint4, typename std::conditional<CW == 8, uint2, uint32_t>::type>::type;
+    constexpr int NK = KB / CW, NV = VB / CW;
+    if (!value_only) {
+        Ch k[NK];
+#pragma unroll
+        for (int c = 0; c < NK; c++)
+            k[c] = src_ro ? __ldg(reinterpret_cast<const Ch*>(ksrc) + c) : reinterpret_cast<const Ch*>(ksrc)[c];
+#pragma unroll
+        for (int c = 0; c < NK; c++) reinterpret_cast<Ch*>(t.keys + dst * KB)[c] = k[c];
+    }
+    constexpr int G = (64 / CW) > 0 ? (64 / CW) : 1;
+#pragma unroll
+    for (int c0 = 0; c0 < NV; c0 += G) {
+        Ch v[G];
+#pragma unroll
+        for (int c = 0; c < G; c++)
+            if (c0 + c < NV)
+                v[c] = src_ro ? __ldg(reinterpret_cast<const Ch*>(vsrc) + c0 + c)
+                              : reinterpret_cast<const Ch*>(vsrc)[c0 + c];
+#pragma unroll
+        for (int c = 0; c < G; c++)
+            if (c0 + c < NV) reinterpret_cast<Ch*>(t.vals + dst * VB)[c0 + c] = v[c];
+    }
+}
+
+constexpr int TH_MAXK = 3;  // evictions per op on the thread path
+constexpr int TH_MAXC = 2;  // possible updates per op on the thread path
+
+// The sequential insert of one key by one thread, for the common short walk
+// (capacity >= 8, rounds that are not serial, so the walk ends at or before
+// the op's free slot and visits each slot once).  Dependent memory round
+// trips: the two aligned 8-slot metadata windows from home (one trip), the
+// key compares at the slots where the stored distance equals the probe depth
+// (one trip), then one per entry move.
+//   1. walk the 16 metadata words in registers, recording the eviction slots
+//      (slot P_i takes the entry carried there; the evicted resident continues
+//      at the next slot with depth dist+1) and the possible updates;
+//   2. compare the carried key at those slots, the first match in walk order
+//      ending the walk as an in-place update;
+//   3. move entries, highest first: the end slot gets the entry evicted at
+//      P_(k-1), P_i the one evicted at P_(i-1), P_0 the new entry; then the
+//      metadata words.
+// A walk that leaves the two windows, needs more than TH_MAXK evictions or
+// more than TH_MAXC compares returns -1 having written nothing.  The small
+// arrays are written through unrolled selects so they stay in registers.
+template <int KB, int VB>
+__device__ __noinline__ int exec_insert_thread(const TableView& t, const RegKey<KB>& key, const uint8_t* kin,
+                                               const uint8_t* vin, ExecAcc& a) {
+    const uint64_t mask = t.mask;
+    uint64_t ev_pos[TH_MAXK];
+    uint32_t ev_p[TH_MAXK];
+    uint64_t cd_pos[TH_MAXC];
+    uint32_t cd_stage[TH_MAXC];
+#pragma unroll
+    for (int i = 0; i < TH_MAXK; i++) ev_pos[i] = 0, ev_p[i] = 0;
+#pragma unroll
+    for (int i = 0; i < TH_MAXC; i++) cd_pos[i] = 0, cd_stage[i] = 0;
+    uint32_t k = 0, nc = 0;
+    int kind = 0;  // 1 claim, 2 update, 3 drop, 4 too long for this path
+    uint64_t end_pos = 0, end_p = 0;
+    bool end_tomb = false;
+    const uint64_t h = key.hash(KB, t.hash_mode) & mask;
+    const uint64_t wb = h & ~7ull;
+    const uint4* w0 = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
+    const uint4* w1 = reinterpret_cast<const uint4*>(t.flags + ((wb + 8) & mask));
+    const uint4 fa = w0[0], fb = w0[1], fc = w1[0], fd = w1[1];
+    const uint32_t f16[16] = {fa.x, fa.y, fa.z, fa.w, fb.x, fb.y, fb.z, fb.w,
+                              fc.x, fc.y, fc.z, fc.w, fd.x, fd.y, fd.z, fd.w};
+    uint64_t p = 0;
+#pragma unroll
+    for (int l = 0; l < 16; l++) {
+        const uint64_t pos = wb + l;
+        if (kind != 0 || pos < h) continue;
+        const uint32_t f = f16[l];
+        const uint32_t s = st_of(f);
+        if (p > mask) {
+            kind = 3;  // drop (rayon_cpu.rs:167-169)
+        } else if (s == ST_EMPTY || s == ST_TOMB) {
+            kind = 1;
+            end_pos = pos;
+            end_p = p;
+            end_tomb = s == ST_TOMB;
+        } else if (s == ST_OCC) {
+            if (dist_matches(f, p)) {
+                if (nc < TH_MAXC) {
+#pragma unroll
+                    for (int i = 0; i < TH_MAXC; i++)
+                        if (i == (int)nc) cd_pos[i] = pos, cd_stage[i] = k;
+                    ++nc;
+                } else {
+                    kind = 4;
+                }
+                ++p;
+            } else if (p > dist_of(f)) {
+                if (k < TH_MAXK) {
+#pragma unroll
+                    for (int i = 0; i < TH_MAXK; i++)
+                        if (i == (int)k) ev_pos[i] = pos, ev_p[i] = (uint32_t)p;
+                    ++k;
+                    p = dist_of(f) + 1;
+                } else {
+                    kind = 4;
+                }
+            } else {
+                ++p;
+            }
+        } else {
+            ++p;
+        }
+    }
+    if (kind == 0 || kind == 4) return -1;  // nothing written; the warp-per-op pass runs it
+    // 2. possible updates: every compare's loads in one round trip, then the
+    // first match in walk order (slots at or past a claimed end are not reached)
+    {
+        RegKey<KB> sk[TH_MAXC], ck[TH_MAXC];
+#pragma unroll
+        for (int c = 0; c < TH_MAXC; c++) {
+            if (c < (int)nc) {
+                sk[c].load_table(t.keys + (cd_pos[c] & mask) * KB, KB);
+                uint32_t st = cd_stage[c];
+                uint64_t src = 0;
+#pragma unroll
+                for (int i = 0; i < TH_MAXK; i++)
+                    if (i + 1 == (int)st) src = ev_pos[i];
+                // the entry carried at that point, still at its old slot
+                if (st) ck[c].load_table(t.keys + (src & mask) * KB, KB);
+                else ck[c] = key;
+            }
+        }
+        bool found = false;
+#pragma unroll
+        for (int c = 0; c < TH_MAXC; c++) {
+            if (found || c >= (int)nc) continue;
+            if (kind == 1 && cd_pos[c] >= end_pos) continue;
+            if (ck[c].same(sk[c])) {
+                found = true;
+                kind = 2;
+                end_pos = cd_pos[c];
+                k = cd_stage[c];
+            }
+        }
+    }
+    // 3. moves, highest first (kind 3: the last carried entry is dropped)
+    const int M = (kind == 3) ? (int)k : (int)k + 1;
+#pragma unroll
+    for (int m = TH_MAXK; m >= 0; m--) {
+        if (m >= M) continue;
+        uint64_t dst = end_pos, src = 0;
+#pragma unroll
+        for (int i = 0; i < TH_MAXK; i++) {
+            if (i == m && m < (int)k) dst = ev_pos[i];
+            if (i + 1 == m) src = ev_pos[i];
+        }
+        dst &= mask;
+        const bool value_only = (m == (int)k) && kind == 2;
+        if (m == 0) {
+            move_entry<KB, VB>(t, kin, vin, dst, value_only, true);
+        } else {
+            src &= mask;
+            move_entry<KB, VB>(t, t.keys + src * KB, t.vals + src * VB, dst, value_only, false);
+        }
+    }
+    uint32_t md = 0;
+#pragma unroll
+    for (int m = 0; m < TH_MAXK; m++) {
+        if (m < (int)k) {
+            t.flags[ev_pos[m] & mask] = mk_flag(ST_OCC, ev_p[m]);
+            md = max(md, min(ev_p[m], DIST_MASK));
+        }
+    }
+    if (kind == 1) {
+        t.flags[end_pos & mask] = mk_flag(ST_OCC, end_p);
+        md = max(md, (uint32_t)min(end_p, (uint64_t)DIST_MASK));
+        a.tomb = a.tomb || end_tomb;
+    }
+    a.maxd = max(a.maxd, md);
+    return kind == 1 ? 1 : 0;
 }
 
 // Run-time sizes (up to GENERIC_MAX_KV bytes each): the carried entry lives in
@@ -225,27 +474,55 @@ __device__ __forceinline__ int exec_insert_generic(const TableView& t, const uin
     }
 }
 
-// Phase 3 for op j (scalar path): run it if it leads an unblocked segment of a
-// non-serial round, then clear its registration.  Returns whether it ran.
+// Phase 3 for op j (one thread per op): run it if it leads an unblocked
+// segment of a non-serial round, then clear its registration.  Returns whether
+// it ran.  A walk too long for the thread path is appended to long_list (when
+// given; it then counts as run: its segment is disjoint from every other
+// segment of the round, so running it after them gives the same result),
+// otherwise it takes the scalar walk.
 template <int KB, int VB>
 __device__ __forceinline__ bool finish_op(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t j,
-                                          bool serial, const OpScratch& sc, ExecAcc& a) {
-    const bool run = !serial && sc.op_flag[j] != 0 && sc.op_word[j] > j;
-    if (run) {
-        const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
-        const uint32_t vsz = VB ? (uint32_t)VB : t.vsz;
-        if constexpr (KB == 0 || VB == 0)
-            a.claimed += exec_insert_generic(t, keys + (uint64_t)j * ksz, vals + (uint64_t)j * vsz, a);
-        else
-            a.claimed += exec_insert<KB, VB>(t, keys + (uint64_t)j * ksz, vals + (uint64_t)j * vsz, a);
+                                          bool serial, const OpScratch& sc, ExecAcc& a, uint32_t* long_list = nullptr,
+                                          uint32_t* long_n = nullptr) {
+    const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
+    const uint32_t vsz = VB ? (uint32_t)VB : t.vsz;
+    if constexpr (KB == 0 || VB == 0) {
+        const bool run = !serial && sc.op_flag[j] != 0 && sc.op_word[j] > j;
+        if (run) a.claimed += exec_insert_generic(t, keys + (uint64_t)j * ksz, vals + (uint64_t)j * vsz, a);
+        const uint64_t F = sc.op_slot[j];
+        if (F != NONE64) {
+            t.seg_min[F] = IDLE;
+            t.seg_cnt[F] = 0;
+        }
+        sc.op_word[j] = IDLE;
+        return run;
+    } else {
+        // independent loads issued together: decision words, registration, key
+        const uint8_t lead = sc.op_flag[j];
+        const uint32_t blk = sc.op_word[j];
+        const uint64_t F = sc.op_slot[j];
+        RegKey<KB> key;
+        key.load(keys + (uint64_t)j * ksz, ksz);
+        const bool run = !serial && lead != 0 && blk > j;
+        bool defer = false;
+        if (run) {
+            // windows need capacity >= 8; consecutive walk positions need
+            // probe depths below 2^28 (the stored distance width)
+            int c = -1;
+            if (t.mask >= 7 && t.mask < (uint64_t)DIST_MASK)
+                c = exec_insert_thread<KB, VB>(t, key, keys + (uint64_t)j * ksz, vals + (uint64_t)j * vsz, a);
+            if (c < 0 && long_list) defer = true;
+            else if (c < 0) c = exec_insert_key<KB, VB>(t, key, vals + (uint64_t)j * vsz, a);
+            if (c > 0) a.claimed += c;
+        }
+        if (long_list) append(long_list, long_n, j, defer);
+        if (F != NONE64) {
+            t.seg_min[F] = IDLE;
+            t.seg_cnt[F] = 0;
+        }
+        sc.op_word[j] = IDLE;
+        return run;
     }
-    const uint64_t F = sc.op_slot[j];
-    if (F != NONE64) {
-        t.seg_min[F] = IDLE;
-        t.seg_cnt[F] = 0;
-    }
-    sc.op_word[j] = IDLE;
-    return run;
 }
 
 // Rare facts, once per warp: the largest stored distance, tombstone reuse and
@@ -334,8 +611,18 @@ struct ChunkOf {
     static constexpr int NC = NK + NV;
 };
 
+// Chunk c (CK bytes) of a key held in registers.
+template <int KB, class Ch, int CK>
+__device__ __forceinline__ Ch key_chunk(const RegKey<KB>& key, int c) {
+    Ch x;
+    uint32_t* w = reinterpret_cast<uint32_t*>(&x);
+#pragma unroll
+    for (int i = 0; i < CK / 4; i++) w[i] = key.w[c * (CK / 4) + i];
+    return x;
+}
+
 template <int KB, int VB, int T>
-__device__ __forceinline__ void exec_tile(const TableView& t, const uint8_t* __restrict__ keys_in,
+__device__ __forceinline__ void exec_tile(const TableView& t, const RegKey<KB>& key,
                                           const uint8_t* __restrict__ vals_in, uint32_t j, const Tile<T>& tl,
                                           uint64_t* s_pos, uint32_t* s_p, ExecAcc& a) {
     using CO = ChunkOf<KB, VB>;
@@ -345,8 +632,6 @@ __device__ __forceinline__ void exec_tile(const TableView& t, const uint8_t* __r
     constexpr int CPL = (MB * NC + T - 1) / T;
     const uint64_t mask = t.mask;
     const uint32_t lane = tl.lane;
-    RegKey<KB> key;
-    key.load(keys_in + (uint64_t)j * KB, KB);
     const uint64_t h = key.hash(KB, t.hash_mode) & mask;
 
     // -- walk: metadata only, plus key compares at possible updates ----------
@@ -416,7 +701,7 @@ __device__ __forceinline__ void exec_tile(const TableView& t, const uint8_t* __r
         wb += T;
     }
     if (kind == 4) {  // very long chain: the sequential walk, on lane 0
-        if (lane == 0) a.claimed += exec_insert<KB, VB>(t, keys_in + (uint64_t)j * KB, vals_in + (uint64_t)j * VB, a);
+        if (lane == 0) a.claimed += exec_insert_key<KB, VB>(t, key, vals_in + (uint64_t)j * VB, a);
         tl.sync();
         return;
     }
@@ -440,7 +725,11 @@ __device__ __forceinline__ void exec_tile(const TableView& t, const uint8_t* __r
                 const bool value_only = (m == (int)k) && kind == 2;
                 if (value_only && c < NK) continue;
                 const uint8_t* src;
-                if (m == 0) src = c < NK ? keys_in + (uint64_t)j * KB + c * CK : vals_in + (uint64_t)j * VB + (c - NK) * CK;
+                if (m == 0 && c < NK) {
+                    buf[u] = key_chunk<KB, Ch, CK>(key, c);
+                    continue;
+                }
+                if (m == 0) src = vals_in + (uint64_t)j * VB + (c - NK) * CK;
                 else {
                     const uint64_t ss = s_pos[m - 1] & mask;
                     src = c < NK ? t.keys + ss * KB + c * CK : t.vals + ss * VB + (c - NK) * CK;
@@ -509,15 +798,17 @@ __global__ void __launch_bounds__(RBLOCK) k_ins_p2(TableView t, uint32_t n0, uin
 }
 
 template <int KB, int VB>
-__global__ void __launch_bounds__(RBLOCK) k_ins_p3(TableView t, const uint8_t* __restrict__ keys,
+__global__ void __launch_bounds__(RBLOCK, 3) k_ins_p3(TableView t, const uint8_t* __restrict__ keys,
                                                    const uint8_t* __restrict__ vals, uint32_t n0, uint32_t r,
                                                    OpScratch sc, Ctl* ctl) {
     __shared__ AppendSmem s_app;
     __shared__ uint32_t s_tmp[RBLOCK / 32];
+    append_init(s_app);
     const RoundOps ops = round_ops(sc, ctl, r, n0);
     const bool serial = *(volatile uint32_t*)&ctl->serial[r & 1] != 0;
     uint32_t* out = pend_of(sc, r + 1);
     uint32_t* out_n = &ctl->npend[(r + 1) & 1];
+    uint32_t* long_n = &ctl->nlong[r & 1];
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t iters = grid_iters(ops.n);
@@ -529,7 +820,7 @@ __global__ void __launch_bounds__(RBLOCK) k_ins_p3(TableView t, const uint8_t* _
         bool ran = false;
         if (valid) {
             j = ops.op(i);
-            ran = finish_op<KB, VB>(t, keys, vals, j, serial, sc, a);
+            ran = finish_op<KB, VB>(t, keys, vals, j, serial, sc, a, sc.long_list, long_n);
         }
         block_append(out, out_n, j, valid && !ran, s_app);
     }
@@ -565,11 +856,16 @@ template <int KB, int VB, int T>
 __device__ __forceinline__ bool finish_tile(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t j,
                                             bool serial, const OpScratch& sc, const Tile<T>& tl, uint64_t* s_pos,
                                             uint32_t* s_p, ExecAcc& a) {
-    const bool run = !serial && sc.op_flag[j] != 0 && sc.op_word[j] > j;
-    if (run) exec_tile<KB, VB, T>(t, keys, vals, j, tl, s_pos, s_p, a);
+    // independent loads issued together: decision words, registration, key
+    const uint8_t lead = sc.op_flag[j];
+    const uint32_t blk = sc.op_word[j];
+    const uint64_t F = sc.op_slot[j];
+    RegKey<KB> key;
+    key.load(keys + (uint64_t)j * KB, KB);
+    const bool run = !serial && lead != 0 && blk > j;
+    if (run) exec_tile<KB, VB, T>(t, key, vals, j, tl, s_pos, s_p, a);
     tl.sync();
     if (tl.lane == 0) {
-        const uint64_t F = sc.op_slot[j];
         if (F != NONE64) {
             t.seg_min[F] = IDLE;
             t.seg_cnt[F] = 0;
@@ -580,13 +876,14 @@ __device__ __forceinline__ bool finish_tile(const TableView& t, const uint8_t* k
 }
 
 template <int KB, int VB, int T>
-__global__ void __launch_bounds__(RBLOCK, 3) k_ins_p3t(TableView t, const uint8_t* __restrict__ keys,
+__global__ void __launch_bounds__(RBLOCK, 4) k_ins_p3t(TableView t, const uint8_t* __restrict__ keys,
                                                        const uint8_t* __restrict__ vals, uint32_t n0, uint32_t r,
                                                        OpScratch sc, Ctl* ctl) {
     __shared__ uint64_t s_pos[RBLOCK / T][MAXCH];
     __shared__ uint32_t s_p[RBLOCK / T][MAXCH];
     __shared__ AppendSmem s_app;
     __shared__ uint32_t s_tmp[RBLOCK / 32];
+    append_init(s_app);
     const RoundOps ops = round_ops(sc, ctl, r, n0);
     const bool serial = *(volatile uint32_t*)&ctl->serial[r & 1] != 0;
     uint32_t* out = pend_of(sc, r + 1);
@@ -611,6 +908,35 @@ __global__ void __launch_bounds__(RBLOCK, 3) k_ins_p3t(TableView t, const uint8_
     block_add_count(ctl, a.claimed, s_tmp);
     publish_rare(ctl, a.maxd, a.tomb, a.limit);
     if (blockIdx.x == 0 && threadIdx.x == 0 && ops.n) atomicAdd(&ctl->rounds, 1u);
+}
+
+// Phase 4: the inserts of round r whose walks were too long for one thread,
+// one warp each (32-slot metadata windows, up to 12 entry moves per batch of
+// round trips).  Their segments are disjoint from each other and from every
+// op run in phase 3.
+template <int KB, int VB>
+__global__ void __launch_bounds__(RBLOCK, 2) k_ins_p4(TableView t, const uint8_t* __restrict__ keys,
+                                                   const uint8_t* __restrict__ vals, uint32_t r, OpScratch sc,
+                                                   Ctl* ctl) {
+    constexpr int NW = RBLOCK / 32;
+    __shared__ uint64_t s_pos[NW][MAXCH];
+    __shared__ uint32_t s_p[NW][MAXCH];
+    __shared__ uint32_t s_tmp[NW];
+    const uint32_t n = *(volatile const uint32_t*)&ctl->nlong[r & 1];
+    if (n == 0) return;  // block-uniform
+    const Tile<32> tl;
+    const uint32_t w = threadIdx.x >> 5;
+    const uint32_t nwarps = gridDim.x * NW;
+    ExecAcc a;
+    for (uint32_t i = blockIdx.x * NW + w; i < n; i += nwarps) {
+        const uint32_t j = sc.long_list[i];
+        RegKey<KB> key;
+        key.load(keys + (uint64_t)j * KB, KB);
+        exec_tile<KB, VB, 32>(t, key, vals, j, tl, s_pos[w], s_p[w], a);
+        tl.sync();
+    }
+    block_add_count(ctl, a.claimed, s_tmp);
+    publish_rare(ctl, a.maxd, a.tomb, a.limit);
 }
 
 // ---- single-block tails ----------------------------------------------------
@@ -762,28 +1088,22 @@ template <int KB, int VB>
 void rounds_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, uint32_t r0,
                   uint32_t nrounds, uint32_t grid_ops, uint32_t nops, const OpScratch& sc, Ctl* ctl,
                   cudaStream_t s) {
+    // one op per thread: far more ops in flight than one per tile, which is
+    // what chains of dependent random reads need
+    const unsigned g = grid_for(grid_ops, 8);
     for (uint32_t r = r0; r < r0 + nrounds; r++) {
-        if constexpr (KB != 0 && VB != 0) {
-            const unsigned gt = grid_for((uint64_t)grid_ops * INS_T, 8);
-            const unsigned g = grid_for(grid_ops, 8);
-            k_ins_p1t<KB, INS_T><<<gt, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
-            k_ins_p2<<<g, RBLOCK, 0, s>>>(t, n0, r, nops, sc, ctl);
-            k_ins_p3t<KB, VB, INS_T><<<gt, RBLOCK, 0, s>>>(t, keys, vals, n0, r, sc, ctl);
-        } else {
-            const unsigned g = grid_for(grid_ops, 8);
-            k_ins_p1<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
-            k_ins_p2<<<g, RBLOCK, 0, s>>>(t, n0, r, nops, sc, ctl);
-            k_ins_p3<KB, VB><<<g, RBLOCK, 0, s>>>(t, keys, vals, n0, r, sc, ctl);
-        }
+        k_ins_p1<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
+        k_ins_p2<<<g, RBLOCK, 0, s>>>(t, n0, r, nops, sc, ctl);
+        k_ins_p3<KB, VB><<<g, RBLOCK, 0, s>>>(t, keys, vals, n0, r, sc, ctl);
+        if constexpr (KB != 0 && VB != 0) k_ins_p4<KB, VB><<<g, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
     }
-    count_launches(3 * nrounds);
+    count_launches((KB != 0 && VB != 0 ? 4 : 3) * nrounds);
 }
 
 template <int KB, int VB>
 void tail_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, uint32_t r,
                 uint32_t nops, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
-    constexpr int T = (KB != 0 && VB != 0) ? INS_T : 1;
-    k_ins_tail<KB, VB, T><<<1, TAIL_THREADS, 0, s>>>(t, keys, vals, n0, r, nops, sc, ctl);
+    k_ins_tail<KB, VB, (KB && VB) ? INS_T : 1><<<1, TAIL_THREADS, 0, s>>>(t, keys, vals, n0, r, nops, sc, ctl);
     count_launches(1);
 }
 

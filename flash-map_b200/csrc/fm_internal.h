@@ -26,6 +26,7 @@ struct Ctl {
     uint32_t serial[2];      // 1: a round found no free slot / a flow wrapping the table
     uint32_t err;            // device-side error bits
     uint32_t rounds;         // rounds run by the call (statistics)
+    uint32_t nlong[2];       // inserts deferred to the warp-per-op pass, per round parity
     unsigned long long count;  // new keys (insert) / removed keys (remove), single-block kernels
     unsigned long long count_part[COUNT_PARTS][4];  // the same from grid kernels, [i][0] used
     // Persistent table facts (survive across calls, reset by clear):
@@ -38,7 +39,7 @@ struct Ctl {
         return s;
     }
 };
-constexpr size_t CTL_CALL_BYTES = 32 + 32 * COUNT_PARTS;  // npend .. count_part
+constexpr size_t CTL_CALL_BYTES = 40 + 32 * COUNT_PARTS;  // npend .. count_part
 static_assert(offsetof(Ctl, dmax) == CTL_CALL_BYTES, "Ctl layout");
 
 // Device-side error bits (Ctl::err).
@@ -53,6 +54,7 @@ struct OpScratch {
     uint32_t* op_word;   // insert: inflow lower bound; remove: window length (idle 0xFFFFFFFF)
     uint8_t* op_flag;    // insert: leader bit; remove: potential-target count
     uint32_t* op_pt;     // remove: up to PT_MAX potential-target distances per op
+    uint32_t* long_list; // insert: ops of this round deferred to the warp-per-op pass
     uint64_t cap_ops;
 };
 constexpr int PT_MAX = 4;

@@ -138,6 +138,7 @@ __global__ void __launch_bounds__(RBLOCK) k_rem_p2(TableView t, const uint8_t* _
                                                    uint32_t r, OpScratch sc, Ctl* ctl) {
     __shared__ AppendSmem s_app;
     __shared__ uint32_t s_tmp[RBLOCK / 32];
+    append_init(s_app);
     const RoundOps ops = round_ops(sc, ctl, r, n0);
     uint32_t* out = pend_of(sc, r + 1);
     uint32_t* out_n = &ctl->npend[(r + 1) & 1];

@@ -73,27 +73,42 @@ __device__ __forceinline__ void reset_next_round(Ctl* ctl, uint32_t r) {
     const uint32_t nx = (r + 1) & 1;
     ctl->npend[nx] = 0;
     ctl->serial[nx] = 0;
+    ctl->nlong[nx] = 0;
 }
 
 // Block-aggregated append: one global atomic per block per call.  Every
 // thread of the block calls it (block-uniform control flow); each thread
 // appends at most one entry.
 struct AppendSmem {
-    uint32_t n;
-    uint32_t base;
-    uint32_t buf[RBLOCK > 512 ? RBLOCK : 512];
+    uint32_t n[2];     // per-call counters, alternating (the idle one is reset in passing)
+    uint32_t base[2];
+    uint32_t buf[2][RBLOCK];
+    uint32_t phase;
 };
 
+__device__ __forceinline__ void append_init(AppendSmem& s) {
+    if (threadIdx.x == 0) {
+        s.n[0] = s.n[1] = 0;
+        s.phase = 0;
+    }
+    __syncthreads();
+}
+
+// Two block barriers per call: entries go to a shared buffer, thread 0 takes
+// the block's range with one global atomic, then the buffer is copied out
+// while the other buffer's counter is cleared for the next call.
 __device__ __forceinline__ void block_append(uint32_t* list, uint32_t* counter, uint32_t j, bool take, AppendSmem& s) {
-    if (threadIdx.x == 0) s.n = 0;
+    const uint32_t ph = s.phase;
+    if (take) s.buf[ph][atomicAdd(&s.n[ph], 1u)] = j;
     __syncthreads();
-    if (take) s.buf[atomicAdd(&s.n, 1u)] = j;
+    const uint32_t n = s.n[ph];
+    if (threadIdx.x == 0) {
+        if (n) s.base[ph] = atomicAdd(counter, n);
+        s.n[ph ^ 1] = 0;
+        s.phase = ph ^ 1;
+    }
     __syncthreads();
-    const uint32_t n = s.n;
-    if (threadIdx.x == 0 && n) s.base = atomicAdd(counter, n);
-    __syncthreads();
-    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) list[s.base + k] = s.buf[k];
-    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) list[s.base[ph] + k] = s.buf[ph][k];
 }
 
 // Block sum of v added to one of the spread counters.  Block-uniform call.
