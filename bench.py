@@ -1,19 +1,24 @@
 #!/usr/bin/env python
 """FlashMap B200 backend benchmark: prints ONE JSON line.
 
-Workload (one "step"), the account shape FlashMap<[u8;32],[u8;128]>:
-  with_capacity(10,000,000) (2^24 slots), clear, 8,000,000 distinct pairs
-  inserted as 80 bulk_insert calls of 100,000, one bulk_get of 8,000,000 keys
-  (50% present, 50% fresh random keys, shuffled), one bulk_remove of a random
-  800,000 present keys.  Keys and values are seeded uniform random bytes.
+Workload (one "step"), the account shape FlashMap<[u8;32],[u8;128]> at load
+factor 0.8: with_capacity(2^24), clear, 13,421,773 distinct pairs inserted as
+bulk_insert calls of 100,000 (the last one shorter), one bulk_get of 8,000,000
+keys (50% present, 50% fresh random keys, shuffled), one bulk_remove of a
+random 10% of the present keys.  Keys and values are seeded uniform random
+bytes.  with_capacity(10,000,000) as written rounds up to 2^24 slots, where
+8,000,000 pairs are load 0.477; that variant is timed too and reported under
+"as_written".
 
-  value  = ops of the step (16.8M) x ranks / device time (CUDA events, max
-           over ranks), inputs resident in HBM, device-pointer API.
+  value  = ops of the step x ranks / device time (CUDA events, max over
+           ranks), inputs resident in HBM, device-pointer API.
   e2e    = the same step through the host API (fm_bulk_insert/get/remove with
            pinned host buffers: H2D of inputs and D2H of results inside).
-  roofline: the bulk_get kernel, algorithmic bytes per query (counted by the
-           CPU oracle on the same workload at 1/16 scale) x queries / launch
-           time, against MEASURED_PEAKS.json hbm_gbs.
+  roofline: per kernel set (insert: the round kernels of every call; get: the
+           one lookup kernel), algorithmic bytes per op (counted by the CPU
+           oracle on the same workload at 1/16 scale) x ops / the set's device
+           time, read from the library's per-kernel CUDA events in an extra
+           step, against MEASURED_PEAKS.json hbm_gbs.
   cpu_baseline: the sequential CPU oracle on the 1/16-scale sample.
 
 `--impl reference` times the reference's CPU algorithm (multithreaded CAS
@@ -35,29 +40,49 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "flash-map_b200"))
 
 METRIC = "bulk get/insert Mops/s at load 0.8, % HBM roofline; served p50/p99 vs plain"
-CAP_REQ = 10_000_000
-N_PAIRS = 8_000_000
 CALL = 100_000
-N_GET = 8_000_000
-N_REM = 800_000
 KB, VB = 32, 128
 SAMPLE_DIV = 16  # CPU sample: same load factors and call size at 1/16 scale
 
 
-def workload_desc():
-    return {
-        "workload": "account shape [u8;32]->[u8;128], with_capacity(10M)=2^24 slots: clear, 8M pairs as "
-                    "80 bulk_insert calls of 100K, bulk_get of 8M (50% hits), bulk_remove of 800K present",
-        "capacity": 1 << 24,
-        "pairs": N_PAIRS,
-        "insert_calls": f"80x{CALL}",
-        "gets": N_GET,
-        "get_hit_rate": 0.5,
-        "removes": N_REM,
-        "load_after_insert": round(N_PAIRS / (1 << 24), 4),
-        "l2": "inputs larger than L2 (table 2.9 GB, 256 MB of get keys per call); no flush",
-        "api": "device-pointer API (fm_*_device), stream-ordered",
-    }
+class Workload:
+    def __init__(self, name, cap_req, pairs, gets, removes):
+        self.name, self.cap_req, self.pairs, self.gets, self.removes = name, cap_req, pairs, gets, removes
+
+    @property
+    def cap(self):
+        c = 1
+        while c < self.cap_req:
+            c <<= 1
+        return c
+
+    @property
+    def ops(self):
+        return self.pairs + self.gets + self.removes
+
+    def scaled(self, div):
+        return Workload(self.name, self.cap_req // div, self.pairs // div, self.gets // div, self.removes // div)
+
+    def desc(self):
+        calls = (self.pairs + CALL - 1) // CALL
+        return {
+            "workload": f"account shape [u8;32]->[u8;128], {self.name}: with_capacity({self.cap_req})="
+                        f"{self.cap} slots, clear, {self.pairs} pairs as {calls} bulk_insert calls of <= {CALL}, "
+                        f"bulk_get of {self.gets} (50% hits), bulk_remove of {self.removes} present",
+            "capacity": self.cap,
+            "pairs": self.pairs,
+            "insert_calls": f"{calls}x<={CALL}",
+            "gets": self.gets,
+            "get_hit_rate": 0.5,
+            "removes": self.removes,
+            "load_after_insert": round(self.pairs / self.cap, 4),
+            "l2": "inputs larger than L2 (table 2.9 GB, 256 MB of get keys per call); no flush",
+            "api": "device-pointer API (fm_*_device), stream-ordered",
+        }
+
+
+LOAD08 = Workload("load 0.8", 1 << 24, 13_421_773, 8_000_000, 1_342_177)
+AS_WRITTEN = Workload("as written (load 0.477)", 10_000_000, 8_000_000, 8_000_000, 800_000)
 
 
 def read_peak():
@@ -71,23 +96,23 @@ def read_peak():
 # ---------------------------------------------------------------------------
 # CPU sample (oracle / reference restatement): 1/16 scale, same load factors
 # ---------------------------------------------------------------------------
-def cpu_sample_inputs(seed=3):
+def cpu_sample_inputs(w, seed=3):
     rng = np.random.default_rng(seed)
-    n = N_PAIRS // SAMPLE_DIV
+    n = w.pairs
     keys = rng.integers(0, 256, (n, KB), dtype=np.uint8)
     vals = rng.integers(0, 256, (n, VB), dtype=np.uint8)
-    ng = N_GET // SAMPLE_DIV
+    ng = w.gets
     q = np.concatenate([keys[rng.choice(n, ng // 2, replace=False)],
                         rng.integers(0, 256, (ng - ng // 2, KB), dtype=np.uint8)])
     q = q[rng.permutation(len(q))]
-    rem = keys[rng.choice(n, N_REM // SAMPLE_DIV, replace=False)]
+    rem = keys[rng.choice(n, w.removes, replace=False)]
     return keys, vals, q, rem
 
 
-def cpu_step(O, inp, threads=None, traffic=False):
+def cpu_step(O, w, inp, threads=None, traffic=False):
     """One sample step on the oracle (threads=None: sequential) -> seconds."""
     keys, vals, q, rem = inp
-    m = O.OracleMap((1 << 24) // SAMPLE_DIV, KB, VB)
+    m = O.OracleMap(w.cap, KB, VB)
     if traffic:
         m.traffic(True)
     t0 = time.perf_counter()
@@ -109,10 +134,6 @@ def cpu_step(O, inp, threads=None, traffic=False):
     return dt, tr
 
 
-def sample_ops():
-    return (N_PAIRS + N_GET + N_REM) // SAMPLE_DIV
-
-
 def bytes_per_op(tr):
     out = {}
     for k, v in tr.items():
@@ -121,28 +142,32 @@ def bytes_per_op(tr):
     return out
 
 
-def cpu_baseline_leg():
+def cpu_baseline_leg(w):
+    """Sequential oracle timed on the 1/16-scale sample of workload w, and the
+    algorithmic bytes per op it counts on the same sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
-    inp = cpu_sample_inputs()
+    ws = w.scaled(SAMPLE_DIV)
+    inp = cpu_sample_inputs(ws)
     reps, total = 0, 0.0
     while reps < 64 and (total < 8.0 or reps < 2):  # ~10 s of CPU work
-        dt, _ = cpu_step(O, inp)
+        dt, _ = cpu_step(O, ws, inp)
         total += dt
         reps += 1
-    _, tr = cpu_step(O, inp, traffic=True)
+    _, tr = cpu_step(O, ws, inp, traffic=True)
     return {
-        "value": round(sample_ops() * reps / total / 1e6, 3),
+        "value": round(ws.ops * reps / total / 1e6, 3),
         "unit": "Mops/s",
         "cores": 1,
         "kind": "port",
-        "sample": f"the same step at 1/{SAMPLE_DIV} scale (2^20 slots, 500K pairs in 5x100K inserts, 500K gets, "
-                  f"50K removes; same load factors), sequential C oracle, {reps} reps in {total:.1f} s",
+        "sample": f"the same step at 1/{SAMPLE_DIV} scale ({ws.cap} slots, {ws.pairs} pairs in calls of {CALL}, "
+                  f"{ws.gets} gets, {ws.removes} removes; same load factors), sequential C oracle, "
+                  f"{reps} reps in {total:.1f} s",
     }, bytes_per_op(tr)
 
 
-def reference_arm(args):
+def reference_arm(args, w):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -150,20 +175,22 @@ def reference_arm(args):
     import oracle as O
 
     threads = os.cpu_count() or 1
-    inp = cpu_sample_inputs()
+    ws = w.scaled(SAMPLE_DIV)
+    inp = cpu_sample_inputs(ws)
     for _ in range(args.warmup):
-        cpu_step(O, inp, threads=threads)
-    times = [cpu_step(O, inp, threads=threads)[0] for _ in range(args.steps)]
+        cpu_step(O, ws, inp, threads=threads)
+    times = [cpu_step(O, ws, inp, threads=threads)[0] for _ in range(args.steps)]
     total = sum(times)
-    v = sample_ops() * len(times) / total / 1e6
+    v = ws.ops * len(times) / total / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "Mops/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / len(times) * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": dict(workload_desc(), parallelism="host threads"),
+        "config": dict(w.desc(), parallelism="host threads"),
         "cpu_baseline": {"value": round(v, 3), "unit": "Mops/s", "cores": threads, "kind": "port",
-                         "sample": f"the step at 1/{SAMPLE_DIV} scale; multithreaded CAS restatement of "
-                                   "src/rayon_cpu.rs (the reference's Rust crate cannot be built here)"},
+                         "sample": f"the step at 1/{SAMPLE_DIV} scale ({ws.cap} slots, {ws.pairs} pairs); "
+                                   "multithreaded CAS restatement of src/rayon_cpu.rs (the reference's Rust "
+                                   "crate cannot be built here)"},
         "e2e": {"value": round(v, 3), "unit": "Mops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -223,17 +250,174 @@ class Clocks:
                 "samples": len(rows)}
 
 
-def gpu_inputs(torch, dev, seed=3):
+def gpu_inputs(torch, dev, w, seed=3):
     g = torch.Generator(device=dev)
     g.manual_seed(seed)
-    keys = torch.randint(0, 256, (N_PAIRS, KB), dtype=torch.uint8, device=dev, generator=g)
-    vals = torch.randint(0, 256, (N_PAIRS, VB), dtype=torch.uint8, device=dev, generator=g)
-    hit = torch.randperm(N_PAIRS, device=dev, generator=g)[: N_GET // 2]
-    fresh = torch.randint(0, 256, (N_GET - N_GET // 2, KB), dtype=torch.uint8, device=dev, generator=g)
+    keys = torch.randint(0, 256, (w.pairs, KB), dtype=torch.uint8, device=dev, generator=g)
+    vals = torch.randint(0, 256, (w.pairs, VB), dtype=torch.uint8, device=dev, generator=g)
+    hit = torch.randperm(w.pairs, device=dev, generator=g)[: w.gets // 2]
+    fresh = torch.randint(0, 256, (w.gets - w.gets // 2, KB), dtype=torch.uint8, device=dev, generator=g)
     q = torch.cat([keys[hit], fresh])
-    q = q[torch.randperm(N_GET, device=dev, generator=g)].contiguous()
-    rem = keys[torch.randperm(N_PAIRS, device=dev, generator=g)[:N_REM]].contiguous()
+    q = q[torch.randperm(w.gets, device=dev, generator=g)].contiguous()
+    rem = keys[torch.randperm(w.pairs, device=dev, generator=g)[:w.removes]].contiguous()
     return keys, vals, q, rem
+
+
+INSERT_KERNELS = ("k_ins_p1", "k_ins_p2", "k_ins_p3", "k_ins_p4", "k_ins_tail", "k_ins_serial")
+REMOVE_KERNELS = ("k_rem_p1", "k_rem_p2", "k_rem_p3", "k_rem_tail")
+
+# DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum) per op of
+# each kernel set, from captures of the same kernels on a 2^22-slot table at
+# the same load factor and call size (the traffic summary under
+# profiles/ gives the command and the per-kernel figures); traffic grows with
+# the ops processed.
+NCU_TRAFFIC_PER_OP = {"insert": 1275.6, "get": 330.4, "remove": 846.3}
+
+
+class DeviceRun:
+    """Times one workload's step on one GPU through the device-pointer API."""
+
+    def __init__(self, torch, F, dev, stream, w, local):
+        self.torch, self.w, self.stream = torch, w, stream
+        self.keys, self.vals, self.q, self.rem = gpu_inputs(torch, dev, w)
+        self.out_v = torch.empty((w.gets, VB), dtype=torch.uint8, device=dev)
+        self.out_f = torch.empty((w.gets,), dtype=torch.uint8, device=dev)
+        self.m = F.FlashMap(w.cap_req, KB, VB, F.HashStrategy.Identity, local)
+
+    def step(self, ev=None):
+        w, m, s = self.w, self.m, self.stream
+        m.clear()
+        for b in range(0, w.pairs, CALL):
+            n = min(CALL, w.pairs - b)
+            m.bulk_insert_device(self.keys[b:b + n], self.vals[b:b + n], n, s)
+        if ev:
+            ev[0].record(s)
+        m.bulk_get_device(self.q, w.gets, self.out_v, self.out_f, s)
+        if ev:
+            ev[1].record(s)
+        m.bulk_remove_device(self.rem, w.removes, s)
+
+    def check(self):
+        assert self.m.len() == self.w.pairs - self.w.removes, self.m.len()
+        assert int(self.out_f.sum().item()) == self.w.gets // 2
+
+    def timed(self, steps, barrier, native):
+        torch, s = self.torch, self.stream
+        Ev = torch.cuda.Event
+        phase = [(Ev(enable_timing=True), Ev(enable_timing=True)) for _ in range(steps)]
+        starts = [Ev(enable_timing=True) for _ in range(steps)]
+        ends = [Ev(enable_timing=True) for _ in range(steps)]
+        t0, t1 = Ev(enable_timing=True), Ev(enable_timing=True)
+        l0 = native.launch_count()
+        barrier()
+        torch.cuda.synchronize()
+        t0.record(s)
+        for k in range(steps):
+            starts[k].record(s)
+            self.step(phase[k])
+            ends[k].record(s)
+        t1.record(s)
+        torch.cuda.synchronize()
+        barrier()
+        return {
+            "total_ms": t0.elapsed_time(t1),
+            "launches": native.launch_count() - l0,
+            "ins_ms": statistics.median(starts[k].elapsed_time(phase[k][0]) for k in range(steps)),
+            "get_ms": statistics.median(phase[k][0].elapsed_time(phase[k][1]) for k in range(steps)),
+            "rem_ms": statistics.median(phase[k][1].elapsed_time(ends[k]) for k in range(steps)),
+        }
+
+    def kernel_pass(self, nvtx=False):
+        """One more step with the library's per-kernel CUDA events on.  With
+        nvtx, the middle insert call of the step and its bulk_get sit in NVTX
+        ranges "insert_call" and "get_call" (for ncu --nvtx-include)."""
+        self.m.kernel_timing(True, reset=True)
+        if nvtx:
+            w, m, s, nv = self.w, self.m, self.stream, self.torch.cuda.nvtx
+            m.clear()
+            mid = (w.pairs // CALL // 2) * CALL
+            for b in range(0, w.pairs, CALL):
+                n = min(CALL, w.pairs - b)
+                if b == mid:
+                    nv.range_push("insert_call")
+                m.bulk_insert_device(self.keys[b:b + n], self.vals[b:b + n], n, s)
+                if b == mid:
+                    self.torch.cuda.synchronize()
+                    nv.range_pop()
+            nv.range_push("get_call")
+            m.bulk_get_device(self.q, w.gets, self.out_v, self.out_f, s)
+            self.torch.cuda.synchronize()
+            nv.range_pop()
+            m.bulk_remove_device(self.rem, w.removes, s)
+        else:
+            self.step()
+        self.torch.cuda.synchronize()
+        kt = self.m.kernel_times()
+        self.m.kernel_timing(False)
+        return kt
+
+    def ops(self, t):
+        w = self.w
+        return {"insert_mops": round(w.pairs / t["ins_ms"] / 1e3, 3), "get_mops": round(w.gets / t["get_ms"] / 1e3, 3),
+                "remove_mops": round(w.removes / t["rem_ms"] / 1e3, 3), "insert_ms": round(t["ins_ms"], 3),
+                "get_ms": round(t["get_ms"], 3), "remove_ms": round(t["rem_ms"], 3)}
+
+    def e2e(self, steps, barrier, dist, world):
+        torch, w, m = self.torch, self.w, self.m
+        hk = self.keys.cpu().pin_memory().numpy()
+        hv = self.vals.cpu().pin_memory().numpy()
+        hq = self.q.cpu().pin_memory().numpy()
+        hr = self.rem.cpu().pin_memory().numpy()
+        ho = torch.empty((w.gets, VB), dtype=torch.uint8).pin_memory().numpy()
+        hf = torch.empty((w.gets,), dtype=torch.uint8).pin_memory().numpy()
+
+        def step_host():
+            m.clear()
+            for b in range(0, w.pairs, CALL):
+                m.bulk_insert(hk[b:b + CALL], hv[b:b + CALL])
+            m.bulk_get(hq, out_values=ho, out_found=hf)
+            m.bulk_remove(hr)
+
+        step_host()
+        assert int(hf.sum()) == w.gets // 2
+        n = max(1, min(steps, 3))
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            step_host()
+        torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - t0) / n
+        if dist is not None:
+            t = torch.tensor([e2e_s], device=self.q.device)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        calls = (w.pairs + CALL - 1) // CALL
+        return {"value": round(w.ops * world / e2e_s / 1e6, 3), "unit": "Mops/s",
+                "h2d_bytes_per_step": w.pairs * (KB + VB) + w.gets * KB + w.removes * KB,
+                "d2h_bytes_per_step": w.gets * (VB + 1) + 8 * (calls + 1),
+                "ms_per_step": round(e2e_s * 1e3, 3)}
+
+
+def kernel_summary(kt, w):
+    total = sum(v[0] for v in kt.values()) or 1.0
+    return {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / total, 4)}
+            for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}
+
+
+def roofline_for(kt, names, nops, bpo, peak, kind, label, traffic_per_op):
+    ms = sum(kt[k][0] for k in names if k in kt)
+    launches = sum(kt[k][1] for k in names if k in kt)
+    if ms <= 0:
+        return None
+    achieved = bpo * nops / (ms / 1e3) / 1e9
+    return {"kernel": label, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": kind,
+            "algorithmic_bytes_per_op": round(bpo, 2), "ops": nops, "kernel_ms": round(ms, 3),
+            "launches": launches,
+            "traffic": None if traffic_per_op is None else round(traffic_per_op * nops / max(launches, 1)),
+            "traffic_per_op": traffic_per_op,
+            "traffic_unit": "bytes per launch (ncu dram bytes per op, small case, x ops per launch)"}
 
 
 def main():
@@ -244,19 +428,19 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-as-written", action="store_true", help="skip the load-0.477 variant")
+    ap.add_argument("--nvtx", action="store_true",
+                    help="mark one insert call and the bulk_get of the kernel-timing step with NVTX ranges")
     ap.add_argument("--scale", type=int, default=1,
                     help="divide the table and batch counts by this power of two (same call size and load "
                          "factors; for profiling captures on a small case)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    main_w, alt_w = LOAD08, AS_WRITTEN
     if args.scale > 1:
-        global CAP_REQ, N_PAIRS, N_GET, N_REM
-        CAP_REQ //= args.scale
-        N_PAIRS //= args.scale
-        N_GET //= args.scale
-        N_REM //= args.scale
+        main_w, alt_w = main_w.scaled(args.scale), alt_w.scaled(args.scale)
     if args.impl == "reference":
-        return reference_arm(args)
+        return reference_arm(args, main_w)
 
     import torch
 
@@ -281,126 +465,72 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    keys, vals, q, rem = gpu_inputs(torch, dev)
-    out_v = torch.empty((N_GET, VB), dtype=torch.uint8, device=dev)
-    out_f = torch.empty((N_GET,), dtype=torch.uint8, device=dev)
-    m = F.FlashMap(CAP_REQ, KB, VB, F.HashStrategy.Identity, local)
     stream = torch.cuda.current_stream(dev)
-    Ev = torch.cuda.Event
-
-    def step(ev=None):
-        m.clear()
-        for b in range(0, N_PAIRS, CALL):
-            m.bulk_insert_device(keys[b:b + CALL], vals[b:b + CALL], CALL, stream)
-        if ev:
-            ev[0].record(stream)
-        m.bulk_get_device(q, N_GET, out_v, out_f, stream)
-        if ev:
-            ev[1].record(stream)
-        m.bulk_remove_device(rem, N_REM, stream)
-
-    phase = [(Ev(enable_timing=True), Ev(enable_timing=True)) for _ in range(args.steps)]
-    starts = [Ev(enable_timing=True) for _ in range(args.steps)]
-    ends = [Ev(enable_timing=True) for _ in range(args.steps)]
-    t_all0, t_all1 = Ev(enable_timing=True), Ev(enable_timing=True)
+    run = DeviceRun(torch, F, dev, stream, main_w, local)
     with Clocks(local) as clk:  # sampled from the warm-up on, through the timed steps
         for _ in range(args.warmup):
-            step()
+            run.step()
         torch.cuda.synchronize()
-        # correctness guard on the timed workload (not a parity test)
-        assert m.len() == N_PAIRS - N_REM, m.len()
-        assert int(out_f.sum().item()) == N_GET // 2
-        l0 = _native.launch_count()
-        barrier()
-        torch.cuda.synchronize()
-        t_all0.record(stream)
-        for k in range(args.steps):
-            starts[k].record(stream)
-            step(phase[k])
-            ends[k].record(stream)
-        t_all1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-    launches = _native.launch_count() - l0
-    total_ms = t_all0.elapsed_time(t_all1)
-    ins_ms = statistics.median(starts[k].elapsed_time(phase[k][0]) for k in range(args.steps))
-    get_ms = statistics.median(phase[k][0].elapsed_time(phase[k][1]) for k in range(args.steps))
-    rem_ms = statistics.median(phase[k][1].elapsed_time(ends[k]) for k in range(args.steps))
+        run.check()  # correctness guard on the timed workload (not a parity test)
+        t = run.timed(args.steps, barrier, _native)
+    total_ms = t["total_ms"]
     if dist is not None:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ops_step = N_PAIRS + N_GET + N_REM
+        tt = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
     ms_step = total_ms / args.steps
-    value = ops_step * world / (ms_step / 1e3) / 1e6
-
-    # ---- end to end through the host API (pinned host buffers) ----------
-    def run_e2e():
-        hk = keys.cpu().pin_memory().numpy()
-        hv = vals.cpu().pin_memory().numpy()
-        hq = q.cpu().pin_memory().numpy()
-        hr = rem.cpu().pin_memory().numpy()
-        ho = torch.empty((N_GET, VB), dtype=torch.uint8).pin_memory().numpy()
-        hf = torch.empty((N_GET,), dtype=torch.uint8).pin_memory().numpy()
-
-        def step_host():
-            m.clear()
-            for b in range(0, N_PAIRS, CALL):
-                m.bulk_insert(hk[b:b + CALL], hv[b:b + CALL])
-            m.bulk_get(hq, out_values=ho, out_found=hf)
-            m.bulk_remove(hr)
-
-        for _ in range(1):
-            step_host()
-        assert int(hf.sum()) == N_GET // 2
-        e2e_steps = max(1, min(args.steps, 3))
-        barrier()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(e2e_steps):
-            step_host()
-        torch.cuda.synchronize()
-        e2e_s = (time.perf_counter() - t0) / e2e_steps
-        if dist is not None:
-            t = torch.tensor([e2e_s], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e = {"value": round(ops_step * world / e2e_s / 1e6, 3), "unit": "Mops/s",
-               "h2d_bytes_per_step": N_PAIRS * (KB + VB) + N_GET * KB + N_REM * KB,
-               "d2h_bytes_per_step": N_GET * (VB + 1) + 8 * (N_PAIRS // CALL + 1),
-               "ms_per_step": round(e2e_s * 1e3, 3)}
-        return e2e
-
-    e2e = None if args.no_e2e else run_e2e()
+    value = main_w.ops * world / (ms_step / 1e3) / 1e6
+    kt = run.kernel_pass(args.nvtx)
+    e2e = None if args.no_e2e else run.e2e(args.steps, barrier, dist, world)
 
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Mops/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded uniform random bytes)",
-        "config": dict(workload_desc(), parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
-        "ops": {"insert_mops": round(N_PAIRS / ins_ms / 1e3, 3), "get_mops": round(N_GET / get_ms / 1e3, 3),
-                "remove_mops": round(N_REM / rem_ms / 1e3, 3), "insert_ms": round(ins_ms, 3),
-                "get_ms": round(get_ms, 3), "remove_ms": round(rem_ms, 3)},
-        "gpu_launches": int(launches),
+        "config": dict(main_w.desc(), parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+        "ops": run.ops(t),
+        "gpu_launches": int(t["launches"]),
+        "kernels": kernel_summary(kt, main_w),
     }
     if e2e:
         line["e2e"] = e2e
     clk_sum = clk.summary()
     if clk_sum:
         line["clocks"] = clk_sum
+    run.m.close()
+    del run
+    torch.cuda.empty_cache()
+
+    if not args.no_as_written:
+        alt = DeviceRun(torch, F, dev, stream, alt_w, local)
+        for _ in range(args.warmup):
+            alt.step()
+        torch.cuda.synchronize()
+        alt.check()
+        ta = alt.timed(args.steps, barrier, _native)
+        line["as_written"] = {"config": alt_w.desc(),
+                              "value": round(alt_w.ops * world / (ta["total_ms"] / args.steps / 1e3) / 1e6, 3),
+                              "ms_per_step": round(ta["total_ms"] / args.steps, 4), "ops": alt.ops(ta)}
+        alt.m.close()
+        del alt
+
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb, bpo = cpu_baseline_leg()
+        cb, bpo = cpu_baseline_leg(main_w)
         line["cpu_baseline"] = cb
         peak, kind = read_peak()
-        achieved = bpo["get"] * N_GET / (get_ms / 1e3) / 1e9
-        line["roofline"] = {"kernel": "k_get<32,128,8> (bulk_get, one launch of 8M queries)", "bound": "hbm",
-                            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                            "frac": round(achieved / peak, 4), "peak_kind": kind,
-                            "algorithmic_bytes_per_query": round(bpo["get"], 2), "traffic": None}
+        line["roofline"] = roofline_for(
+            kt, INSERT_KERNELS, main_w.pairs, bpo["insert"], peak, kind,
+            "bulk_insert kernel set (k_ins_p1..p4 per round + k_ins_tail, every call of the step; the step's "
+            "largest device-time share)", NCU_TRAFFIC_PER_OP["insert"])
+        line["roofline_get"] = roofline_for(
+            kt, ("k_get",), main_w.gets, bpo["get"], peak, kind, "k_get_thread<32,128> (one launch of all gets)",
+            NCU_TRAFFIC_PER_OP["get"])
+        line["roofline_remove"] = roofline_for(
+            kt, REMOVE_KERNELS, main_w.removes, bpo["remove"], peak, kind, "bulk_remove kernel set",
+            NCU_TRAFFIC_PER_OP["remove"])
         line["algorithmic_bytes_per_op"] = {k: round(v, 2) for k, v in bpo.items()}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    m.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -66,7 +66,79 @@ cudaError_t grow(T*& p, size_t& cap, size_t need) {
 
 bool aligned(const void* p, uintptr_t a) { return ((uintptr_t)p % a) == 0; }
 
+// Per-table kernel timing: event pairs recorded around each launch while on,
+// read back and summed per kernel class by fm_kernel_times.
+struct KTimer {
+    std::mutex mu;
+    bool on = false;
+    struct Rec {
+        int cls;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> spare;
+    double ms[fm::KC_N] = {};
+    uint64_t launches[fm::KC_N] = {};
+
+    cudaEvent_t take() {
+        if (!spare.empty()) {
+            cudaEvent_t e = spare.back();
+            spare.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        return cudaEventCreate(&e) == cudaSuccess ? e : nullptr;
+    }
+    cudaError_t collect() {
+        cudaError_t err = cudaSuccess;
+        for (const Rec& r : recs) {
+            float x = 0.f;
+            cudaError_t e = cudaEventSynchronize(r.b);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&x, r.a, r.b);
+            if (e == cudaSuccess) {
+                ms[r.cls] += x;
+                launches[r.cls] += 1;
+            } else if (err == cudaSuccess) {
+                err = e;
+            }
+            spare.push_back(r.a);
+            spare.push_back(r.b);
+        }
+        recs.clear();
+        return err;
+    }
+    ~KTimer() {
+        for (const Rec& r : recs) cudaEventDestroy(r.a), cudaEventDestroy(r.b);
+        for (cudaEvent_t e : spare) cudaEventDestroy(e);
+    }
+};
+
+thread_local KTimer* tl_timer = nullptr;
+thread_local cudaEvent_t tl_open[fm::KC_N] = {};
+
 }  // namespace
+
+void fm::kt_mark(int cls, bool begin, cudaStream_t s) {
+    KTimer* k = tl_timer;
+    if (!k || cls < 0 || cls >= KC_N) return;
+    std::lock_guard<std::mutex> g(k->mu);
+    if (begin) {
+        cudaEvent_t e = k->take();
+        if (e && cudaEventRecord(e, s) == cudaSuccess) tl_open[cls] = e;
+        else if (e) k->spare.push_back(e);
+        return;
+    }
+    cudaEvent_t a = tl_open[cls];
+    tl_open[cls] = nullptr;
+    if (!a) return;
+    cudaEvent_t b = k->take();
+    if (b && cudaEventRecord(b, s) == cudaSuccess) {
+        k->recs.push_back({cls, a, b});
+    } else {
+        k->spare.push_back(a);
+        if (b) k->spare.push_back(b);
+    }
+}
 
 struct fm_table {
     int device = 0;
@@ -91,6 +163,7 @@ struct fm_table {
     size_t d_in_cap = 0;
     std::mutex pool_mu;
     std::vector<GetCtx*> pool;
+    KTimer timer;
 
     fm::TableView view() const {
         fm::TableView v;
@@ -117,6 +190,13 @@ struct fm_table {
 };
 
 namespace {
+
+// Makes the table's timer current on this thread for one API call.
+struct TimerScope {
+    KTimer* prev;
+    explicit TimerScope(fm_table* t) : prev(tl_timer) { tl_timer = (t && t->timer.on) ? &t->timer : nullptr; }
+    ~TimerScope() { tl_timer = prev; }
+};
 
 int ensure_scratch(fm_table* t, uint64_t n) {
     if (t->sc.cap_ops >= n) return FM_OK;
@@ -363,6 +443,7 @@ int fm_bulk_get(fm_table* t, const void* keys, uint64_t n, void* out_values, uin
     if (n == 0) return FM_OK;
     if (!keys || (!out_values && t->vsz) || !out_found) return fail(FM_ERR_INVALID_ARG, "NULL buffer");
     DeviceGuard dg(t->device);
+    TimerScope ts(t);
     GetCtx* c = acquire_ctx(t);
     if (!c) return fail(FM_ERR_CUDA_INIT, "stream creation failed");
     const size_t kb = (size_t)n * t->ksz, vb = (size_t)n * t->vsz;
@@ -411,6 +492,7 @@ int fm_bulk_insert(fm_table* t, const void* keys, const void* values, uint64_t n
     int rc = precheck(t, n);
     if (rc) return rc;
     DeviceGuard dg(t->device);
+    TimerScope ts(t);
     const size_t kb = (size_t)n * t->ksz, vb = (size_t)n * t->vsz;
     const size_t off_v = (kb + 255) & ~(size_t)255;
     cudaError_t e = grow(t->d_in, t->d_in_cap, off_v + vb + 1);
@@ -435,6 +517,7 @@ int fm_bulk_remove(fm_table* t, const void* keys, uint64_t n, uint64_t* num_remo
     if (!keys) return fail(FM_ERR_INVALID_ARG, "NULL buffer");
     std::lock_guard<std::mutex> g(t->mu);
     DeviceGuard dg(t->device);
+    TimerScope ts(t);
     const size_t kb = (size_t)n * t->ksz;
     cudaError_t e = grow(t->d_in, t->d_in_cap, kb + 1);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_GPU_ALLOC, "remove buffers", e);
@@ -467,6 +550,7 @@ int fm_bulk_get_device(fm_table* t, const void* d_keys, uint64_t n, void* d_out_
     if (n == 0) return FM_OK;
     if (!d_keys || (!d_out_values && t->vsz)) return fail(FM_ERR_INVALID_ARG, "NULL buffer");
     DeviceGuard dg(t->device);
+    TimerScope ts(t);
     cudaError_t e = fm::launch_get(t->view(), t->shape_for({d_keys, d_out_values}), (const uint8_t*)d_keys, n,
                                    (uint8_t*)d_out_values, d_out_found, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "bulk_get_device", e);
@@ -489,6 +573,7 @@ static int insert_device(fm_table* t, const void* d_keys, const void* d_values, 
         if (rc) return rc;
     }
     DeviceGuard dg(t->device);
+    TimerScope ts(t);
     uint64_t added = 0;
     bool limit = false;
     int rc = run_rounds(t, true, (const uint8_t*)d_keys, (const uint8_t*)d_values, n, (cudaStream_t)stream, &added,
@@ -521,6 +606,7 @@ int fm_bulk_remove_device(fm_table* t, const void* d_keys, uint64_t n, uint64_t*
     if (!d_keys) return fail(FM_ERR_INVALID_ARG, "NULL buffer");
     std::lock_guard<std::mutex> g(t->mu);
     DeviceGuard dg(t->device);
+    TimerScope ts(t);
     uint64_t removed = 0;
     bool limit = false;
     int rc = run_rounds(t, false, (const uint8_t*)d_keys, nullptr, n, (cudaStream_t)stream, &removed, &limit);
@@ -534,6 +620,7 @@ int fm_recount(fm_table* t, uint64_t* out) {
     if (!t) return fail(FM_ERR_INVALID_ARG, "table is NULL");
     std::lock_guard<std::mutex> g(t->mu);
     DeviceGuard dg(t->device);
+    TimerScope ts(t);
     cudaError_t e = cudaMemsetAsync(&t->d_ctl->occupied, 0, 8, t->stream);
     if (e == cudaSuccess) e = fm::launch_count(t->view(), t->d_ctl, t->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, t->stream);
@@ -577,6 +664,43 @@ int fm_load(fm_table* t, const uint32_t* flags, const void* keys, const void* va
     if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "load", e);
     t->len.store(len);
     return FM_OK;
+}
+
+int fm_kernel_timing(fm_table* t, int on) {
+    if (!t) return fail(FM_ERR_INVALID_ARG, "table is NULL");
+    std::lock_guard<std::mutex> g(t->timer.mu);
+    t->timer.on = on != 0;
+    return FM_OK;
+}
+
+int fm_kernel_times(fm_table* t, double* total_ms, uint64_t* launches, uint32_t n) {
+    if (!t) return fail(FM_ERR_INVALID_ARG, "table is NULL");
+    DeviceGuard dg(t->device);
+    std::lock_guard<std::mutex> g(t->timer.mu);
+    cudaError_t e = t->timer.collect();
+    for (uint32_t i = 0; i < n && i < (uint32_t)fm::KC_N; i++) {
+        if (total_ms) total_ms[i] = t->timer.ms[i];
+        if (launches) launches[i] = t->timer.launches[i];
+    }
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "kernel timing", e);
+    return FM_OK;
+}
+
+int fm_kernel_times_reset(fm_table* t) {
+    if (!t) return fail(FM_ERR_INVALID_ARG, "table is NULL");
+    DeviceGuard dg(t->device);
+    std::lock_guard<std::mutex> g(t->timer.mu);
+    cudaError_t e = t->timer.collect();
+    for (int i = 0; i < fm::KC_N; i++) t->timer.ms[i] = 0.0, t->timer.launches[i] = 0;
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "kernel timing", e);
+    return FM_OK;
+}
+
+const char* fm_kernel_class_name(uint32_t cls) {
+    static const char* names[fm::KC_N] = {"k_get",       "k_ins_p1",    "k_ins_p2",    "k_ins_p3",
+                                          "k_ins_p4",    "k_ins_tail",  "k_ins_serial", "k_rem_p1",
+                                          "k_rem_p2",    "k_rem_p3",    "k_rem_tail",  "k_count"};
+    return cls < (uint32_t)fm::KC_N ? names[cls] : nullptr;
 }
 
 }  // extern "C"
@@ -712,6 +836,7 @@ extern "C" int fm_bulk_insert_device_noalloc(fm_table* t, const void* d_keys, co
     int rc = precheck(t, n);
     if (rc) return rc;
     DeviceGuard dg(t->device);
+    TimerScope ts(t);
     uint8_t* base = nullptr;
     rc = na_setup(t->device, &base);
     if (rc) return rc;

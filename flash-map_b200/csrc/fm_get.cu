@@ -185,12 +185,14 @@ template <int KB, int VB>
 cudaError_t get_shape(const TableView& t, const uint8_t* q, uint64_t n, uint8_t* ov, uint8_t* of, cudaStream_t s) {
     if constexpr (KB != 0 && VB != 0) {
         if (t.mask >= 7) {
+            KtScope kt(KC_GET, s);
             k_get_thread<KB, VB><<<grid_for(n, 64), BLOCK, 0, s>>>(t, q, n, ov, of);
             g_launches += 1;
             return cudaGetLastError();
         }
     }
     constexpr int T = 8;
+    KtScope kt(KC_GET, s);
     k_get<KB, VB, T><<<grid_for(n * T, 16), BLOCK, 0, s>>>(t, q, n, ov, of);
     g_launches += 1;
     return cudaGetLastError();
@@ -240,6 +242,7 @@ cudaError_t launch_get(const TableView& t, Shape sh, const uint8_t* q, uint64_t 
 }
 
 cudaError_t launch_count(const TableView& t, Ctl* ctl, cudaStream_t s) {
+    KtScope kt(KC_COUNT_OCC, s);
     k_count<<<grid_for(t.mask + 1, 4), BLOCK, 0, s>>>(t.flags, t.mask + 1, ctl);
     g_launches += 1;
     return cudaGetLastError();

@@ -1092,10 +1092,22 @@ void rounds_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, 
     // what chains of dependent random reads need
     const unsigned g = grid_for(grid_ops, 8);
     for (uint32_t r = r0; r < r0 + nrounds; r++) {
-        k_ins_p1<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
-        k_ins_p2<<<g, RBLOCK, 0, s>>>(t, n0, r, nops, sc, ctl);
-        k_ins_p3<KB, VB><<<g, RBLOCK, 0, s>>>(t, keys, vals, n0, r, sc, ctl);
-        if constexpr (KB != 0 && VB != 0) k_ins_p4<KB, VB><<<g, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
+        {
+            KtScope kt(KC_INS_FIND, s);
+            k_ins_p1<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
+        }
+        {
+            KtScope kt(KC_INS_WALK, s);
+            k_ins_p2<<<g, RBLOCK, 0, s>>>(t, n0, r, nops, sc, ctl);
+        }
+        {
+            KtScope kt(KC_INS_EXEC, s);
+            k_ins_p3<KB, VB><<<g, RBLOCK, 0, s>>>(t, keys, vals, n0, r, sc, ctl);
+        }
+        if constexpr (KB != 0 && VB != 0) {
+            KtScope kt(KC_INS_LONG, s);
+            k_ins_p4<KB, VB><<<g, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
+        }
     }
     count_launches((KB != 0 && VB != 0 ? 4 : 3) * nrounds);
 }
@@ -1103,6 +1115,7 @@ void rounds_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, 
 template <int KB, int VB>
 void tail_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, uint32_t r,
                 uint32_t nops, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+    KtScope kt(KC_INS_TAIL, s);
     k_ins_tail<KB, VB, (KB && VB) ? INS_T : 1><<<1, TAIL_THREADS, 0, s>>>(t, keys, vals, n0, r, nops, sc, ctl);
     count_launches(1);
 }
@@ -1110,6 +1123,7 @@ void tail_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, ui
 template <int KB, int VB>
 void serial_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, uint32_t r,
                   const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+    KtScope kt(KC_INS_SERIAL, s);
     k_ins_serial<KB, VB><<<1, 1024, 0, s>>>(t, keys, vals, n0, r, sc, ctl);
     count_launches(1);
 }

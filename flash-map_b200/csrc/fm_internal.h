@@ -91,6 +91,32 @@ cudaError_t launch_rem_tail(const TableView& t, Shape sh, const uint8_t* keys, u
 cudaError_t launch_count(const TableView& t, Ctl* ctl, cudaStream_t s);
 int num_sms();
 unsigned long long launch_count();
+
+// Optional device timing per kernel class: while a table's timing is on, the
+// library records a CUDA event pair around each launch made for it on the
+// calling thread (no events otherwise).
+enum KernelClass : int {
+    KC_GET = 0,     // k_get_thread / k_get
+    KC_INS_FIND,    // k_ins_p1: first free slot, segment registration
+    KC_INS_WALK,    // k_ins_p2: leaders and flow bounds
+    KC_INS_EXEC,    // k_ins_p3: thread-per-op execution
+    KC_INS_LONG,    // k_ins_p4: warp-per-op execution of long walks
+    KC_INS_TAIL,    // k_ins_tail: remaining rounds in one block
+    KC_INS_SERIAL,  // k_ins_serial
+    KC_REM_MARK,    // k_rem_p1
+    KC_REM_CHECK,   // k_rem_p2
+    KC_REM_EXEC,    // k_rem_p3
+    KC_REM_TAIL,    // k_rem_tail
+    KC_COUNT_OCC,   // k_count
+    KC_N
+};
+void kt_mark(int cls, bool begin, cudaStream_t s);
+struct KtScope {
+    int c;
+    cudaStream_t s;
+    KtScope(int c_, cudaStream_t s_) : c(c_), s(s_) { kt_mark(c, true, s); }
+    ~KtScope() { kt_mark(c, false, s); }
+};
 void count_launches(unsigned n);
 unsigned grid_for(uint64_t threads, unsigned per_sm);
 

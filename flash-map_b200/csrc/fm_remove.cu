@@ -224,9 +224,18 @@ void rounds_shape(const TableView& t, const uint8_t* keys, uint32_t n0, uint32_t
                   uint32_t grid_ops, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
     const unsigned g = grid_for(grid_ops, 8);
     for (uint32_t r = r0; r < r0 + nrounds; r++) {
-        k_rem_p1<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
-        k_rem_p2<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
-        k_rem_p3<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
+        {
+            KtScope kt(KC_REM_MARK, s);
+            k_rem_p1<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
+        }
+        {
+            KtScope kt(KC_REM_CHECK, s);
+            k_rem_p2<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
+        }
+        {
+            KtScope kt(KC_REM_EXEC, s);
+            k_rem_p3<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl);
+        }
     }
     count_launches(3 * nrounds);
 }
@@ -248,6 +257,7 @@ cudaError_t launch_rem_rounds(const TableView& t, Shape sh, const uint8_t* keys,
 
 cudaError_t launch_rem_tail(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, uint32_t r,
                             const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+    KtScope kt(KC_REM_TAIL, s);
     switch (sh) {
         case SHAPE_8_8:
         case SHAPE_8_32: k_rem_tail<8><<<1, TAIL_THREADS, 0, s>>>(t, keys, n0, r, sc, ctl); break;

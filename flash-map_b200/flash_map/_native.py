@@ -21,7 +21,8 @@ EXPORTS = (
     "fm_capacity", "fm_load_factor", "fm_clear", "fm_device", "fm_bulk_get_device",
     "fm_bulk_get_values_device", "fm_bulk_insert_device", "fm_bulk_insert_device_uncounted",
     "fm_bulk_remove_device", "fm_recount", "fm_last_error", "fm_launch_count", "fm_snapshot", "fm_load",
-    "fm_bulk_insert_device_noalloc",
+    "fm_bulk_insert_device_noalloc", "fm_kernel_timing", "fm_kernel_times", "fm_kernel_times_reset",
+    "fm_kernel_class_name",
 )
 
 _lock = threading.Lock()
@@ -73,6 +74,14 @@ def _declare(L) -> None:
     L.fm_snapshot.argtypes = [vp, vp, vp, vp]
     L.fm_load.restype = i32
     L.fm_load.argtypes = [vp, vp, vp, vp, u64]
+    L.fm_kernel_timing.restype = i32
+    L.fm_kernel_timing.argtypes = [vp, i32]
+    L.fm_kernel_times.restype = i32
+    L.fm_kernel_times.argtypes = [vp, C.POINTER(C.c_double), u64p, u32]
+    L.fm_kernel_times_reset.restype = i32
+    L.fm_kernel_times_reset.argtypes = [vp]
+    L.fm_kernel_class_name.restype = C.c_char_p
+    L.fm_kernel_class_name.argtypes = [u32]
 
 
 def load_library(path: str = LIB_PATH):

@@ -225,6 +225,27 @@ class FlashMap:
         self._check(self._L.fm_recount(self._h, C.byref(out)))
         return out.value
 
+    # -- per-kernel device timing (instrumentation) -------------------------
+    def kernel_timing(self, on: bool = True, reset: bool = False) -> None:
+        """Record CUDA events around this table's kernel launches while on."""
+        if reset:
+            self._check(self._L.fm_kernel_times_reset(self._h))
+        self._check(self._L.fm_kernel_timing(self._h, 1 if on else 0))
+
+    def kernel_times(self) -> dict:
+        """{kernel class: (total device ms, launches)} since the last reset;
+        waits for the recorded launches."""
+        n = 12
+        ms = (C.c_double * n)()
+        cnt = (C.c_uint64 * n)()
+        self._check(self._L.fm_kernel_times(self._h, ms, cnt, n))
+        out = {}
+        for i in range(n):
+            name = self._L.fm_kernel_class_name(i)
+            if name and cnt[i]:
+                out[name.decode()] = (ms[i], int(cnt[i]))
+        return out
+
     # -- raw table access (layout checks) -----------------------------------
     def snapshot(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
         """(flags, keys, values) of the whole table, free slots' key/value

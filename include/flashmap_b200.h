@@ -138,6 +138,18 @@ const char* fm_last_error(void);
  * has launched in the process so far, across all tables. */
 uint64_t fm_launch_count(void);
 
+/* Per-kernel device timing (no counterpart in gpu.rs).  While on, every call
+ * on the table records a CUDA event pair around each kernel it launches;
+ * fm_kernel_times waits for the recorded launches and returns, per kernel
+ * class (index < FM_KERNEL_CLASSES, named by fm_kernel_class_name), the summed
+ * device milliseconds and the launch count since the last reset.  Off by
+ * default: no events are recorded then. */
+#define FM_KERNEL_CLASSES 12u
+int fm_kernel_timing(fm_table* t, int on);
+int fm_kernel_times(fm_table* t, double* total_ms, uint64_t* launches, uint32_t n);
+int fm_kernel_times_reset(fm_table* t);
+const char* fm_kernel_class_name(uint32_t cls);
+
 /* Raw table access for layout checks and for loading a prefilled table:
  * flags (capacity u32), keys (capacity*K bytes), values (capacity*V bytes),
  * all host pointers; any may be NULL to skip it. */
