@@ -329,13 +329,14 @@ class DeviceRun:
 
     def kernel_pass(self, nvtx=False):
         """One more step with the library's per-kernel CUDA events on.  With
-        nvtx, the middle insert call of the step and its bulk_get sit in NVTX
-        ranges "insert_call" and "get_call" (for ncu --nvtx-include)."""
+        nvtx, the last full insert call of the step (the highest load) and
+        its bulk_get sit in NVTX ranges "insert_call" and "get_call" (for ncu
+        --nvtx-include)."""
         self.m.kernel_timing(True, reset=True)
         if nvtx:
             w, m, s, nv = self.w, self.m, self.stream, self.torch.cuda.nvtx
             m.clear()
-            mid = (w.pairs // CALL // 2) * CALL
+            mid = (w.pairs // CALL - 1) * CALL
             for b in range(0, w.pairs, CALL):
                 n = min(CALL, w.pairs - b)
                 if b == mid:

@@ -27,6 +27,7 @@
 // TAIL_MAX ops are left.  The host reads the control block once per pass.
 // Grid kernels aggregate list appends and counts per block so no address
 // takes more than one atomic per block.
+#include <climits>
 #include <type_traits>
 
 #include "fm_rounds.cuh"
@@ -569,20 +570,45 @@ __device__ void serial_process(const TableView& t, const uint8_t* keys, const ui
 }
 
 
-// ---- tile-cooperative probe and execute (compile-time shapes) -------------
+// ---- tile-cooperative execute (compile-time shapes) -----------------------
 //
-// A tile of T lanes reads T consecutive metadata words per step (T = 8: one
-// 32-byte sector).  The walk of an insert is decided by the metadata alone
-// except for key equality, so the tile computes the whole Robin Hood chain
-// (eviction slots P_0 < P_1 < ... and the end: claim, update or drop) with
-// ballots over the window, checks the possible updates (slots whose stored
-// distance equals the carried entry's probe depth) with parallel key
-// compares, and only then moves data: slot P_i receives the entry evicted at
-// P_(i-1) (P_0 the new entry), the end slot the last evicted one.  Sources are
-// read before destinations are written, highest move first, so the moves are
-// the sequential walk's writes in one pass.
+// A tile of T lanes runs one insert whose walk is too long for one thread.
+//
+// The walk in closed form.  Write the carried entry's state as its home
+// H = position - depth.  At an OCCUPIED slot holding a resident with home
+// h = position - dist: dist == depth is h == H (a possible update), and
+// depth > dist is h > H (an eviction, after which the carried entry is that
+// resident, so H becomes h); otherwise the walk moves on with H unchanged.
+// So H is the running maximum of the residents' homes from the op's own home
+// on, the evictions are the slots whose home exceeds the running maximum
+// before them, the possible updates those whose home equals it, and the walk
+// ends at the first EMPTY/TOMBSTONE slot or where position - H passes the
+// capacity (drop).  A tile reads 4T slots per round trip (one 16-byte load
+// per lane) and classifies them with one max-scan, one count-scan and
+// ballots, whatever the number of evictions.
+//
+// Then: the possible updates of each window are compared before the next
+// window is read (the first equal key, in walk order, ends the walk as an
+// in-place update), and the records move highest first in batches of round
+// trips -- the end slot gets the entry evicted at P_(k-1), P_i the one
+// evicted at P_(i-1), P_0 the new entry -- sources read before their slots
+// are written.  The tile keeps up to TMAXCH eviction slots; a longer chain's
+// last chunk is moved first, then each earlier piece of the chain is found
+// again by a walk from home (slots before a piece's end are untouched by the
+// later moves) and moved, last to first.
 
-constexpr int MAXCH = 48;  // eviction chain kept per tile; longer chains run the scalar walk
+constexpr int TMAXCH = 256;  // eviction slots held per tile
+constexpr int TMAXC = 128;   // possible updates of one window (>= 4T)
+constexpr uint32_t NOSRC = 0xFFFFFFFFu;
+
+struct TileChain {
+    uint32_t pos[TMAXCH];   // eviction slots of the current chunk
+    uint32_t p[TMAXCH];     // depth stored at each of them
+    uint32_t cpos[TMAXC];   // possible updates of the current window: slot,
+    uint32_t cstage[TMAXC]; //   evictions before it,
+    uint32_t csrc[TMAXC];   //   slot holding the carried key (NOSRC: the new key)
+    uint32_t src_base;      // slot evicted just before the chunk's first stage
+};
 
 template <int T>
 __device__ __forceinline__ uint64_t find_free_tile(const TableView& t, uint64_t h, const Tile<T>& tl) {
@@ -621,117 +647,61 @@ __device__ __forceinline__ Ch key_chunk(const RegKey<KB>& key, int c) {
     return x;
 }
 
-template <int KB, int VB, int T>
-__device__ __forceinline__ void exec_tile(const TableView& t, const RegKey<KB>& key,
-                                          const uint8_t* __restrict__ vals_in, uint32_t j, const Tile<T>& tl,
-                                          uint64_t* s_pos, uint32_t* s_p, ExecAcc& a) {
+// Inclusive scans over the T lanes of a tile.
+template <int T>
+__device__ __forceinline__ uint32_t tile_sum(uint32_t v, const Tile<T>& tl) {
+#pragma unroll
+    for (int d = 1; d < T; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(tl.wmask, v, d, T);
+        if ((int)tl.lane >= d) v += o;
+    }
+    return v;
+}
+template <int T>
+__device__ __forceinline__ long long tile_max(long long v, const Tile<T>& tl) {
+#pragma unroll
+    for (int d = 1; d < T; d <<= 1) {
+        const long long o = __shfl_up_sync(tl.wmask, v, d, T);
+        if ((int)tl.lane >= d) v = max(v, o);
+    }
+    return v;
+}
+
+// Record moves m = hi down to lo (absolute stage numbers, lo >= chunk_base)
+// of a chain whose stages from chunk_base sit in s.pos: move m writes
+// dest(m) = P_m (m < k) or the end slot (m == k) from source(m) = P_(m-1), the
+// slot `src_base` for m == chunk_base > 0, or the new entry for m == 0.  MB
+// moves per round trip, every lane holding up to CPL chunks.
+template <int KB, int VB, int T, int CPL>
+__device__ __forceinline__ void tile_moves(const TableView& t, const RegKey<KB>& key, const uint8_t* vin,
+                                           const TileChain& s, uint32_t chunk_base, int hi, int lo, uint32_t k,
+                                           int kind, uint64_t end_slot, uint32_t src_base, const Tile<T>& tl) {
     using CO = ChunkOf<KB, VB>;
     using Ch = typename CO::type;
     constexpr int CK = CO::CK, NK = CO::NK, NC = CO::NC;
-    constexpr int MB = (4 * T) / NC > 0 ? (4 * T) / NC : 1;  // moves per batch (<= 4 chunks per lane)
-    constexpr int CPL = (MB * NC + T - 1) / T;
-    const uint64_t mask = t.mask;
+    constexpr int MB = (CPL * T) / NC > 0 ? (CPL * T) / NC : 1;
+    constexpr int CL = (MB * NC + T - 1) / T;
     const uint32_t lane = tl.lane;
-    const uint64_t h = key.hash(KB, t.hash_mode) & mask;
-
-    // -- walk: metadata only, plus key compares at possible updates ----------
-    uint64_t sstart = h, pstart = 0;
-    uint32_t stage = 0;
-    int kind = 0;  // 1 claim, 2 update, 3 drop, 4 chain too long
-    uint64_t end_pos = 0, end_p = 0;
-    bool end_tomb = false;
-    uint64_t wb = h & ~(uint64_t)(T - 1);
-    while (kind == 0) {
-        const uint64_t pos = wb + lane;
-        const uint32_t f = t.flags[pos & mask];
-        for (;;) {
-            const bool in = pos >= sstart;
-            const uint64_t q = pstart + (pos - sstart);
-            const uint32_t st = st_of(f);
-            const bool drop = in && q > mask;
-            const bool occ = in && !drop && st == ST_OCC;
-            const bool ev_l = drop || (in && !drop && (st == ST_EMPTY || st == ST_TOMB)) || (occ && q > dist_of(f));
-            const uint32_t em = tl.ballot(ev_l);
-            const uint32_t elane = em ? (uint32_t)(__ffs(em) - 1) : (uint32_t)T;
-            bool match = false;
-            if (occ && lane < elane && dist_matches(f, q)) {
-                const uint8_t* sk = t.keys + (pos & mask) * KB;
-                if (stage == 0) {
-                    match = key.eq(sk, KB);
-                } else {
-                    RegKey<KB> ck;  // the carried entry's key, still at its old slot
-                    ck.load_table(t.keys + (s_pos[stage - 1] & mask) * KB, KB);
-                    match = ck.eq(sk, KB);
-                }
-            }
-            const uint32_t mm = tl.ballot(match);
-            if (mm) {
-                kind = 2;
-                end_pos = wb + __ffs(mm) - 1;
-                break;
-            }
-            if (!em) break;
-            const uint64_t epos = wb + elane;
-            const uint32_t ef = tl.shfl(f, elane);
-            const uint64_t eq = pstart + (epos - sstart);
-            if (eq > mask) {
-                kind = 3;
-                break;
-            }
-            if (st_of(ef) == ST_EMPTY || st_of(ef) == ST_TOMB) {
-                kind = 1;
-                end_pos = epos;
-                end_p = eq;
-                end_tomb = st_of(ef) == ST_TOMB;
-                break;
-            }
-            if (stage >= (uint32_t)MAXCH) {
-                kind = 4;
-                break;
-            }
-            if (lane == 0) {
-                s_pos[stage] = epos;
-                s_p[stage] = (uint32_t)min(eq, (uint64_t)0xFFFFFFFFu);
-            }
-            tl.sync();
-            ++stage;
-            sstart = epos + 1;
-            pstart = dist_of(ef) + 1;
-        }
-        wb += T;
-    }
-    if (kind == 4) {  // very long chain: the sequential walk, on lane 0
-        if (lane == 0) a.claimed += exec_insert_key<KB, VB>(t, key, vals_in + (uint64_t)j * VB, a);
-        tl.sync();
-        return;
-    }
-    tl.sync();
-
-    // -- moves: move m puts the entry of source(m) into dest(m) ---------------
-    // m < stage: dest P_m; m == stage: dest = end slot (claim: whole entry;
-    // update: value only; drop: no such move).  source(0) = the new entry,
-    // source(m) = P_(m-1).
-    const uint32_t k = stage;
-    const int M = (kind == 3) ? (int)k : (int)k + 1;
-    for (int hi = M - 1; hi >= 0; hi -= MB) {
-        const int lo = hi - MB + 1 > 0 ? hi - MB + 1 : 0;
-        const int nchunks = (hi - lo + 1) * NC;
-        Ch buf[CPL];
+    for (int top = hi; top >= lo; top -= MB) {
+        const int bot = top - MB + 1 > lo ? top - MB + 1 : lo;
+        const int nchunks = (top - bot + 1) * NC;
+        Ch buf[CL];
 #pragma unroll
-        for (int u = 0; u < CPL; u++) {
+        for (int u = 0; u < CL; u++) {
             const int g = (int)lane + u * T;
             if (g < nchunks) {
-                const int m = lo + g / NC, c = g % NC;
+                const int m = bot + g / NC, c = g % NC;
                 const bool value_only = (m == (int)k) && kind == 2;
                 if (value_only && c < NK) continue;
-                const uint8_t* src;
                 if (m == 0 && c < NK) {
                     buf[u] = key_chunk<KB, Ch, CK>(key, c);
                     continue;
                 }
-                if (m == 0) src = vals_in + (uint64_t)j * VB + (c - NK) * CK;
-                else {
-                    const uint64_t ss = s_pos[m - 1] & mask;
+                const uint8_t* src;
+                if (m == 0) {
+                    src = vin + (c - NK) * CK;
+                } else {
+                    const uint64_t ss = (m == (int)chunk_base) ? src_base : s.pos[m - 1 - chunk_base];
                     src = c < NK ? t.keys + ss * KB + c * CK : t.vals + ss * VB + (c - NK) * CK;
                 }
                 buf[u] = *reinterpret_cast<const Ch*>(src);
@@ -739,32 +709,245 @@ __device__ __forceinline__ void exec_tile(const TableView& t, const RegKey<KB>& 
         }
         tl.sync();
 #pragma unroll
-        for (int u = 0; u < CPL; u++) {
+        for (int u = 0; u < CL; u++) {
             const int g = (int)lane + u * T;
             if (g < nchunks) {
-                const int m = lo + g / NC, c = g % NC;
+                const int m = bot + g / NC, c = g % NC;
                 const bool value_only = (m == (int)k) && kind == 2;
                 if (value_only && c < NK) continue;
-                const uint64_t ds = ((m < (int)k) ? s_pos[m] : end_pos) & mask;
+                const uint64_t ds = (m < (int)k) ? s.pos[m - chunk_base] : end_slot;
                 uint8_t* dst = c < NK ? t.keys + ds * KB + c * CK : t.vals + ds * VB + (c - NK) * CK;
                 *reinterpret_cast<Ch*>(dst) = buf[u];
             }
         }
         tl.sync();
     }
-    // metadata of every moved entry
-    uint32_t md = 0;
-    for (uint32_t m = lane; m < k; m += T) {
-        t.flags[s_pos[m] & mask] = mk_flag(ST_OCC, s_p[m]);
-        md = max(md, min(s_p[m], DIST_MASK));
-    }
-    if (lane == 0) {
-        if (kind == 1) {
-            t.flags[end_pos & mask] = mk_flag(ST_OCC, end_p);
-            md = max(md, (uint32_t)min(end_p, (uint64_t)DIST_MASK));
-            a.claimed += 1;
-            a.tomb = a.tomb || end_tomb;
+}
+
+// Walks an insert chain from home with a tile, window by window.
+//   find: to the end of the walk, comparing each window's possible updates
+//         before reading the next; keeps the eviction slots of the last chunk
+//         (stages from chunk_base) in s.pos; returns 1 claim, 2 update,
+//         3 drop, 5 (never in a non-serial round) walk past the bound.
+//   otherwise: records the eviction slots of stages [lo, hi) and stops.
+template <int KB, int T>
+__device__ int tile_walk(const TableView& t, const RegKey<KB>& key, TileChain& s, const Tile<T>& tl, bool find,
+                         uint32_t lo, uint32_t hi, uint32_t& k, uint32_t& chunk_base, uint32_t& src_base,
+                         uint64_t& end_slot, uint64_t& end_p, bool& end_tomb) {
+    static_assert(TMAXC >= 4 * T && TMAXCH >= 8 * T, "a window's updates and evictions must fit the buffers");
+    const uint64_t mask = t.mask;
+    const uint64_t h = key.hash(KB, t.hash_mode) & mask;
+    long long M = (long long)h;  // the carried entry's home (unwrapped positions)
+    uint32_t g = 0;              // evictions so far
+    uint32_t last_ev = NOSRC;    // slot of the last eviction
+    int kind = 0;
+    chunk_base = find ? 0 : lo;
+    src_base = NOSRC;
+    if (!find && tl.lane == 0) s.src_base = NOSRC;
+    uint64_t wb = h & ~(uint64_t)(4 * T - 1);
+    // a walk of a non-serial round ends within one pass over the table; the
+    // bound only guards against a broken invariant (reported, nothing written)
+    const uint64_t wb_end = wb + 2 * (mask + 1) + 4 * T;
+    while (kind == 0) {
+        if (wb > wb_end) {
+            kind = 5;
+            break;
         }
+        if (find && g - chunk_base > (uint32_t)(TMAXCH - 4 * T)) {  // room for this window's evictions
+            src_base = last_ev;
+            chunk_base = g;
+        }
+        const uint64_t base = wb + 4 * tl.lane;
+        const uint4 fw = *reinterpret_cast<const uint4*>(t.flags + (base & mask));
+        const uint32_t f[4] = {fw.x, fw.y, fw.z, fw.w};
+        // homes of the occupied slots on the walk, and the running maximum
+        long long hh[4];
+        long long lm = LLONG_MIN;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint64_t pos = base + i;
+            hh[i] = (pos >= h && st_of(f[i]) == ST_OCC) ? (long long)pos - (long long)dist_of(f[i]) : LLONG_MIN;
+            lm = max(lm, hh[i]);
+        }
+        const long long incl = tile_max<T>(lm, tl);
+        long long mx = __shfl_up_sync(tl.wmask, incl, 1, T);
+        mx = tl.lane == 0 ? M : max(M, mx);
+        // classify: end (free or drop), eviction, possible update
+        uint32_t endb = 0, evb = 0, cdb = 0, pend[4];
+        long long mi[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint64_t pos = base + i;
+            mi[i] = mx;
+            const uint64_t depth = (uint64_t)((long long)pos - mx);
+            pend[i] = (uint32_t)depth;
+            if (pos >= h) {
+                const uint32_t st = st_of(f[i]);
+                if (depth > mask || st == ST_EMPTY || st == ST_TOMB) endb |= 1u << i;
+                else if (hh[i] > mx) evb |= 1u << i;
+                else if (hh[i] == mx) cdb |= 1u << i;
+            }
+            mx = max(mx, hh[i]);
+        }
+        const uint32_t em = tl.ballot(endb != 0);
+        const uint32_t elane = em ? (uint32_t)(__ffs(em) - 1) : (uint32_t)T;
+        const uint32_t myi = endb ? (uint32_t)(__ffs(endb) - 1) : 4u;
+        // only the slots before the end
+        if (tl.lane > elane) evb = cdb = 0;
+        else if (tl.lane == elane) evb &= (1u << myi) - 1u, cdb &= (1u << myi) - 1u;
+        // evictions in walk order: global stage numbers and the eviction slots
+        const uint32_t ne = __popc(evb);
+        const uint32_t einc = tile_sum<T>(ne, tl);
+        const uint32_t etot = tl.shfl(einc, T - 1);
+        uint32_t gi = g + einc - ne;
+        // the last eviction before each slot (for the possible updates' carried key)
+        long long lastpos = evb ? (long long)(base + 31 - __clz(evb)) : -1;
+        const long long linc = tile_max<T>(lastpos, tl);
+        long long lprev = __shfl_up_sync(tl.wmask, linc, 1, T);
+        if (tl.lane == 0) lprev = -1;
+        uint32_t co = 0;
+        uint32_t nc_tot = 0;
+        if (find) {
+            const uint32_t ncd = __popc(cdb);
+            const uint32_t cinc = tile_sum<T>(ncd, tl);
+            nc_tot = tl.shfl(cinc, T - 1);
+            co = cinc - ncd;
+        }
+        uint32_t stg = gi;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint64_t pos = base + i;
+            if ((evb >> i) & 1u) {
+                if (stg >= chunk_base && stg < (find ? chunk_base + TMAXCH : hi)) {
+                    s.pos[stg - chunk_base] = (uint32_t)(pos & mask);
+                    s.p[stg - chunk_base] = pend[i];
+                }
+                if (!find && stg + 1 == lo) s.src_base = (uint32_t)(pos & mask);
+                lprev = (long long)pos;
+                ++stg;
+            } else if (find && ((cdb >> i) & 1u)) {
+                s.cpos[co] = (uint32_t)(pos & mask);
+                s.cstage[co] = stg;
+                s.csrc[co] = lprev >= 0 ? (uint32_t)((uint64_t)lprev & mask)
+                                        : (last_ev == NOSRC ? NOSRC : last_ev);
+                ++co;
+            }
+        }
+        tl.sync();
+        // compare this window's possible updates, T per round trip
+        if (find && nc_tot) {
+            int found = -1;
+            for (uint32_t b0 = 0; b0 < nc_tot && found < 0; b0 += T) {
+                const uint32_t c = b0 + tl.lane;
+                bool eq = false;
+                if (c < nc_tot) {
+                    const uint8_t* sk = t.keys + (uint64_t)s.cpos[c] * KB;
+                    const uint32_t src = s.csrc[c];
+                    if (src == NOSRC) {
+                        eq = key.eq(sk, KB);
+                    } else {
+                        RegKey<KB> ck;  // the carried entry's key, still at its old slot
+                        ck.load_table(t.keys + (uint64_t)src * KB, KB);
+                        eq = ck.eq(sk, KB);
+                    }
+                }
+                const uint32_t mm = tl.ballot(eq);
+                if (mm) found = (int)(b0 + __ffs(mm) - 1);
+            }
+            if (found >= 0) {
+                kind = 2;
+                end_slot = s.cpos[found];
+                k = s.cstage[found];
+                tl.sync();
+                break;
+            }
+        }
+        // advance: evictions, last eviction slot, carried home
+        if (etot) {
+            const long long lw = tl.shfl(linc, T - 1);
+            last_ev = (uint32_t)((uint64_t)lw & mask);
+        }
+        g += etot;
+        const long long mall = tl.shfl(incl, T - 1);
+        if (em) {
+            // the end slot: its depth is position - running max before it
+            const uint32_t dsel = myi == 0 ? pend[0] : (myi == 1 ? pend[1] : (myi == 2 ? pend[2] : pend[3]));
+            const uint32_t fsel = myi == 0 ? f[0] : (myi == 1 ? f[1] : (myi == 2 ? f[2] : f[3]));
+            const uint64_t ep = (uint64_t)(long long)tl.shfl((long long)dsel, elane);
+            const uint32_t ef = tl.shfl(fsel, elane);
+            const uint64_t epos = wb + 4 * elane + tl.shfl(myi, elane);
+            // depth as a full 64-bit value (pend holds its low 32 bits)
+            const long long mend = tl.shfl(myi == 0 ? mi[0] : (myi == 1 ? mi[1] : (myi == 2 ? mi[2] : mi[3])), elane);
+            const uint64_t edepth = (uint64_t)((long long)epos - mend);
+            (void)ep;
+            kind = (edepth > mask) ? 3 : 1;
+            end_slot = epos & mask;
+            end_p = edepth;
+            end_tomb = st_of(ef) == ST_TOMB;
+            k = g;
+            if (!find) kind = 4;
+            break;
+        }
+        M = max(M, mall);
+        if (!find && g >= hi) {
+            kind = 4;
+            break;
+        }
+        wb += 4 * T;
+    }
+    if (!find) src_base = s.src_base;
+    tl.sync();
+    return kind;
+}
+
+// One insert by a tile (capacity >= 4T, rounds that are not serial).
+template <int KB, int VB, int T>
+__device__ __forceinline__ void exec_tile(const TableView& t, const RegKey<KB>& key,
+                                          const uint8_t* __restrict__ vals_in, uint32_t j, const Tile<T>& tl,
+                                          TileChain& s, ExecAcc& a) {
+    constexpr int CPL = 4;
+    const uint8_t* vin = vals_in + (uint64_t)j * VB;
+    uint32_t k = 0, chunk_base = 0, src_base = NOSRC;
+    uint64_t end_slot = 0, end_p = 0;
+    bool end_tomb = false;
+    const int kind =
+        tile_walk<KB, T>(t, key, s, tl, true, 0, 0, k, chunk_base, src_base, end_slot, end_p, end_tomb);
+    if (kind == 5) {
+        a.limit = true;
+        return;
+    }
+    uint32_t md = 0;
+    // last chunk: moves from the end (or the last eviction) down to chunk_base
+    {
+        const int hi = (kind == 3) ? (int)k - 1 : (int)k;
+        tile_moves<KB, VB, T, CPL>(t, key, vin, s, chunk_base, hi, (int)chunk_base, k, kind, end_slot, src_base, tl);
+        for (uint32_t m = chunk_base + tl.lane; m < k; m += T) {
+            t.flags[s.pos[m - chunk_base]] = mk_flag(ST_OCC, s.p[m - chunk_base]);
+            md = max(md, min(s.p[m - chunk_base], DIST_MASK));
+        }
+        tl.sync();
+    }
+    // earlier stages, TMAXCH at a time from the top, each found again by a
+    // walk from home
+    for (uint32_t top = chunk_base; top > 0;) {
+        const uint32_t lo = top > (uint32_t)TMAXCH ? top - TMAXCH : 0u;
+        uint32_t k2, cb2, sb2;
+        uint64_t es2, ep2;
+        bool et2;
+        tile_walk<KB, T>(t, key, s, tl, false, lo, top, k2, cb2, sb2, es2, ep2, et2);
+        tile_moves<KB, VB, T, CPL>(t, key, vin, s, lo, (int)top - 1, (int)lo, k, kind, end_slot, sb2, tl);
+        for (uint32_t m = tl.lane; m < top - lo; m += T) {
+            t.flags[s.pos[m]] = mk_flag(ST_OCC, s.p[m]);
+            md = max(md, min(s.p[m], DIST_MASK));
+        }
+        tl.sync();
+        top = lo;
+    }
+    if (tl.lane == 0 && kind == 1) {
+        t.flags[end_slot] = mk_flag(ST_OCC, end_p);
+        md = max(md, (uint32_t)min(end_p, (uint64_t)DIST_MASK));
+        a.claimed += 1;
+        a.tomb = a.tomb || end_tomb;
     }
     a.maxd = max(a.maxd, md);
 }
@@ -829,33 +1012,14 @@ __global__ void __launch_bounds__(RBLOCK, 3) k_ins_p3(TableView t, const uint8_t
     if (blockIdx.x == 0 && threadIdx.x == 0 && ops.n) atomicAdd(&ctl->rounds, 1u);
 }
 
-// ---- tile-cooperative round phases (compile-time shapes) -----------------
+// ---- tile-cooperative phases (compile-time shapes) -----------------------
 
-template <int KB, int T>
-__global__ void __launch_bounds__(RBLOCK) k_ins_p1t(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
-                                                    uint32_t r, OpScratch sc, Ctl* ctl) {
-    const RoundOps ops = round_ops(sc, ctl, r, n0);
-    if (blockIdx.x == 0 && threadIdx.x == 0) reset_next_round(ctl, r);
-    const Tile<T> tl;
-    const uint32_t ntiles = gridDim.x * (blockDim.x / T);
-    bool no_free = false;
-    for (uint32_t i = blockIdx.x * (blockDim.x / T) + threadIdx.x / T; i < ops.n; i += ntiles) {
-        const uint32_t j = ops.op(i);
-        RegKey<KB> key;
-        key.load(keys + (uint64_t)j * KB, KB);
-        const uint64_t F = find_free_tile<T>(t, key.hash(KB, t.hash_mode) & t.mask, tl);
-        if (tl.lane == 0) register_op(t, j, F, sc.op_slot);
-        no_free = no_free || F == NONE64;
-    }
-    if (no_free && (threadIdx.x & (T - 1)) == 0) ctl->serial[r & 1] = 1u;
-}
-
-// Phase 3 for op j on a tile: run the tile walk if j leads an unblocked
-// segment of a non-serial round; clear the registration.  Returns whether it ran.
+// Phase 3 for op j on a tile (the single-block tail): run the tile walk if j
+// leads an unblocked segment; clear the registration.  Returns whether it ran.
 template <int KB, int VB, int T>
 __device__ __forceinline__ bool finish_tile(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t j,
-                                            bool serial, const OpScratch& sc, const Tile<T>& tl, uint64_t* s_pos,
-                                            uint32_t* s_p, ExecAcc& a) {
+                                            bool serial, const OpScratch& sc, const Tile<T>& tl, TileChain& s,
+                                            ExecAcc& a) {
     // independent loads issued together: decision words, registration, key
     const uint8_t lead = sc.op_flag[j];
     const uint32_t blk = sc.op_word[j];
@@ -863,7 +1027,13 @@ __device__ __forceinline__ bool finish_tile(const TableView& t, const uint8_t* k
     RegKey<KB> key;
     key.load(keys + (uint64_t)j * KB, KB);
     const bool run = !serial && lead != 0 && blk > j;
-    if (run) exec_tile<KB, VB, T>(t, key, vals, j, tl, s_pos, s_p, a);
+    if (run) {
+        if (t.mask >= 4 * T - 1) {
+            exec_tile<KB, VB, T>(t, key, vals, j, tl, s, a);
+        } else {
+            if (tl.lane == 0) a.claimed += exec_insert_key<KB, VB>(t, key, vals + (uint64_t)j * VB, a);
+        }
+    }
     tl.sync();
     if (tl.lane == 0) {
         if (F != NONE64) {
@@ -875,64 +1045,38 @@ __device__ __forceinline__ bool finish_tile(const TableView& t, const uint8_t* k
     return run;
 }
 
-template <int KB, int VB, int T>
-__global__ void __launch_bounds__(RBLOCK, 4) k_ins_p3t(TableView t, const uint8_t* __restrict__ keys,
-                                                       const uint8_t* __restrict__ vals, uint32_t n0, uint32_t r,
-                                                       OpScratch sc, Ctl* ctl) {
-    __shared__ uint64_t s_pos[RBLOCK / T][MAXCH];
-    __shared__ uint32_t s_p[RBLOCK / T][MAXCH];
-    __shared__ AppendSmem s_app;
-    __shared__ uint32_t s_tmp[RBLOCK / 32];
-    append_init(s_app);
-    const RoundOps ops = round_ops(sc, ctl, r, n0);
-    const bool serial = *(volatile uint32_t*)&ctl->serial[r & 1] != 0;
-    uint32_t* out = pend_of(sc, r + 1);
-    uint32_t* out_n = &ctl->npend[(r + 1) & 1];
-    const Tile<T> tl;
-    const uint32_t tix = threadIdx.x / T;
-    const uint32_t ntiles = gridDim.x * (blockDim.x / T);
-    const uint32_t t0 = blockIdx.x * (blockDim.x / T) + tix;
-    const uint32_t iters = (ops.n + ntiles - 1) / ntiles;
-    ExecAcc a;
-    for (uint32_t it = 0; it < iters; it++) {
-        const uint32_t i = t0 + it * ntiles;
-        const bool valid = i < ops.n;
-        uint32_t j = 0;
-        bool ran = false;
-        if (valid) {
-            j = ops.op(i);
-            ran = finish_tile<KB, VB, T>(t, keys, vals, j, serial, sc, tl, s_pos[tix], s_p[tix], a);
-        }
-        block_append(out, out_n, j, valid && !ran && tl.lane == 0, s_app);
-    }
-    block_add_count(ctl, a.claimed, s_tmp);
-    publish_rare(ctl, a.maxd, a.tomb, a.limit);
-    if (blockIdx.x == 0 && threadIdx.x == 0 && ops.n) atomicAdd(&ctl->rounds, 1u);
-}
-
 // Phase 4: the inserts of round r whose walks were too long for one thread,
-// one warp each (32-slot metadata windows, up to 12 entry moves per batch of
-// round trips).  Their segments are disjoint from each other and from every
-// op run in phase 3.
+// one P4_T-lane tile each.  Their segments are disjoint from each other and
+// from every op run in phase 3.
+constexpr int P4_T = 32;
+
 template <int KB, int VB>
-__global__ void __launch_bounds__(RBLOCK, 2) k_ins_p4(TableView t, const uint8_t* __restrict__ keys,
-                                                   const uint8_t* __restrict__ vals, uint32_t r, OpScratch sc,
-                                                   Ctl* ctl) {
-    constexpr int NW = RBLOCK / 32;
-    __shared__ uint64_t s_pos[NW][MAXCH];
-    __shared__ uint32_t s_p[NW][MAXCH];
-    __shared__ uint32_t s_tmp[NW];
+__global__ void __launch_bounds__(RBLOCK, 3) k_ins_p4(TableView t, const uint8_t* __restrict__ keys,
+                                                      const uint8_t* __restrict__ vals, uint32_t r, OpScratch sc,
+                                                      Ctl* ctl) {
+    constexpr int NT = RBLOCK / P4_T;
+    __shared__ TileChain s_chain[NT];
+    __shared__ uint32_t s_tmp[RBLOCK / 32];
     const uint32_t n = *(volatile const uint32_t*)&ctl->nlong[r & 1];
     if (n == 0) return;  // block-uniform
-    const Tile<32> tl;
-    const uint32_t w = threadIdx.x >> 5;
-    const uint32_t nwarps = gridDim.x * NW;
+    const Tile<P4_T> tl;
+    const uint32_t ti = threadIdx.x / P4_T;
+    const uint32_t ntiles = gridDim.x * NT;
     ExecAcc a;
-    for (uint32_t i = blockIdx.x * NW + w; i < n; i += nwarps) {
-        const uint32_t j = sc.long_list[i];
-        RegKey<KB> key;
-        key.load(keys + (uint64_t)j * KB, KB);
-        exec_tile<KB, VB, 32>(t, key, vals, j, tl, s_pos[w], s_p[w], a);
+    // uniform trip count per warp (all tiles of a warp loop together)
+    const uint32_t iters = (n + ntiles - 1) / ntiles;
+    for (uint32_t it = 0; it < iters; it++) {
+        const uint32_t i = blockIdx.x * NT + ti + it * ntiles;
+        if (i < n) {
+            const uint32_t j = sc.long_list[i];
+            RegKey<KB> key;
+            key.load(keys + (uint64_t)j * KB, KB);
+            if (t.mask >= 4 * P4_T - 1) {
+                exec_tile<KB, VB, P4_T>(t, key, vals, j, tl, s_chain[ti], a);
+            } else {
+                if (tl.lane == 0) a.claimed += exec_insert_key<KB, VB>(t, key, vals + (uint64_t)j * VB, a);
+            }
+        }
         tl.sync();
     }
     block_add_count(ctl, a.claimed, s_tmp);
@@ -950,10 +1094,11 @@ template <int KB, int VB, int T>
 __global__ void __launch_bounds__(TAIL_THREADS) k_ins_tail(TableView t, const uint8_t* __restrict__ keys,
                                                            const uint8_t* __restrict__ vals, uint32_t n0,
                                                            uint32_t r0, uint32_t nops, OpScratch sc, Ctl* ctl) {
-    constexpr int NT = T > 1 ? TAIL_THREADS / T : 1;
+    // tiles holding a chain buffer (T > 1): as many as the static shared
+    // memory allows; the block's other warps idle in the tile phases
+    constexpr int NT = T > 1 ? (TAIL_THREADS / T < 12 ? TAIL_THREADS / T : 12) : 1;
     __shared__ uint32_t s_n, s_next, s_serial, s_err;
-    __shared__ uint64_t s_pos[NT][T > 1 ? MAXCH : 1];
-    __shared__ uint32_t s_p[NT][T > 1 ? MAXCH : 1];
+    __shared__ TileChain s_chain[T > 1 ? NT : 1];
     __shared__ uint32_t s_buf[TAIL_THREADS];
     __shared__ uint32_t s_woff[33];
     if (threadIdx.x == 0) {
@@ -968,7 +1113,7 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_ins_tail(TableView t, const ui
     uint32_t rounds = 0;
     // tiles (T > 1) or single threads (T == 1) as the unit of work
     const uint32_t unit = T > 1 ? threadIdx.x / T : threadIdx.x;
-    const uint32_t nunits = T > 1 ? blockDim.x / T : blockDim.x;
+    const uint32_t nunits = T > 1 ? (uint32_t)NT : blockDim.x;
     const bool leader_lane = T > 1 ? (threadIdx.x & (T - 1)) == 0 : true;
     for (;;) {
         const uint32_t* in = (r == 0) ? nullptr : pend_of(sc, r);
@@ -978,7 +1123,7 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_ins_tail(TableView t, const ui
             s_serial = 0;
         }
         __syncthreads();
-        for (uint32_t i = unit; i < n; i += nunits) {
+        for (uint32_t i = unit; unit < nunits && i < n; i += nunits) {
             const uint32_t j = in ? in[i] : i;
             uint64_t F;
             if constexpr (T > 1) {
@@ -1019,12 +1164,12 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_ins_tail(TableView t, const ui
             ++rounds;
             break;
         }
-        for (uint32_t i = unit; i < n; i += nunits) {
+        for (uint32_t i = unit; unit < nunits && i < n; i += nunits) {
             const uint32_t j = in ? in[i] : i;
             bool ran;
             if constexpr (T > 1) {
                 const Tile<(T > 1 ? T : 8)> tl;
-                ran = finish_tile<KB, VB, (T > 1 ? T : 8)>(t, keys, vals, j, false, sc, tl, s_pos[unit], s_p[unit], a);
+                ran = finish_tile<KB, VB, (T > 1 ? T : 8)>(t, keys, vals, j, false, sc, tl, s_chain[unit], a);
             } else {
                 ran = finish_op<KB, VB>(t, keys, vals, j, false, sc, a);
             }
@@ -1082,7 +1227,7 @@ __global__ void __launch_bounds__(1024) k_ins_serial(TableView t, const uint8_t*
     }
 }
 
-constexpr int INS_T = 8;  // lanes per insert in the tile kernels
+constexpr int INS_T = 32;  // lanes per insert in the single-block tail
 
 template <int KB, int VB>
 void rounds_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, uint32_t r0,

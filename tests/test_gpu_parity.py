@@ -319,14 +319,14 @@ def test_skewed_duplicate_heavy_scaled():
 
 
 @pytest.mark.parametrize("shape", [(8, 8), (32, 128)])
-@pytest.mark.parametrize("chain", [5, 30, 47, 48, 49, 70])
+@pytest.mark.parametrize("chain", [3, 4, 5, 30, 63, 64, 65, 70, 128, 129, 200])
 def test_long_eviction_chains(shape, chain):
     """An insert whose Robin Hood walk evicts `chain` entries in a row (homes
-    1..chain each at dist 0 behind a home-0 entry): exercises chains spanning
-    several metadata windows and the scalar walk past the per-tile chain
-    buffer."""
+    1..chain each at dist 0 behind a home-0 entry): exercises the thread
+    path's eviction limit, chains spanning several metadata windows and
+    chains longer than the tile's chain buffer (moved chunk by chunk)."""
     ks, vs = shape
-    cap = 256
+    cap = 256 if chain < 200 else 512
     g = gpu_map(cap, ks, vs)
     o = OracleAdapter(cap, ks, vs)
     homes = np.arange(0, chain + 1, dtype=np.uint64)
@@ -381,3 +381,53 @@ def test_overfull_table_serial_path(extra_n):
     assert g.len() == o.len() == cap + extra_n
     assert_same_layout(g, o)
     assert g.recount() == o.recount()
+
+
+@pytest.mark.parametrize("shape", [(8, 8), (32, 128)])
+@pytest.mark.parametrize("run", [2, 3, 10, 33, 40, 100])
+def test_many_possible_updates(shape, run):
+    """`run` keys sharing one home sit at distances 0..run-1, so a walk from
+    that home meets a possible update (stored distance == probe depth) at
+    every slot: a fresh key compares all of them and claims the slot after;
+    an existing key deep in the run updates in place (buffered compares
+    flushed in walk order)."""
+    ks, vs = shape
+    cap = 256
+    g = gpu_map(cap, ks, vs)
+    o = OracleAdapter(cap, ks, vs)
+    homes0 = np.arange(run, dtype=np.uint64) * cap + 5
+    keys = le(homes0, ks)
+    vals = le(homes0 + 1, vs)
+    assert g.bulk_insert(keys, vals) == o.bulk_insert(keys, vals)
+    # a fresh key and an update of the key at depth run-2, in one batch and alone
+    fresh = le([np.uint64(run * cap + 5)], ks)
+    upd = le([homes0[max(run - 2, 0)]], ks)
+    for batch in (np.concatenate([fresh, upd]), upd, fresh):
+        bv = le(np.arange(len(batch), dtype=np.uint64) + 777, vs)
+        assert g.bulk_insert(batch, bv) == o.bulk_insert(batch, bv)
+        assert_same_layout(g, o)
+
+
+@pytest.mark.parametrize("load", [0.9, 0.97])
+def test_high_load_fill_and_churn(load):
+    """u64 pairs filled to a high load in calls of 2% of the capacity (eviction
+    chains of hundreds of entries, many possible updates per walk), then
+    remove/insert churn that reuses tombstones; full layout after each call."""
+    cap = 1 << 14
+    rng = np.random.default_rng(int(load * 100))
+    g = gpu_map(cap, 8, 8)
+    o = OracleAdapter(cap, 8, 8)
+    n = int(cap * load)
+    keys = rng.integers(0, 1 << 63, n, dtype=np.uint64)
+    call = cap // 50
+    for b in range(0, n, call):
+        k = le(keys[b:b + call])
+        assert g.bulk_insert(k, k) == o.bulk_insert(k, k)
+    assert_same_layout(g, o)
+    for r in range(3):
+        rm = le(keys[rng.choice(n, call, replace=False)])
+        assert g.bulk_remove(rm) == o.bulk_remove(rm)
+        fresh = le(rng.integers(0, 1 << 63, call, dtype=np.uint64))
+        assert g.bulk_insert(fresh, fresh) == o.bulk_insert(fresh, fresh)
+        assert_same_layout(g, o)
+    assert_same_gets(g, o, le(keys))
