@@ -394,9 +394,27 @@ class DeviceRun:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_s = float(t.item())
         calls = (w.pairs + CALL - 1) // CALL
+        # the link these copies cross: pinned 256 MB copies each way
+        hb = torch.empty(1 << 28, dtype=torch.uint8).pin_memory()
+        db = torch.empty(1 << 28, dtype=torch.uint8, device=self.q.device)
+        Ev = torch.cuda.Event
+        bw = {}
+        for name, dst, src in (("h2d_gbs", db, hb), ("d2h_gbs", hb, db)):
+            dst.copy_(src, non_blocking=True)
+            a, b = Ev(enable_timing=True), Ev(enable_timing=True)
+            a.record()
+            for _ in range(3):
+                dst.copy_(src, non_blocking=True)
+            b.record()
+            torch.cuda.synchronize()
+            bw[name] = round(3 * (1 << 28) / (a.elapsed_time(b) / 1e3) / 1e9, 1)
+        h2d = w.pairs * (KB + VB) + w.gets * KB + w.removes * KB
+        d2h = w.gets * (VB + 1) + 8 * (calls + 1)
         return {"value": round(w.ops * world / e2e_s / 1e6, 3), "unit": "Mops/s",
-                "h2d_bytes_per_step": w.pairs * (KB + VB) + w.gets * KB + w.removes * KB,
-                "d2h_bytes_per_step": w.gets * (VB + 1) + 8 * (calls + 1),
+                "link_gbs": bw,
+                "copy_bound_ms": round((h2d / bw["h2d_gbs"] + d2h / bw["d2h_gbs"]) / 1e6, 3),
+                "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
                 "ms_per_step": round(e2e_s * 1e3, 3)}
 
 

@@ -46,10 +46,18 @@ struct DeviceGuard {
     }
 };
 
+// Host-API pipelining: a host call is split into pieces whose host->device
+// copy, kernels and device->host copy overlap with the neighbouring pieces'
+// (two streams alternate for get; a copy stream prefetches the next piece of
+// a mutating call while the current one runs).  Splitting a mutating batch
+// into consecutive pieces keeps the sequential semantics.
+constexpr uint64_t HOST_GET_PIECE = 1ull << 19;  // queries per get piece
+constexpr uint64_t HOST_MUT_PIECE = 1ull << 16;  // ops per insert/remove piece
+
 struct GetCtx {
-    cudaStream_t s = nullptr;
-    uint8_t* d_buf = nullptr;
-    size_t cap = 0;
+    cudaStream_t s[2] = {nullptr, nullptr};
+    uint8_t* d_buf[2] = {nullptr, nullptr};
+    size_t cap[2] = {0, 0};
 };
 
 template <class T>
@@ -159,8 +167,10 @@ struct fm_table {
     OpScratch sc{};
     size_t sc_bytes = 0;
     uint8_t* sc_base = nullptr;
-    uint8_t* d_in = nullptr;  // host-API staging for mutating calls
+    uint8_t* d_in = nullptr;  // host-API staging for mutating calls (two pieces)
     size_t d_in_cap = 0;
+    cudaStream_t copy_stream = nullptr;  // prefetch of the next piece
+    cudaEvent_t piece_ready[2] = {nullptr, nullptr};
     std::mutex pool_mu;
     std::vector<GetCtx*> pool;
     KTimer timer;
@@ -328,9 +338,12 @@ GetCtx* acquire_ctx(fm_table* t) {
         }
     }
     GetCtx* c = new GetCtx();
-    if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess) {
-        delete c;
-        return nullptr;
+    for (int i = 0; i < 2; i++) {
+        if (cudaStreamCreateWithFlags(&c->s[i], cudaStreamNonBlocking) != cudaSuccess) {
+            if (i) cudaStreamDestroy(c->s[0]);
+            delete c;
+            return nullptr;
+        }
     }
     return c;
 }
@@ -388,6 +401,11 @@ int fm_create(uint64_t capacity, uint32_t key_size, uint32_t value_size, uint32_
     };
     if ((e = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking)) != cudaSuccess)
         return bail(FM_ERR_CUDA_INIT, "stream", e);
+    if ((e = cudaStreamCreateWithFlags(&t->copy_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(FM_ERR_CUDA_INIT, "stream", e);
+    for (int i = 0; i < 2; i++)
+        if ((e = cudaEventCreateWithFlags(&t->piece_ready[i], cudaEventDisableTiming)) != cudaSuccess)
+            return bail(FM_ERR_CUDA_INIT, "event", e);
     const size_t kb = (size_t)cap * (key_size ? key_size : 1);
     const size_t vb = (size_t)cap * (value_size ? value_size : 1);
     if ((e = cudaMalloc((void**)&t->d_flags, cap * 4)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "flags", e);
@@ -415,11 +433,19 @@ void fm_destroy(fm_table* t) {
     DeviceGuard dg(t->device);
     if (t->stream) cudaStreamSynchronize(t->stream);
     for (GetCtx* c : t->pool) {
-        cudaStreamSynchronize(c->s);
-        cudaStreamDestroy(c->s);
-        if (c->d_buf) cudaFree(c->d_buf);
+        for (int i = 0; i < 2; i++) {
+            cudaStreamSynchronize(c->s[i]);
+            cudaStreamDestroy(c->s[i]);
+            if (c->d_buf[i]) cudaFree(c->d_buf[i]);
+        }
         delete c;
     }
+    if (t->copy_stream) {
+        cudaStreamSynchronize(t->copy_stream);
+        cudaStreamDestroy(t->copy_stream);
+    }
+    for (int i = 0; i < 2; i++)
+        if (t->piece_ready[i]) cudaEventDestroy(t->piece_ready[i]);
     cudaFree(t->d_flags);
     cudaFree(t->d_keys);
     cudaFree(t->d_vals);
@@ -446,27 +472,37 @@ int fm_bulk_get(fm_table* t, const void* keys, uint64_t n, void* out_values, uin
     TimerScope ts(t);
     GetCtx* c = acquire_ctx(t);
     if (!c) return fail(FM_ERR_CUDA_INIT, "stream creation failed");
-    const size_t kb = (size_t)n * t->ksz, vb = (size_t)n * t->vsz;
+    // pieces alternate between two streams and staging buffers: piece i+1's
+    // keys upload while piece i's lookups and downloads run
+    const uint64_t piece = n < HOST_GET_PIECE ? n : HOST_GET_PIECE;
+    const size_t kb = (size_t)piece * t->ksz, vb = (size_t)piece * t->vsz;
     const size_t off_v = (kb + 255) & ~(size_t)255;
     const size_t off_f = off_v + ((vb + 255) & ~(size_t)255);
-    cudaError_t e = grow(c->d_buf, c->cap, off_f + n);
-    if (e != cudaSuccess) {
-        release_ctx(t, c);
-        return cuda_fail(FM_ERR_GPU_ALLOC, "get buffers", e);
-    }
-    uint8_t* dq = c->d_buf;
-    uint8_t* dv = c->d_buf + off_v;
-    uint8_t* df = c->d_buf + off_f;
     int rc = FM_OK;
-    if ((e = cudaMemcpyAsync(dq, keys, kb, cudaMemcpyHostToDevice, c->s)) != cudaSuccess)
-        rc = cuda_fail(FM_ERR_TRANSFER, "htod keys", e);
-    if (!rc && (e = fm::launch_get(t->view(), t->shape, dq, n, dv, df, c->s)) != cudaSuccess)
-        rc = cuda_fail(FM_ERR_KERNEL_LAUNCH, "bulk_get", e);
-    if (!rc && vb && (e = cudaMemcpyAsync(out_values, dv, vb, cudaMemcpyDeviceToHost, c->s)) != cudaSuccess)
-        rc = cuda_fail(FM_ERR_TRANSFER, "dtoh values", e);
-    if (!rc && (e = cudaMemcpyAsync(out_found, df, n, cudaMemcpyDeviceToHost, c->s)) != cudaSuccess)
-        rc = cuda_fail(FM_ERR_TRANSFER, "dtoh found", e);
-    if ((e = cudaStreamSynchronize(c->s)) != cudaSuccess && !rc) rc = cuda_fail(FM_ERR_TRANSFER, "bulk_get sync", e);
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 2 && !rc; i++)
+        if ((e = grow(c->d_buf[i], c->cap[i], off_f + piece)) != cudaSuccess) rc = cuda_fail(FM_ERR_GPU_ALLOC, "get buffers", e);
+    const uint8_t* hk = (const uint8_t*)keys;
+    uint8_t* hv = (uint8_t*)out_values;
+    for (uint64_t base = 0, i = 0; base < n && !rc; base += piece, ++i) {
+        const uint64_t m = (n - base) < piece ? (n - base) : piece;
+        const int sl = (int)(i & 1);
+        cudaStream_t st = c->s[sl];
+        uint8_t* dq = c->d_buf[sl];
+        uint8_t* dv = c->d_buf[sl] + off_v;
+        uint8_t* df = c->d_buf[sl] + off_f;
+        if ((e = cudaMemcpyAsync(dq, hk + base * t->ksz, m * t->ksz, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+            rc = cuda_fail(FM_ERR_TRANSFER, "htod keys", e);
+        if (!rc && (e = fm::launch_get(t->view(), t->shape, dq, m, dv, df, st)) != cudaSuccess)
+            rc = cuda_fail(FM_ERR_KERNEL_LAUNCH, "bulk_get", e);
+        if (!rc && t->vsz &&
+            (e = cudaMemcpyAsync(hv + base * t->vsz, dv, m * t->vsz, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            rc = cuda_fail(FM_ERR_TRANSFER, "dtoh values", e);
+        if (!rc && (e = cudaMemcpyAsync(out_found + base, df, m, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            rc = cuda_fail(FM_ERR_TRANSFER, "dtoh found", e);
+    }
+    for (int i = 0; i < 2; i++)
+        if ((e = cudaStreamSynchronize(c->s[i])) != cudaSuccess && !rc) rc = cuda_fail(FM_ERR_TRANSFER, "bulk_get sync", e);
     release_ctx(t, c);
     return rc;
 }
@@ -483,27 +519,74 @@ static int precheck(fm_table* t, uint64_t n) {
     return FM_OK;
 }
 
+namespace {
+
+// A host-buffer insert (values != nullptr or vsz == 0) or remove, in pieces:
+// the copy stream uploads piece i+1 into the other staging half while the
+// rounds of piece i run on the table's stream.
+int host_pieces(fm_table* t, bool insert, const void* keys, const void* values, uint64_t n, uint64_t* out,
+                bool* limit) {
+    const uint64_t piece = n < HOST_MUT_PIECE ? n : HOST_MUT_PIECE;
+    const size_t kb = (size_t)piece * t->ksz, vb = insert ? (size_t)piece * t->vsz : 0;
+    const size_t off_v = (kb + 255) & ~(size_t)255;
+    const size_t half = (off_v + vb + 256) & ~(size_t)255;
+    cudaError_t e = grow(t->d_in, t->d_in_cap, 2 * half);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_GPU_ALLOC, insert ? "insert buffers" : "remove buffers", e);
+    const uint8_t* hk = (const uint8_t*)keys;
+    const uint8_t* hv = (const uint8_t*)values;
+    auto upload = [&](uint64_t base, int sl) -> cudaError_t {
+        const uint64_t m = (n - base) < piece ? (n - base) : piece;
+        uint8_t* d = t->d_in + sl * half;
+        cudaError_t err = cudaMemcpyAsync(d, hk + base * t->ksz, m * t->ksz, cudaMemcpyHostToDevice, t->copy_stream);
+        if (err == cudaSuccess && vb)
+            err = cudaMemcpyAsync(d + off_v, hv + base * t->vsz, m * t->vsz, cudaMemcpyHostToDevice, t->copy_stream);
+        if (err == cudaSuccess) err = cudaEventRecord(t->piece_ready[sl], t->copy_stream);
+        return err;
+    };
+    // the staging halves may still be read by the previous call's kernels
+    if ((e = cudaStreamSynchronize(t->stream)) != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "sync", e);
+    if ((e = upload(0, 0)) != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "htod", e);
+    uint64_t total = 0;
+    bool lim = false;
+    for (uint64_t base = 0, i = 0; base < n; base += piece, ++i) {
+        const int sl = (int)(i & 1);
+        const uint64_t m = (n - base) < piece ? (n - base) : piece;
+        if ((e = cudaStreamWaitEvent(t->stream, t->piece_ready[sl], 0)) != cudaSuccess)
+            return cuda_fail(FM_ERR_TRANSFER, "piece wait", e);
+        // the other half was last read by piece i-1, whose rounds have returned
+        if (base + piece < n && (e = upload(base + piece, sl ^ 1)) != cudaSuccess)
+            return cuda_fail(FM_ERR_TRANSFER, "htod", e);
+        uint8_t* d = t->d_in + sl * half;
+        uint64_t c = 0;
+        bool l = false;
+        int rc = run_rounds(t, insert, d, insert && t->vsz ? d + off_v : (insert ? d : nullptr), m, t->stream, &c, &l);
+        if (rc) {
+            cudaStreamSynchronize(t->copy_stream);
+            return rc;
+        }
+        total += c;
+        lim = lim || l;
+    }
+    *out = total;
+    *limit = lim;
+    return FM_OK;
+}
+
+}  // namespace
+
 int fm_bulk_insert(fm_table* t, const void* keys, const void* values, uint64_t n, uint64_t* num_new) {
     if (!t || !num_new) return fail(FM_ERR_INVALID_ARG, "NULL argument");
     *num_new = 0;
     if (n == 0) return FM_OK;  // gpu.rs:194-196
     if (!keys || (!values && t->vsz)) return fail(FM_ERR_INVALID_ARG, "NULL buffer");
     std::lock_guard<std::mutex> g(t->mu);
-    int rc = precheck(t, n);
+    int rc = precheck(t, n);  // whole batch, before any piece runs
     if (rc) return rc;
     DeviceGuard dg(t->device);
     TimerScope ts(t);
-    const size_t kb = (size_t)n * t->ksz, vb = (size_t)n * t->vsz;
-    const size_t off_v = (kb + 255) & ~(size_t)255;
-    cudaError_t e = grow(t->d_in, t->d_in_cap, off_v + vb + 1);
-    if (e != cudaSuccess) return cuda_fail(FM_ERR_GPU_ALLOC, "insert buffers", e);
-    if ((e = cudaMemcpyAsync(t->d_in, keys, kb, cudaMemcpyHostToDevice, t->stream)) != cudaSuccess)
-        return cuda_fail(FM_ERR_TRANSFER, "htod keys", e);
-    if (vb && (e = cudaMemcpyAsync(t->d_in + off_v, values, vb, cudaMemcpyHostToDevice, t->stream)) != cudaSuccess)
-        return cuda_fail(FM_ERR_TRANSFER, "htod values", e);
     uint64_t added = 0;
     bool limit = false;
-    rc = run_rounds(t, true, t->d_in, t->d_in + off_v, n, t->stream, &added, &limit);
+    rc = host_pieces(t, true, keys, values, n, &added, &limit);
     if (rc) return rc;
     t->len += added;
     *num_new = added;
@@ -518,14 +601,9 @@ int fm_bulk_remove(fm_table* t, const void* keys, uint64_t n, uint64_t* num_remo
     std::lock_guard<std::mutex> g(t->mu);
     DeviceGuard dg(t->device);
     TimerScope ts(t);
-    const size_t kb = (size_t)n * t->ksz;
-    cudaError_t e = grow(t->d_in, t->d_in_cap, kb + 1);
-    if (e != cudaSuccess) return cuda_fail(FM_ERR_GPU_ALLOC, "remove buffers", e);
-    if ((e = cudaMemcpyAsync(t->d_in, keys, kb, cudaMemcpyHostToDevice, t->stream)) != cudaSuccess)
-        return cuda_fail(FM_ERR_TRANSFER, "htod keys", e);
     uint64_t removed = 0;
     bool limit = false;
-    int rc = run_rounds(t, false, t->d_in, nullptr, n, t->stream, &removed, &limit);
+    int rc = host_pieces(t, false, keys, nullptr, n, &removed, &limit);
     if (rc) return rc;
     t->len -= removed;
     *num_removed = removed;

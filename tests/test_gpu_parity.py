@@ -431,3 +431,37 @@ def test_high_load_fill_and_churn(load):
         assert g.bulk_insert(fresh, fresh) == o.bulk_insert(fresh, fresh)
         assert_same_layout(g, o)
     assert_same_gets(g, o, le(keys))
+
+
+def test_host_api_pieces_pinned_buffers():
+    """Host-API calls larger than one transfer piece, from pinned host
+    buffers: an insert of 150K account-shape pairs whose in-batch duplicates
+    straddle piece boundaries (later wins), a get of 1.2M keys and a remove of
+    100K, each split into overlapping upload/compute/download pieces."""
+    import torch
+
+    cap = 1 << 18
+    rng = np.random.default_rng(11)
+    n = 150_000
+    keys = rng.integers(0, 256, (n, 32), dtype=np.uint8)
+    dup = rng.choice(n // 2, n // 10, replace=False)
+    keys[n // 2 + dup] = keys[dup]  # repeats of first-half keys in the second half
+    vals = rng.integers(0, 256, (n, 128), dtype=np.uint8)
+    pk = torch.from_numpy(keys).pin_memory().numpy()
+    pv = torch.from_numpy(vals).pin_memory().numpy()
+    g = gpu_map(cap, 32, 128)
+    o = OracleAdapter(cap, 32, 128)
+    assert g.bulk_insert(pk, pv) == o.bulk_insert(keys, vals)
+    assert_same_layout(g, o)
+    q = np.concatenate([keys, rng.integers(0, 256, (1_200_000 - n, 32), dtype=np.uint8)])
+    q = q[rng.permutation(len(q))]
+    pq = torch.from_numpy(q).pin_memory().numpy()
+    ov = torch.empty((len(q), 128), dtype=torch.uint8).pin_memory().numpy()
+    of = torch.empty((len(q),), dtype=torch.uint8).pin_memory().numpy()
+    gv, gf = g.bulk_get(pq, out_values=ov, out_found=of)
+    ev, ef = o.bulk_get(q)
+    assert np.array_equal(np.asarray(gf, bool), np.asarray(ef, bool))
+    assert np.array_equal(gv, ev)
+    rm = torch.from_numpy(keys[rng.choice(n, 100_000, replace=False)]).pin_memory().numpy()
+    assert g.bulk_remove(rm) == o.bulk_remove(np.array(rm))
+    assert_same_layout(g, o)
