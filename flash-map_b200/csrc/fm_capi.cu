@@ -2,6 +2,7 @@
 // lifetime, host<->device transfers, the round loop of the mutating
 // operations, error mapping and len bookkeeping.  Replaces the reference's
 // src/gpu.rs (bajpainaman/flash-map 0.5.0); see include/flashmap_b200.h.
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -935,3 +936,337 @@ extern "C" int fm_bulk_insert_device_noalloc(fm_table* t, const void* d_keys, co
     *num_new = added;
     return limit ? limit_error() : FM_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Batched form (no counterpart in gpu.rs): a queue of bulk operations over
+// many tables of one device, executed with the sequential result of running
+// them one by one in queue order.
+//
+// Planning (fm_batch_create): an op goes into the wave after the previous op
+// on its table, except that a get following a get on the same table joins
+// that get's wave (lookups do not change the table).  So the ops of a wave
+// touch distinct tables (several gets of one table aside) and are independent.
+// Each wave launches one grouped lookup kernel per record shape and one
+// grouped round pipeline per shape for its inserts and for its removes
+// (precheck against the table's count at that point of the batch, grid
+// rounds, a block-per-op tail that runs to completion, result write-back):
+// no host synchronisation between waves, so the whole batch can be captured
+// in one CUDA graph and replayed.
+// ---------------------------------------------------------------------------
+
+static_assert(fm::STATUS_TABLE_FULL == FM_ERR_TABLE_FULL && fm::STATUS_PROBE_LIMIT == FM_ERR_PROBE_LIMIT &&
+                  fm::STATUS_KERNEL == FM_ERR_KERNEL_LAUNCH,
+              "device status codes");
+
+struct fm_batch {
+    int device = 0;
+    std::vector<fm_op> ops;
+    std::vector<fm_table*> tables;      // distinct tables, batch order
+    std::vector<uint32_t> table_of;     // op -> index in tables
+    struct Group {
+        uint32_t wave;
+        uint32_t kind;
+        fm::Shape shape;
+        std::vector<uint32_t> members;  // op indices
+        size_t desc_off = 0;            // GroupGet[] / GroupOp[] in the descriptor buffer
+        size_t prefix_off = 0;          // gets: uint64 prefix[n+1]
+        uint64_t total = 0;             // gets: queries; mutating: sum of sizes
+        fm::GetCfg cfg;
+    };
+    std::vector<Group> groups;          // in execution order
+    uint32_t waves = 0;
+    size_t desc_bytes = 0;
+    uint8_t* d_desc = nullptr;          // descriptors (device)
+    uint8_t* h_desc = nullptr;          // descriptors (pinned host)
+    unsigned long long* d_len = nullptr;   // per table
+    unsigned long long* d_res = nullptr;   // per op
+    int* d_status = nullptr;               // per op
+    uint8_t* h_io = nullptr;               // pinned: len[tables], res[ops], status[ops]
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long launches_per_run = 0;
+    cudaStream_t last_stream = nullptr;
+    bool pending = false;
+
+    unsigned long long* h_len() { return reinterpret_cast<unsigned long long*>(h_io); }
+    unsigned long long* h_res() { return h_len() + tables.size(); }
+    int* h_status() { return reinterpret_cast<int*>(h_res() + ops.size()); }
+    size_t io_bytes() const { return (tables.size() + ops.size()) * 8 + ops.size() * 4; }
+};
+
+namespace {
+
+bool batch_aligned(const fm_op& o) {
+    for (const void* p : {(const void*)o.d_keys, (const void*)o.d_values, (const void*)o.d_out_values})
+        if (p && !aligned(p, 16)) return false;
+    return true;
+}
+
+// Fills the descriptor buffer from the current table state (scratch pointers
+// can move when a table's scratch grows between runs).
+int batch_fill(fm_batch* b) {
+    for (size_t i = 0; i < b->tables.size(); i++) b->h_len()[i] = b->tables[i]->len.load();
+    for (auto& g : b->groups) {
+        if (g.kind == FM_OP_GET) {
+            auto* d = reinterpret_cast<fm::GroupGet*>(b->h_desc + g.desc_off);
+            auto* pre = reinterpret_cast<uint64_t*>(b->h_desc + g.prefix_off);
+            uint64_t acc = 0;
+            double load = 0.0;
+            for (size_t k = 0; k < g.members.size(); k++) {
+                const fm_op& o = b->ops[g.members[k]];
+                fm_table* t = o.table;
+                d[k].t = t->view();
+                d[k].keys = (const uint8_t*)o.d_keys;
+                d[k].out_vals = (uint8_t*)o.d_out_values;
+                d[k].out_found = o.d_out_found;
+                pre[k] = acc;
+                acc += o.n;
+                load = std::max(load, (double)t->len.load() / (double)t->cap);
+            }
+            pre[g.members.size()] = acc;
+            g.total = acc;
+            g.cfg = fm::tuned_get_cfg(g.shape, load);
+            // one thread per query needs 8-slot windows
+            for (uint32_t m : g.members)
+                if (b->ops[m].table->mask < 7 && g.cfg.lanes == 1) g.cfg.lanes = 8;
+        } else {
+            auto* d = reinterpret_cast<fm::GroupOp*>(b->h_desc + g.desc_off);
+            uint64_t sum = 0;
+            for (size_t k = 0; k < g.members.size(); k++) {
+                const uint32_t oi = g.members[k];
+                const fm_op& o = b->ops[oi];
+                fm_table* t = o.table;
+                int rc = ensure_scratch(t, o.n);
+                if (rc) return rc;
+                d[k].t = t->view();
+                d[k].keys = (const uint8_t*)o.d_keys;
+                d[k].vals = (const uint8_t*)o.d_values;
+                d[k].sc = t->sc;
+                d[k].ctl = t->d_ctl;
+                d[k].len = b->d_len + b->table_of[oi];
+                d[k].result = b->d_res + oi;
+                d[k].status = b->d_status + oi;
+                d[k].n = (uint32_t)o.n;
+                d[k].counted = 1;
+                sum += o.n;
+            }
+            g.total = sum;
+        }
+    }
+    return FM_OK;
+}
+
+// Enqueues the batch on stream s: descriptor and count upload, the waves,
+// result download.
+int batch_enqueue(fm_batch* b, cudaStream_t s) {
+    cudaError_t e = cudaMemcpyAsync(b->d_desc, b->h_desc, b->desc_bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_len, b->h_len(), b->tables.size() * 8, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "batch upload", e);
+    for (const auto& g : b->groups) {
+        const uint32_t n = (uint32_t)g.members.size();
+        if (g.kind == FM_OP_GET) {
+            e = fm::launch_grp_get(g.shape, reinterpret_cast<const fm::GroupGet*>(b->d_desc + g.desc_off),
+                                   reinterpret_cast<const uint64_t*>(b->d_desc + g.prefix_off), n, g.total, g.cfg, s);
+        } else if (g.kind == FM_OP_INSERT) {
+            e = fm::launch_grp_ins(g.shape, reinterpret_cast<const fm::GroupOp*>(b->d_desc + g.desc_off), n, g.total,
+                                   s);
+        } else {
+            e = fm::launch_grp_rem(g.shape, reinterpret_cast<const fm::GroupOp*>(b->d_desc + g.desc_off), n, g.total,
+                                   s);
+        }
+        if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch wave", e);
+    }
+    e = cudaMemcpyAsync(b->h_len(), b->d_len, b->tables.size() * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_res(), b->d_res, b->ops.size() * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_status(), b->d_status, b->ops.size() * 4, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "batch download", e);
+    return FM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fm_batch_create(const fm_op* ops, uint32_t nops, fm_batch** out) {
+    if (!out) return fail(FM_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (!ops || nops == 0) return fail(FM_ERR_INVALID_ARG, "empty batch");
+    fm_batch* b = new fm_batch();
+    b->ops.assign(ops, ops + nops);
+    b->device = ops[0].table ? ops[0].table->device : 0;
+    std::vector<int> last_wave;
+    std::vector<uint32_t> last_kind;
+    for (uint32_t i = 0; i < nops; i++) {
+        const fm_op& o = ops[i];
+        auto bad = [&](const char* why) {
+            delete b;
+            return fail(FM_ERR_INVALID_ARG, std::string("batch op ") + std::to_string(i) + ": " + why);
+        };
+        if (!o.table) return bad("table is NULL");
+        if (o.table->device != b->device) return bad("tables on different devices");
+        if (o.kind > FM_OP_REMOVE) return bad("unknown kind");
+        if (o.n > 0xFFFFFFFFull - 1) return bad("more than 2^32-2 keys in one op");
+        if (o.n && !o.d_keys) return bad("NULL keys");
+        if (o.n && o.kind == FM_OP_INSERT && o.table->vsz && !o.d_values) return bad("NULL values");
+        uint32_t ti = 0;
+        while (ti < b->tables.size() && b->tables[ti] != o.table) ti++;
+        if (ti == b->tables.size()) {
+            b->tables.push_back(o.table);
+            last_wave.push_back(-1);
+            last_kind.push_back(0xFFu);
+        }
+        b->table_of.push_back(ti);
+        int w;
+        if (last_wave[ti] < 0) w = 0;
+        else if (o.kind == FM_OP_GET && last_kind[ti] == FM_OP_GET) w = last_wave[ti];
+        else w = last_wave[ti] + 1;
+        last_wave[ti] = w;
+        last_kind[ti] = o.kind;
+        if ((uint32_t)w + 1 > b->waves) b->waves = (uint32_t)w + 1;
+        if (o.n == 0) continue;  // nothing to launch; result 0, status OK
+        const fm::Shape sh = batch_aligned(o) ? o.table->shape : fm::SHAPE_GENERIC;
+        // the group of (wave, kind, shape), split at GROUP_MAX members
+        fm_batch::Group* g = nullptr;
+        for (auto it = b->groups.rbegin(); it != b->groups.rend(); ++it) {
+            if (it->wave == (uint32_t)w && it->kind == o.kind && it->shape == sh && it->members.size() < fm::GROUP_MAX) {
+                g = &*it;
+                break;
+            }
+        }
+        if (!g) {
+            b->groups.push_back(fm_batch::Group{(uint32_t)w, o.kind, sh, {}});
+            g = &b->groups.back();
+        }
+        g->members.push_back(i);
+    }
+    // execution order: by wave (groups of one wave are independent)
+    std::stable_sort(b->groups.begin(), b->groups.end(),
+                     [](const fm_batch::Group& x, const fm_batch::Group& y) { return x.wave < y.wave; });
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = (off + bytes + 255) & ~(size_t)255;
+        return o;
+    };
+    for (auto& g : b->groups) {
+        if (g.kind == FM_OP_GET) {
+            g.desc_off = take(g.members.size() * sizeof(fm::GroupGet));
+            g.prefix_off = take((g.members.size() + 1) * 8);
+        } else {
+            g.desc_off = take(g.members.size() * sizeof(fm::GroupOp));
+        }
+    }
+    b->desc_bytes = off ? off : 256;
+    DeviceGuard dg(b->device);
+    cudaError_t e = cudaMalloc((void**)&b->d_desc, b->desc_bytes);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_desc, b->desc_bytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_len, b->tables.size() * 8);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_res, nops * 8);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_status, nops * 4);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_io, b->io_bytes());
+    if (e == cudaSuccess) e = cudaMemset(b->d_res, 0, nops * 8);
+    if (e == cudaSuccess) e = cudaMemset(b->d_status, 0, nops * 4);
+    if (e != cudaSuccess) {
+        fm_batch_destroy(b);
+        return cuda_fail(FM_ERR_GPU_ALLOC, "batch buffers", e);
+    }
+    memset(b->h_desc, 0, b->desc_bytes);
+    memset(b->h_io, 0, b->io_bytes());
+    *out = b;
+    return FM_OK;
+}
+
+uint32_t fm_batch_waves(const fm_batch* b) { return b ? b->waves : 0; }
+
+int fm_batch_capture(fm_batch* b, void* stream) {
+    if (!b) return fail(FM_ERR_INVALID_ARG, "batch is NULL");
+    if (b->pending) return fail(FM_ERR_INVALID_ARG, "batch still running: call fm_batch_wait first");
+    DeviceGuard dg(b->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = batch_fill(b);  // allocations (scratch growth) happen here, outside the capture
+    if (rc) return rc;
+    if (b->exec) cudaGraphExecDestroy(b->exec), b->exec = nullptr;
+    if (b->graph) cudaGraphDestroy(b->graph), b->graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "begin capture", e);
+    const unsigned long long l0 = fm::launch_count();
+    rc = batch_enqueue(b, s);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(s, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "end capture", e);
+    b->launches_per_run = fm::launch_count() - l0;
+    b->graph = g;
+    e = cudaGraphInstantiate(&b->exec, g, 0);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "graph instantiate", e);
+    return FM_OK;
+}
+
+int fm_batch_run(fm_batch* b, void* stream) {
+    if (!b) return fail(FM_ERR_INVALID_ARG, "batch is NULL");
+    if (b->pending) return fail(FM_ERR_INVALID_ARG, "batch still running: call fm_batch_wait first");
+    DeviceGuard dg(b->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    // tables must not have host-side work in flight on their own streams
+    for (fm_table* t : b->tables) cudaStreamSynchronize(t->stream);
+    int rc;
+    if (b->exec) {
+        rc = batch_fill(b);
+        if (rc) return rc;
+        cudaError_t e = cudaGraphLaunch(b->exec, s);
+        if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "graph launch", e);
+        fm::count_launches((unsigned)b->launches_per_run);
+    } else {
+        TimerScope ts(b->tables.size() == 1 ? b->tables[0] : nullptr);
+        rc = batch_fill(b);
+        if (!rc) rc = batch_enqueue(b, s);
+        if (rc) return rc;
+    }
+    b->last_stream = s;
+    b->pending = true;
+    return FM_OK;
+}
+
+int fm_batch_wait(fm_batch* b, fm_op* ops) {
+    if (!b) return fail(FM_ERR_INVALID_ARG, "batch is NULL");
+    if (!b->pending) return fail(FM_ERR_INVALID_ARG, "batch was not run");
+    DeviceGuard dg(b->device);
+    cudaError_t e = cudaStreamSynchronize(b->last_stream);
+    b->pending = false;
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch", e);
+    int rc = FM_OK;
+    for (size_t i = 0; i < b->tables.size(); i++) b->tables[i]->len.store(b->h_len()[i]);
+    for (size_t i = 0; i < b->ops.size(); i++) {
+        const int st = b->h_status()[i];
+        if (ops) {
+            ops[i].result = b->h_res()[i];
+            ops[i].status = st;
+        }
+        if (st == FM_ERR_KERNEL_LAUNCH) {
+            recover(b->ops[i].table, b->ops[i].table->stream);
+            rc = fail(FM_ERR_KERNEL_LAUNCH, "batch op " + std::to_string(i) + ": round scheduling error");
+        }
+    }
+    return rc;
+}
+
+void fm_batch_destroy(fm_batch* b) {
+    if (!b) return;
+    DeviceGuard dg(b->device);
+    if (b->pending && b->last_stream) cudaStreamSynchronize(b->last_stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    cudaFree(b->d_desc);
+    cudaFree(b->d_len);
+    cudaFree(b->d_res);
+    cudaFree(b->d_status);
+    if (b->h_desc) cudaFreeHost(b->h_desc);
+    if (b->h_io) cudaFreeHost(b->h_io);
+    delete b;
+}
+
+}  // extern "C"

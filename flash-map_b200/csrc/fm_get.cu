@@ -64,9 +64,11 @@ __device__ __forceinline__ void tile_zero(uint8_t* __restrict__ dst, uint32_t vs
 // ---------------------------------------------------------------------------
 // bulk_get: one T-lane tile per query.
 // ---------------------------------------------------------------------------
+// One query by the tile of lanes [tbase, tbase+T) of the warp; qk is the
+// query key, ov / of its output value and found byte (either may be null).
 template <int KB, int VB, int T>
-__global__ void __launch_bounds__(BLOCK) k_get(TableView t, const uint8_t* __restrict__ qkeys, uint64_t n,
-                                               uint8_t* __restrict__ out_vals, uint8_t* __restrict__ out_found) {
+__device__ __forceinline__ void get_query_tile(const TableView& t, const uint8_t* __restrict__ qk,
+                                               uint8_t* __restrict__ ov, uint8_t* __restrict__ of) {
     static_assert(T == 4 || T == 8 || T == 16 || T == 32, "tile width");
     constexpr uint32_t TM = (T == 32) ? 0xFFFFFFFFu : ((1u << T) - 1u);
     const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
@@ -75,43 +77,50 @@ __global__ void __launch_bounds__(BLOCK) k_get(TableView t, const uint8_t* __res
     const uint32_t tbase = (threadIdx.x & 31u) & ~(uint32_t)(T - 1);
     const uint32_t tmask = TM << tbase;
     const uint64_t mask = t.mask;
-    const uint64_t ntiles = ((uint64_t)gridDim.x * blockDim.x) / T;
-    for (uint64_t q = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / T; q < n; q += ntiles) {
-        RegKey<KB> key;
-        key.load(qkeys + q * ksz, ksz);
-        const uint64_t h = key.hash(ksz, t.hash_mode) & mask;
-        uint64_t wbase = h & ~(uint64_t)(T - 1);  // sector-aligned window start
-        uint64_t hit = NONE64;
-        for (;;) {
-            const uint64_t pos = wbase + lane;
-            const bool before = pos < h;
-            const uint64_t p = pos - h;
-            const uint64_t slot = pos & mask;
-            const uint32_t f = __ldg(t.flags + slot);
-            const uint32_t s = st_of(f);
-            const bool past = !before && p > mask;
-            // Terminators: EMPTY, or OCCUPIED with p > dist (rayon_cpu.rs:97-111);
-            // the probe also ends once p passes the capacity (rayon_cpu.rs:91).
-            const bool term = !before && (past || s == ST_EMPTY || (s == ST_OCC && p > dist_of(f)));
-            const bool cand = !before && !past && s == ST_OCC && dist_matches(f, p);
-            const uint32_t tm = (__ballot_sync(tmask, term) >> tbase) & TM;
-            const uint32_t lim = tm ? (uint32_t)(__ffs(tm) - 1) : (uint32_t)T;
-            const bool m = cand && lane < lim && key.eq(t.keys + slot * ksz, ksz);
-            const uint32_t mm = (__ballot_sync(tmask, m) >> tbase) & TM;
-            if (mm) {
-                hit = __shfl_sync(tmask, slot, tbase + __ffs(mm) - 1);
-                break;
-            }
-            if (tm) break;
-            wbase += T;
+    RegKey<KB> key;
+    key.load(qk, ksz);
+    const uint64_t h = key.hash(ksz, t.hash_mode) & mask;
+    uint64_t wbase = h & ~(uint64_t)(T - 1);  // sector-aligned window start
+    uint64_t hit = NONE64;
+    for (;;) {
+        const uint64_t pos = wbase + lane;
+        const bool before = pos < h;
+        const uint64_t p = pos - h;
+        const uint64_t slot = pos & mask;
+        const uint32_t f = __ldg(t.flags + slot);
+        const uint32_t s = st_of(f);
+        const bool past = !before && p > mask;
+        // Terminators: EMPTY, or OCCUPIED with p > dist (rayon_cpu.rs:97-111);
+        // the probe also ends once p passes the capacity (rayon_cpu.rs:91).
+        const bool term = !before && (past || s == ST_EMPTY || (s == ST_OCC && p > dist_of(f)));
+        const bool cand = !before && !past && s == ST_OCC && dist_matches(f, p);
+        const uint32_t tm = (__ballot_sync(tmask, term) >> tbase) & TM;
+        const uint32_t lim = tm ? (uint32_t)(__ffs(tm) - 1) : (uint32_t)T;
+        const bool m = cand && lane < lim && key.eq(t.keys + slot * ksz, ksz);
+        const uint32_t mm = (__ballot_sync(tmask, m) >> tbase) & TM;
+        if (mm) {
+            hit = __shfl_sync(tmask, slot, tbase + __ffs(mm) - 1);
+            break;
         }
-        if (out_vals) {
-            uint8_t* dst = out_vals + q * vsz;
-            if (hit != NONE64) tile_copy<VB, T>(dst, t.vals + hit * vsz, vsz, lane);
-            else tile_zero<VB, T>(dst, vsz, lane);
-        }
-        if (out_found && lane == 0) out_found[q] = hit != NONE64 ? 1 : 0;
+        if (tm) break;
+        wbase += T;
     }
+    if (ov) {
+        if (hit != NONE64) tile_copy<VB, T>(ov, t.vals + hit * vsz, vsz, lane);
+        else tile_zero<VB, T>(ov, vsz, lane);
+    }
+    if (of && lane == 0) *of = hit != NONE64 ? 1 : 0;
+}
+
+template <int KB, int VB, int T>
+__global__ void __launch_bounds__(BLOCK) k_get(TableView t, const uint8_t* __restrict__ qkeys, uint64_t n,
+                                               uint8_t* __restrict__ out_vals, uint8_t* __restrict__ out_found) {
+    const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
+    const uint32_t vsz = VB ? (uint32_t)VB : t.vsz;
+    const uint64_t ntiles = ((uint64_t)gridDim.x * blockDim.x) / T;
+    for (uint64_t q = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / T; q < n; q += ntiles)
+        get_query_tile<KB, VB, T>(t, qkeys + q * ksz, out_vals ? out_vals + q * vsz : nullptr,
+                                  out_found ? out_found + q : nullptr);
 }
 
 // Count OCCUPIED slots (kernels.cu:328-337), reduced per block.
@@ -138,63 +147,133 @@ __global__ void __launch_bounds__(BLOCK) k_count(const uint32_t* __restrict__ fl
 // as with one query per 8-lane tile, which is what a chain of dependent
 // random reads (key -> metadata -> key -> value) needs.
 template <int KB, int VB>
-__global__ void __launch_bounds__(BLOCK) k_get_thread(TableView t, const uint8_t* __restrict__ qkeys, uint64_t n,
-                                                      uint8_t* __restrict__ out_vals,
-                                                      uint8_t* __restrict__ out_found) {
+__device__ __forceinline__ void get_query_thread(const TableView& t, const uint8_t* __restrict__ qk,
+                                                 uint8_t* __restrict__ ov, uint8_t* __restrict__ of) {
     const uint64_t mask = t.mask;
-    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (uint64_t)gridDim.x * blockDim.x) {
-        RegKey<KB> key;
-        key.load(qkeys + q * KB, KB);
-        const uint64_t h = key.hash(KB, t.hash_mode) & mask;
-        uint64_t wb = h & ~7ull;
-        uint64_t hit = NONE64;
-        bool done = false;
-        while (!done) {
-            const uint4* fp = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
-            const uint4 a = __ldg(fp), b = __ldg(fp + 1);
-            const uint32_t f8[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    RegKey<KB> key;
+    key.load(qk, KB);
+    const uint64_t h = key.hash(KB, t.hash_mode) & mask;
+    uint64_t wb = h & ~7ull;
+    uint64_t hit = NONE64;
+    bool done = false;
+    while (!done) {
+        const uint4* fp = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
+        const uint4 a = __ldg(fp), b = __ldg(fp + 1);
+        const uint32_t f8[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
-            for (int l = 0; l < 8; l++) {
-                const uint64_t pos = wb + l;
-                if (done || pos < h) continue;
-                const uint64_t p = pos - h;
-                const uint32_t f = f8[l];
-                const uint32_t s = st_of(f);
-                // Terminators: probe past the capacity, EMPTY, or OCCUPIED with
-                // p > dist (rayon_cpu.rs:91-111); tombstones are skipped.
-                if (p > mask || s == ST_EMPTY || (s == ST_OCC && p > dist_of(f))) {
-                    done = true;
-                } else if (s == ST_OCC && dist_matches(f, p) && key.eq(t.keys + (pos & mask) * KB, KB)) {
-                    hit = pos & mask;
-                    done = true;
-                }
+        for (int l = 0; l < 8; l++) {
+            const uint64_t pos = wb + l;
+            if (done || pos < h) continue;
+            const uint64_t p = pos - h;
+            const uint32_t f = f8[l];
+            const uint32_t s = st_of(f);
+            // Terminators: probe past the capacity, EMPTY, or OCCUPIED with
+            // p > dist (rayon_cpu.rs:91-111); tombstones are skipped.
+            if (p > mask || s == ST_EMPTY || (s == ST_OCC && p > dist_of(f))) {
+                done = true;
+            } else if (s == ST_OCC && dist_matches(f, p) && key.eq(t.keys + (pos & mask) * KB, KB)) {
+                hit = pos & mask;
+                done = true;
             }
-            wb += 8;
         }
-        if (out_vals) {
-            RegVal<VB> v;
-            if (hit != NONE64) v.load_ro(t.vals + hit * VB);
-            else v.zero();
-            v.store(out_vals + q * VB, VB);
-        }
-        if (out_found) out_found[q] = hit != NONE64 ? 1 : 0;
+        wb += 8;
     }
+    if (ov) {
+        RegVal<VB> v;
+        if (hit != NONE64) v.load_ro(t.vals + hit * VB);
+        else v.zero();
+        v.store(ov, VB);
+    }
+    if (of) *of = hit != NONE64 ? 1 : 0;
 }
 
 template <int KB, int VB>
-cudaError_t get_shape(const TableView& t, const uint8_t* q, uint64_t n, uint8_t* ov, uint8_t* of, cudaStream_t s) {
-    if constexpr (KB != 0 && VB != 0) {
-        if (t.mask >= 7) {
-            KtScope kt(KC_GET, s);
-            k_get_thread<KB, VB><<<grid_for(n, 64), BLOCK, 0, s>>>(t, q, n, ov, of);
-            g_launches += 1;
-            return cudaGetLastError();
+__global__ void __launch_bounds__(BLOCK) k_get_thread(TableView t, const uint8_t* __restrict__ qkeys, uint64_t n,
+                                                      uint8_t* __restrict__ out_vals,
+                                                      uint8_t* __restrict__ out_found) {
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (uint64_t)gridDim.x * blockDim.x)
+        get_query_thread<KB, VB>(t, qkeys + q * KB, out_vals ? out_vals + q * VB : nullptr,
+                                 out_found ? out_found + q : nullptr);
+}
+
+// Grouped lookups: the gets of a batch wave, one flat index space over their
+// queries (prefix[o] = first flat index of get o), T lanes per query (T == 1:
+// one thread per query).  Load-balanced over gets of any sizes.
+template <int KB, int VB, int T>
+__global__ void __launch_bounds__(BLOCK) k_grp_get(const GroupGet* __restrict__ ops,
+                                                   const uint64_t* __restrict__ prefix, uint32_t nops,
+                                                   uint64_t total) {
+    const uint64_t units = ((uint64_t)gridDim.x * blockDim.x) / T;
+    for (uint64_t q = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / T; q < total; q += units) {
+        uint32_t lo = 0, hi = nops;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(prefix + mid) <= q) lo = mid;
+            else hi = mid;
         }
+        const GroupGet& g = ops[lo];
+        const uint64_t i = q - __ldg(prefix + lo);
+        const uint32_t ksz = KB ? (uint32_t)KB : g.t.ksz;
+        const uint32_t vsz = VB ? (uint32_t)VB : g.t.vsz;
+        uint8_t* ov = g.out_vals ? g.out_vals + i * vsz : nullptr;
+        uint8_t* of = g.out_found ? g.out_found + i : nullptr;
+        if constexpr (T == 1) get_query_thread<KB, VB>(g.t, g.keys + i * ksz, ov, of);
+        else get_query_tile<KB, VB, T>(g.t, g.keys + i * ksz, ov, of);
     }
-    constexpr int T = 8;
+}
+
+// Tuned lookup configurations, per shape and load bucket (0: not measured).
+GetCfg g_tuned[SHAPE_GENERIC + 1][LOAD_BUCKETS];
+
+template <int KB, int VB, int T>
+void get_launch(const TableView& t, const uint8_t* q, uint64_t n, uint8_t* ov, uint8_t* of, int bps,
+                cudaStream_t s) {
     KtScope kt(KC_GET, s);
-    k_get<KB, VB, T><<<grid_for(n * T, 16), BLOCK, 0, s>>>(t, q, n, ov, of);
+    if constexpr (T == 1) k_get_thread<KB, VB><<<grid_for(n, bps), BLOCK, 0, s>>>(t, q, n, ov, of);
+    else k_get<KB, VB, T><<<grid_for(n * T, bps), BLOCK, 0, s>>>(t, q, n, ov, of);
     g_launches += 1;
+}
+
+template <int KB, int VB>
+cudaError_t get_shape(const TableView& t, const uint8_t* q, uint64_t n, uint8_t* ov, uint8_t* of, GetCfg cfg,
+                      cudaStream_t s) {
+    int lanes = cfg.lanes;
+    // one thread per query needs compile-time sizes and 8-slot windows
+    if (lanes == 1 && !(KB != 0 && VB != 0 && t.mask >= 7)) lanes = 8;
+    switch (lanes) {
+        case 1:
+            if constexpr (KB != 0 && VB != 0) get_launch<KB, VB, 1>(t, q, n, ov, of, cfg.blocks_per_sm, s);
+            break;
+        case 4: get_launch<KB, VB, 4>(t, q, n, ov, of, cfg.blocks_per_sm, s); break;
+        case 16: get_launch<KB, VB, 16>(t, q, n, ov, of, cfg.blocks_per_sm, s); break;
+        case 32: get_launch<KB, VB, 32>(t, q, n, ov, of, cfg.blocks_per_sm, s); break;
+        default: get_launch<KB, VB, 8>(t, q, n, ov, of, cfg.blocks_per_sm, s); break;
+    }
+    return cudaGetLastError();
+}
+
+template <int KB, int VB, int T>
+void grp_get_launch(const GroupGet* ops, const uint64_t* prefix, uint32_t nops, uint64_t total, int bps,
+                    cudaStream_t s) {
+    KtScope kt(KC_GET, s);
+    k_grp_get<KB, VB, T><<<grid_for(total * T, bps), BLOCK, 0, s>>>(ops, prefix, nops, total);
+    g_launches += 1;
+}
+
+template <int KB, int VB>
+cudaError_t grp_get_shape(const GroupGet* ops, const uint64_t* prefix, uint32_t nops, uint64_t total, GetCfg cfg,
+                          cudaStream_t s) {
+    int lanes = cfg.lanes;
+    if (lanes == 1 && !(KB != 0 && VB != 0)) lanes = 8;
+    switch (lanes) {
+        case 1:
+            if constexpr (KB != 0 && VB != 0) grp_get_launch<KB, VB, 1>(ops, prefix, nops, total, cfg.blocks_per_sm, s);
+            break;
+        case 4: grp_get_launch<KB, VB, 4>(ops, prefix, nops, total, cfg.blocks_per_sm, s); break;
+        case 16: grp_get_launch<KB, VB, 16>(ops, prefix, nops, total, cfg.blocks_per_sm, s); break;
+        case 32: grp_get_launch<KB, VB, 32>(ops, prefix, nops, total, cfg.blocks_per_sm, s); break;
+        default: grp_get_launch<KB, VB, 8>(ops, prefix, nops, total, cfg.blocks_per_sm, s); break;
+    }
     return cudaGetLastError();
 }
 
@@ -228,17 +307,49 @@ Shape pick_shape(uint32_t k, uint32_t v) {
     return SHAPE_GENERIC;
 }
 
+#define FM_GET_SWITCH(sh, CALL)                          \
+    switch (sh) {                                        \
+        case SHAPE_8_8: return CALL(8, 8);               \
+        case SHAPE_32_128: return CALL(32, 128);         \
+        case SHAPE_32_64: return CALL(32, 64);           \
+        case SHAPE_32_32: return CALL(32, 32);           \
+        case SHAPE_8_32: return CALL(8, 32);             \
+        default: return CALL(0, 0);                      \
+    }
+
+cudaError_t launch_get_cfg(const TableView& t, Shape sh, const uint8_t* q, uint64_t n, uint8_t* ov, uint8_t* of,
+                           GetCfg cfg, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+#define FM_CALL(K, V) get_shape<K, V>(t, q, n, ov, of, cfg, s)
+    FM_GET_SWITCH(sh, FM_CALL)
+#undef FM_CALL
+}
+
+GetCfg tuned_get_cfg(Shape sh, double load) {
+    const GetCfg c = g_tuned[sh][load_bucket(load)];
+    if (c.lanes > 0 && c.blocks_per_sm > 0) return c;
+    GetCfg d;  // measured default on B200: one thread per query, 64 blocks per SM
+    if (sh == SHAPE_GENERIC) d.lanes = 8, d.blocks_per_sm = 16;
+    return d;
+}
+
+void set_tuned_get_cfg(Shape sh, int bucket, GetCfg cfg) {
+    if (bucket >= 0 && bucket < LOAD_BUCKETS) g_tuned[sh][bucket] = cfg;
+}
+
 cudaError_t launch_get(const TableView& t, Shape sh, const uint8_t* q, uint64_t n, uint8_t* ov, uint8_t* of,
                        cudaStream_t s) {
-    if (n == 0) return cudaSuccess;
-    switch (sh) {
-        case SHAPE_8_8: return get_shape<8, 8>(t, q, n, ov, of, s);
-        case SHAPE_32_128: return get_shape<32, 128>(t, q, n, ov, of, s);
-        case SHAPE_32_64: return get_shape<32, 64>(t, q, n, ov, of, s);
-        case SHAPE_32_32: return get_shape<32, 32>(t, q, n, ov, of, s);
-        case SHAPE_8_32: return get_shape<8, 32>(t, q, n, ov, of, s);
-        default: return get_shape<0, 0>(t, q, n, ov, of, s);
-    }
+    GetCfg cfg;
+    if (sh == SHAPE_GENERIC) cfg.lanes = 8, cfg.blocks_per_sm = 16;
+    return launch_get_cfg(t, sh, q, n, ov, of, cfg, s);
+}
+
+cudaError_t launch_grp_get(Shape sh, const GroupGet* ops, const uint64_t* prefix, uint32_t nops, uint64_t total,
+                           GetCfg cfg, cudaStream_t s) {
+    if (total == 0 || nops == 0) return cudaSuccess;
+#define FM_CALL(K, V) grp_get_shape<K, V>(ops, prefix, nops, total, cfg, s)
+    FM_GET_SWITCH(sh, FM_CALL)
+#undef FM_CALL
 }
 
 cudaError_t launch_count(const TableView& t, Ctl* ctl, cudaStream_t s) {

@@ -476,15 +476,15 @@ __device__ __forceinline__ int exec_insert_generic(const TableView& t, const uin
 }
 
 // Phase 3 for op j (one thread per op): run it if it leads an unblocked
-// segment of a non-serial round, then clear its registration.  Returns whether
-// it ran.  A walk too long for the thread path is appended to long_list (when
-// given; it then counts as run: its segment is disjoint from every other
-// segment of the round, so running it after them gives the same result),
-// otherwise it takes the scalar walk.
+// segment of a non-serial round, then clear its registration.  Returns 0 when
+// it did not run, 1 when it ran and 2 when its walk is too long for the
+// thread path and `defer` allows handing it to the tile pass (it then counts
+// as run: its segment is disjoint from every other segment of the round, so
+// running it after them gives the same result); without `defer` such a walk
+// takes the scalar path.
 template <int KB, int VB>
-__device__ __forceinline__ bool finish_op(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t j,
-                                          bool serial, const OpScratch& sc, ExecAcc& a, uint32_t* long_list = nullptr,
-                                          uint32_t* long_n = nullptr) {
+__device__ __forceinline__ int finish_op(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t j,
+                                         bool serial, const OpScratch& sc, ExecAcc& a, bool defer) {
     const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
     const uint32_t vsz = VB ? (uint32_t)VB : t.vsz;
     if constexpr (KB == 0 || VB == 0) {
@@ -496,7 +496,7 @@ __device__ __forceinline__ bool finish_op(const TableView& t, const uint8_t* key
             t.seg_cnt[F] = 0;
         }
         sc.op_word[j] = IDLE;
-        return run;
+        return run ? 1 : 0;
     } else {
         // independent loads issued together: decision words, registration, key
         const uint8_t lead = sc.op_flag[j];
@@ -505,24 +505,23 @@ __device__ __forceinline__ bool finish_op(const TableView& t, const uint8_t* key
         RegKey<KB> key;
         key.load(keys + (uint64_t)j * ksz, ksz);
         const bool run = !serial && lead != 0 && blk > j;
-        bool defer = false;
+        int code = run ? 1 : 0;
         if (run) {
             // windows need capacity >= 8; consecutive walk positions need
             // probe depths below 2^28 (the stored distance width)
             int c = -1;
             if (t.mask >= 7 && t.mask < (uint64_t)DIST_MASK)
                 c = exec_insert_thread<KB, VB>(t, key, keys + (uint64_t)j * ksz, vals + (uint64_t)j * vsz, a);
-            if (c < 0 && long_list) defer = true;
+            if (c < 0 && defer) code = 2;
             else if (c < 0) c = exec_insert_key<KB, VB>(t, key, vals + (uint64_t)j * vsz, a);
             if (c > 0) a.claimed += c;
         }
-        if (long_list) append(long_list, long_n, j, defer);
         if (F != NONE64) {
             t.seg_min[F] = IDLE;
             t.seg_cnt[F] = 0;
         }
         sc.op_word[j] = IDLE;
-        return run;
+        return code;
     }
 }
 
@@ -1003,7 +1002,9 @@ __global__ void __launch_bounds__(RBLOCK, 3) k_ins_p3(TableView t, const uint8_t
         bool ran = false;
         if (valid) {
             j = ops.op(i);
-            ran = finish_op<KB, VB>(t, keys, vals, j, serial, sc, a, sc.long_list, long_n);
+            const int code = finish_op<KB, VB>(t, keys, vals, j, serial, sc, a, true);
+            if constexpr (KB != 0 && VB != 0) append(sc.long_list, long_n, j, code == 2);
+            ran = code != 0;
         }
         block_append(out, out_n, j, valid && !ran, s_app);
     }
@@ -1091,9 +1092,9 @@ __global__ void __launch_bounds__(RBLOCK, 3) k_ins_p4(TableView t, const uint8_t
 // counts are zero (the host's done marker).
 
 template <int KB, int VB, int T>
-__global__ void __launch_bounds__(TAIL_THREADS) k_ins_tail(TableView t, const uint8_t* __restrict__ keys,
-                                                           const uint8_t* __restrict__ vals, uint32_t n0,
-                                                           uint32_t r0, uint32_t nops, OpScratch sc, Ctl* ctl) {
+__device__ __forceinline__ void ins_tail_body(const TableView& t, const uint8_t* __restrict__ keys,
+                                              const uint8_t* __restrict__ vals, uint32_t n0, uint32_t r0,
+                                              uint32_t nops, const OpScratch& sc, Ctl* ctl, uint32_t limit) {
     // tiles holding a chain buffer (T > 1): as many as the static shared
     // memory allows; the block's other warps idle in the tile phases
     constexpr int NT = T > 1 ? (TAIL_THREADS / T < 12 ? TAIL_THREADS / T : 12) : 1;
@@ -1107,7 +1108,7 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_ins_tail(TableView t, const ui
     }
     __syncthreads();
     uint32_t n = s_n;
-    if (n == 0 || n > TAIL_MAX) return;
+    if (n == 0 || n > limit) return;
     ExecAcc a;
     uint32_t r = r0;
     uint32_t rounds = 0;
@@ -1171,7 +1172,7 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_ins_tail(TableView t, const ui
                 const Tile<(T > 1 ? T : 8)> tl;
                 ran = finish_tile<KB, VB, (T > 1 ? T : 8)>(t, keys, vals, j, false, sc, tl, s_chain[unit], a);
             } else {
-                ran = finish_op<KB, VB>(t, keys, vals, j, false, sc, a);
+                ran = finish_op<KB, VB>(t, keys, vals, j, false, sc, a, false) != 0;
             }
             if (!ran && leader_lane) out[atomicAdd(&s_next, 1u)] = j;
         }
@@ -1204,6 +1205,13 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_ins_tail(TableView t, const ui
     }
 }
 
+template <int KB, int VB, int T>
+__global__ void __launch_bounds__(TAIL_THREADS) k_ins_tail(TableView t, const uint8_t* __restrict__ keys,
+                                                           const uint8_t* __restrict__ vals, uint32_t n0,
+                                                           uint32_t r0, uint32_t nops, OpScratch sc, Ctl* ctl) {
+    ins_tail_body<KB, VB, T>(t, keys, vals, n0, r0, nops, sc, ctl, TAIL_MAX);
+}
+
 // Host-launched fallback for a serial round whose pending count is above
 // TAIL_MAX: applies round r's ops in index order.
 template <int KB, int VB>
@@ -1228,6 +1236,153 @@ __global__ void __launch_bounds__(1024) k_ins_serial(TableView t, const uint8_t*
 }
 
 constexpr int INS_T = 32;  // lanes per insert in the single-block tail
+
+// ---- grouped rounds (batch waves) ------------------------------------------
+//
+// The same phases over the inserts of a batch wave (distinct tables), one
+// launch per phase for all of them: a flat item index is mapped to (op, item)
+// through the prefix of the ops' pending counts, list appends and counts are
+// aggregated over the lanes of a warp working on the same op, and the tail
+// runs one block per op until every op is done.
+
+__device__ __forceinline__ uint32_t grp_pending(const GroupOp* ops, uint32_t o, uint32_t r) {
+    const Ctl* c = ops[o].ctl;
+    return r == 0 ? *(volatile const uint32_t*)&c->n0 : *(volatile const uint32_t*)&c->npend[r & 1];
+}
+
+__device__ __forceinline__ void grp_rare(Ctl* ctl, const ExecAcc& a) {
+    if (a.maxd > *(volatile uint32_t*)&ctl->dmax) atomicMax(&ctl->dmax, a.maxd);
+    if (a.tomb && !*(volatile uint32_t*)&ctl->tomb_claimed) ctl->tomb_claimed = 1u;
+    if (a.limit) atomicOr(&ctl->err, ERR_WALK_LIMIT);
+}
+
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_grp_ins_p1(const GroupOp* __restrict__ ops, uint32_t nops, uint32_t r) {
+    __shared__ uint32_t s_pre[GROUP_MAX + 1];
+    const uint32_t total = group_prefix(nops, [&](uint32_t o) { return grp_pending(ops, o, r); }, s_pre);
+    if (blockIdx.x == 0)
+        for (uint32_t o = threadIdx.x; o < nops; o += blockDim.x) reset_next_round(ops[o].ctl, r);
+    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < total; f += gridDim.x * blockDim.x) {
+        const uint32_t o = group_find(s_pre, nops, f);
+        const GroupOp& g = ops[o];
+        const uint32_t i = f - s_pre[o];
+        const uint32_t j = r == 0 ? i : pend_of(g.sc, r)[i];
+        const uint64_t F = find_free<KB>(g.t, g.keys, j);
+        register_op(g.t, j, F, g.sc.op_slot);
+        if (F == NONE64) g.ctl->serial[r & 1] = 1u;
+    }
+}
+
+__global__ void __launch_bounds__(RBLOCK) k_grp_ins_p2(const GroupOp* __restrict__ ops, uint32_t nops, uint32_t r) {
+    __shared__ uint32_t s_pre[GROUP_MAX + 1];
+    const uint32_t total = group_prefix(nops, [&](uint32_t o) { return grp_pending(ops, o, r); }, s_pre);
+    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < total; f += gridDim.x * blockDim.x) {
+        const uint32_t o = group_find(s_pre, nops, f);
+        const GroupOp& g = ops[o];
+        const uint32_t i = f - s_pre[o];
+        const uint32_t j = r == 0 ? i : pend_of(g.sc, r)[i];
+        const uint32_t bits = walk_op(g.t, j, g.n, g.sc.op_slot, g.sc.op_word, g.sc.op_flag);
+        if (bits & 1u) g.ctl->serial[r & 1] = 1u;
+        if (bits & 2u) atomicOr(&g.ctl->err, ERR_SCRATCH);
+    }
+}
+
+template <int KB, int VB>
+__global__ void __launch_bounds__(RBLOCK, 3) k_grp_ins_p3(const GroupOp* __restrict__ ops, uint32_t nops,
+                                                          uint32_t r) {
+    __shared__ uint32_t s_pre[GROUP_MAX + 1];
+    const uint32_t total = group_prefix(nops, [&](uint32_t o) { return grp_pending(ops, o, r); }, s_pre);
+    if (blockIdx.x == 0)
+        for (uint32_t o = threadIdx.x; o < nops; o += blockDim.x)
+            if (s_pre[o + 1] > s_pre[o]) atomicAdd(&ops[o].ctl->rounds, 1u);
+    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < total; f += gridDim.x * blockDim.x) {
+        const uint32_t o = group_find(s_pre, nops, f);
+        const GroupOp& g = ops[o];
+        const uint32_t i = f - s_pre[o];
+        const uint32_t j = r == 0 ? i : pend_of(g.sc, r)[i];
+        const bool serial = *(volatile uint32_t*)&g.ctl->serial[r & 1] != 0;
+        ExecAcc a;
+        const int code = finish_op<KB, VB>(g.t, g.keys, g.vals, j, serial, g.sc, a, KB != 0 && VB != 0);
+        append_peer(pend_of(g.sc, r + 1), &g.ctl->npend[(r + 1) & 1], j, code == 0, o);
+        if constexpr (KB != 0 && VB != 0) append_peer(g.sc.long_list, &g.ctl->nlong[r & 1], j, code == 2, o);
+        add_peer(g.ctl, a.claimed, o);
+        grp_rare(g.ctl, a);
+    }
+}
+
+template <int KB, int VB>
+__global__ void __launch_bounds__(RBLOCK, 3) k_grp_ins_p4(const GroupOp* __restrict__ ops, uint32_t nops,
+                                                          uint32_t r) {
+    constexpr int NW = RBLOCK / 32;
+    __shared__ uint32_t s_pre[GROUP_MAX + 1];
+    __shared__ TileChain s_chain[NW];
+    const uint32_t total = group_prefix(
+        nops, [&](uint32_t o) { return *(volatile const uint32_t*)&ops[o].ctl->nlong[r & 1]; }, s_pre);
+    if (total == 0) return;  // block-uniform
+    const Tile<32> tl;
+    const uint32_t w = threadIdx.x >> 5;
+    for (uint32_t f = blockIdx.x * NW + w; f < total; f += gridDim.x * NW) {  // warp-uniform
+        const uint32_t o = group_find(s_pre, nops, f);
+        const GroupOp& g = ops[o];
+        const uint32_t j = g.sc.long_list[f - s_pre[o]];
+        RegKey<KB> key;
+        key.load(g.keys + (uint64_t)j * KB, KB);
+        ExecAcc a;
+        if (g.t.mask >= 4 * 32 - 1) {
+            exec_tile<KB, VB, 32>(g.t, key, g.vals, j, tl, s_chain[w], a);
+        } else {
+            if (tl.lane == 0) a.claimed += exec_insert_key<KB, VB>(g.t, key, g.vals + (uint64_t)j * VB, a);
+        }
+        tl.sync();
+        a.maxd = __reduce_max_sync(0xFFFFFFFFu, a.maxd);
+        a.tomb = __any_sync(0xFFFFFFFFu, a.tomb);
+        a.limit = __any_sync(0xFFFFFFFFu, a.limit);
+        a.claimed = __reduce_add_sync(0xFFFFFFFFu, a.claimed);
+        if (tl.lane == 0) {
+            if (a.claimed) atomicAdd(&g.ctl->count_part[blockIdx.x % COUNT_PARTS][0], (unsigned long long)a.claimed);
+            grp_rare(g.ctl, a);
+        }
+    }
+}
+
+template <int KB, int VB, int T>
+__global__ void __launch_bounds__(TAIL_THREADS) k_grp_ins_tail(const GroupOp* __restrict__ ops, uint32_t r0) {
+    const GroupOp& g = ops[blockIdx.x];
+    const uint32_t n0 = *(volatile const uint32_t*)&g.ctl->n0;
+    ins_tail_body<KB, VB, T>(g.t, g.keys, g.vals, n0, r0, g.n, g.sc, g.ctl, 0xFFFFFFFFu);
+}
+
+constexpr uint32_t GRP_ROUNDS = 3;  // grid rounds before the block-per-op tail
+
+template <int KB, int VB>
+void grp_ins_shape(const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream_t s) {
+    const unsigned g = grid_for(sum_n, 8);
+    k_grp_setup<<<nops, 256, 0, s>>>(ops, 1);
+    for (uint32_t r = 0; r < GRP_ROUNDS; r++) {
+        {
+            KtScope kt(KC_INS_FIND, s);
+            k_grp_ins_p1<KB><<<g, RBLOCK, 0, s>>>(ops, nops, r);
+        }
+        {
+            KtScope kt(KC_INS_WALK, s);
+            k_grp_ins_p2<<<g, RBLOCK, 0, s>>>(ops, nops, r);
+        }
+        {
+            KtScope kt(KC_INS_EXEC, s);
+            k_grp_ins_p3<KB, VB><<<g, RBLOCK, 0, s>>>(ops, nops, r);
+        }
+        if constexpr (KB != 0 && VB != 0) {
+            KtScope kt(KC_INS_LONG, s);
+            k_grp_ins_p4<KB, VB><<<g, RBLOCK, 0, s>>>(ops, nops, r);
+        }
+    }
+    {
+        KtScope kt(KC_INS_TAIL, s);
+        k_grp_ins_tail<KB, VB, (KB && VB) ? INS_T : 1><<<nops, TAIL_THREADS, 0, s>>>(ops, GRP_ROUNDS);
+    }
+    k_grp_finish<<<(nops + 255) / 256, 256, 0, s>>>(ops, nops, 1);
+    count_launches(2 + GRP_ROUNDS * ((KB != 0 && VB != 0) ? 4 : 3) + 1 + 1);
+}
 
 template <int KB, int VB>
 void rounds_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, uint32_t r0,
@@ -1297,6 +1452,14 @@ cudaError_t launch_ins_rounds(const TableView& t, Shape sh, const uint8_t* keys,
 cudaError_t launch_ins_tail(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
                             uint32_t r, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
 #define FM_CALL(K, V) tail_shape<K, V>(t, keys, vals, n0, r, n0, sc, ctl, s)
+    FM_SHAPE_SWITCH(sh, FM_CALL)
+#undef FM_CALL
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grp_ins(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream_t s) {
+    if (nops == 0) return cudaSuccess;
+#define FM_CALL(K, V) grp_ins_shape<K, V>(ops, nops, sum_n, s)
     FM_SHAPE_SWITCH(sh, FM_CALL)
 #undef FM_CALL
     return cudaGetLastError();

@@ -27,20 +27,28 @@ struct Ctl {
     uint32_t err;            // device-side error bits
     uint32_t rounds;         // rounds run by the call (statistics)
     uint32_t nlong[2];       // inserts deferred to the warp-per-op pass, per round parity
+    uint32_t n0;             // grouped (batch) calls: the call's op count after the precheck
+    uint32_t pad_;
     unsigned long long count;  // new keys (insert) / removed keys (remove), single-block kernels
     unsigned long long count_part[COUNT_PARTS][4];  // the same from grid kernels, [i][0] used
     // Persistent table facts (survive across calls, reset by clear):
     uint32_t dmax;           // largest probe distance ever stored since clear
     uint32_t tomb_claimed;   // 1 once an insert reused a tombstone since clear
     unsigned long long occupied;  // recount result
-    unsigned long long total_count() const {
+    __host__ __device__ unsigned long long total_count() const {
         unsigned long long s = count;
         for (int i = 0; i < COUNT_PARTS; i++) s += count_part[i][0];
         return s;
     }
 };
-constexpr size_t CTL_CALL_BYTES = 40 + 32 * COUNT_PARTS;  // npend .. count_part
+constexpr size_t CTL_CALL_BYTES = 48 + 32 * COUNT_PARTS;  // npend .. count_part
 static_assert(offsetof(Ctl, dmax) == CTL_CALL_BYTES, "Ctl layout");
+
+// Op status codes written by device code (the FM_* values of the C ABI).
+constexpr int STATUS_OK = 0;
+constexpr int STATUS_KERNEL = 3;       // FM_ERR_KERNEL_LAUNCH
+constexpr int STATUS_TABLE_FULL = 5;   // FM_ERR_TABLE_FULL
+constexpr int STATUS_PROBE_LIMIT = 9;  // FM_ERR_PROBE_LIMIT
 
 // Device-side error bits (Ctl::err).
 constexpr uint32_t ERR_WALK_LIMIT = 1u;   // an insert walk passed 2*capacity+2 slots (full table)
@@ -91,6 +99,58 @@ cudaError_t launch_rem_tail(const TableView& t, Shape sh, const uint8_t* keys, u
 cudaError_t launch_count(const TableView& t, Ctl* ctl, cudaStream_t s);
 int num_sms();
 unsigned long long launch_count();
+
+// ---- grouped (batch) execution ---------------------------------------------
+//
+// A batch wave runs many bulk operations on distinct tables with one launch
+// per phase: every thread maps a flat item index to (op, item) through a
+// prefix of the ops' item counts.  GROUP_MAX bounds the ops of one launch.
+constexpr uint32_t GROUP_MAX = 1024;
+
+// One get of a wave.
+struct GroupGet {
+    TableView t;
+    const uint8_t* keys;
+    uint8_t* out_vals;   // may be null (values not wanted)
+    uint8_t* out_found;  // may be null
+};
+
+// One insert or remove of a wave, on its table's control block and scratch.
+struct GroupOp {
+    TableView t;
+    const uint8_t* keys;
+    const uint8_t* vals;        // insert values
+    OpScratch sc;
+    Ctl* ctl;
+    unsigned long long* len;    // the table's element count within the batch
+    unsigned long long* result; // new keys / removed keys
+    int* status;                // FM status of the op
+    uint32_t n;                 // requested ops
+    uint32_t counted;           // insert: precheck and count (1)
+};
+
+// Lookup kernel configuration: lanes per query (1: one thread per query with
+// 8-slot windows; 4..32: a tile) and resident blocks per SM for the grid.
+struct GetCfg {
+    int lanes = 1;
+    int blocks_per_sm = 64;
+};
+cudaError_t launch_get_cfg(const TableView& t, Shape sh, const uint8_t* qkeys, uint64_t n, uint8_t* out_vals,
+                           uint8_t* out_found, GetCfg cfg, cudaStream_t s);
+// The tuned configuration for a table (defaults when none was measured).
+GetCfg tuned_get_cfg(Shape sh, double load);
+void set_tuned_get_cfg(Shape sh, int load_bucket, GetCfg cfg);
+constexpr int LOAD_BUCKETS = 3;  // load < 0.6, < 0.8, >= 0.8
+inline int load_bucket(double load) { return load < 0.6 ? 0 : (load < 0.8 ? 1 : 2); }
+
+// Grouped launchers (all ops of one call share the shape).  `prefix` holds
+// the nops+1 exclusive prefix sums of the gets' sizes (device memory).
+cudaError_t launch_grp_get(Shape sh, const GroupGet* ops, const uint64_t* prefix, uint32_t nops, uint64_t total,
+                           GetCfg cfg, cudaStream_t s);
+// Precheck, grid rounds, block-per-op tail to completion, and the result
+// write-back, stream-ordered with no host synchronisation.
+cudaError_t launch_grp_ins(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream_t s);
+cudaError_t launch_grp_rem(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream_t s);
 
 // Optional device timing per kernel class: while a table's timing is on, the
 // library records a CUDA event pair around each launch made for it on the

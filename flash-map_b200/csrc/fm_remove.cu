@@ -170,13 +170,13 @@ __global__ void __launch_bounds__(RBLOCK) k_rem_p3(TableView t, const uint8_t* _
 }
 
 template <int KB>
-__global__ void __launch_bounds__(TAIL_THREADS) k_rem_tail(TableView t, const uint8_t* __restrict__ keys,
-                                                           uint32_t n0, uint32_t r0, OpScratch sc, Ctl* ctl) {
+__device__ __forceinline__ void rem_tail_body(const TableView& t, const uint8_t* __restrict__ keys, uint32_t n0,
+                                              uint32_t r0, const OpScratch& sc, Ctl* ctl, uint32_t limit) {
     __shared__ uint32_t s_n, s_next;
     if (threadIdx.x == 0) s_n = (r0 == 0) ? n0 : *(volatile uint32_t*)&ctl->npend[r0 & 1];
     __syncthreads();
     uint32_t n = s_n;
-    if (n == 0 || n > TAIL_MAX) return;
+    if (n == 0 || n > limit) return;
     const uint64_t dmax = *(volatile uint32_t*)&ctl->dmax;
     uint32_t removed = 0, rounds = 0;
     uint32_t r = r0;
@@ -220,6 +220,102 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_rem_tail(TableView t, const ui
 }
 
 template <int KB>
+__global__ void __launch_bounds__(TAIL_THREADS) k_rem_tail(TableView t, const uint8_t* __restrict__ keys,
+                                                           uint32_t n0, uint32_t r0, OpScratch sc, Ctl* ctl) {
+    rem_tail_body<KB>(t, keys, n0, r0, sc, ctl, TAIL_MAX);
+}
+
+// ---- grouped rounds (batch waves): the removes of a wave, one launch per
+// phase for all of them (see the grouped inserts in fm_insert.cu) -----------
+
+__device__ __forceinline__ uint32_t grp_rem_pending(const GroupOp* ops, uint32_t o, uint32_t r) {
+    const Ctl* c = ops[o].ctl;
+    return r == 0 ? *(volatile const uint32_t*)&c->n0 : *(volatile const uint32_t*)&c->npend[r & 1];
+}
+
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_grp_rem_p1(const GroupOp* __restrict__ ops, uint32_t nops, uint32_t r) {
+    __shared__ uint32_t s_pre[GROUP_MAX + 1];
+    const uint32_t total = group_prefix(nops, [&](uint32_t o) { return grp_rem_pending(ops, o, r); }, s_pre);
+    if (blockIdx.x == 0)
+        for (uint32_t o = threadIdx.x; o < nops; o += blockDim.x) reset_next_round(ops[o].ctl, r);
+    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < total; f += gridDim.x * blockDim.x) {
+        const uint32_t o = group_find(s_pre, nops, f);
+        const GroupOp& g = ops[o];
+        const uint32_t i = f - s_pre[o];
+        const uint32_t j = r == 0 ? i : pend_of(g.sc, r)[i];
+        scan_op<KB>(g.t, g.keys, j, *(volatile uint32_t*)&g.ctl->dmax, g.sc);
+    }
+}
+
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_grp_rem_p2(const GroupOp* __restrict__ ops, uint32_t nops, uint32_t r) {
+    __shared__ uint32_t s_pre[GROUP_MAX + 1];
+    const uint32_t total = group_prefix(nops, [&](uint32_t o) { return grp_rem_pending(ops, o, r); }, s_pre);
+    if (blockIdx.x == 0)
+        for (uint32_t o = threadIdx.x; o < nops; o += blockDim.x)
+            if (s_pre[o + 1] > s_pre[o]) atomicAdd(&ops[o].ctl->rounds, 1u);
+    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < total; f += gridDim.x * blockDim.x) {
+        const uint32_t o = group_find(s_pre, nops, f);
+        const GroupOp& g = ops[o];
+        const uint32_t i = f - s_pre[o];
+        const uint32_t j = r == 0 ? i : pend_of(g.sc, r)[i];
+        uint32_t removed = 0;
+        const bool ran = check_op<KB>(g.t, g.keys, j, g.sc, removed);
+        append_peer(pend_of(g.sc, r + 1), &g.ctl->npend[(r + 1) & 1], j, !ran, o);
+        add_peer(g.ctl, removed, o);
+    }
+}
+
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_grp_rem_p3(const GroupOp* __restrict__ ops, uint32_t nops, uint32_t r) {
+    __shared__ uint32_t s_pre[GROUP_MAX + 1];
+    const uint32_t total = group_prefix(nops, [&](uint32_t o) { return grp_rem_pending(ops, o, r); }, s_pre);
+    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < total; f += gridDim.x * blockDim.x) {
+        const uint32_t o = group_find(s_pre, nops, f);
+        const GroupOp& g = ops[o];
+        const uint32_t i = f - s_pre[o];
+        const uint32_t j = r == 0 ? i : pend_of(g.sc, r)[i];
+        reset_op<KB>(g.t, g.keys, j, g.sc);
+    }
+}
+
+template <int KB>
+__global__ void __launch_bounds__(TAIL_THREADS) k_grp_rem_tail(const GroupOp* __restrict__ ops, uint32_t r0) {
+    const GroupOp& g = ops[blockIdx.x];
+    const uint32_t n0 = *(volatile const uint32_t*)&g.ctl->n0;
+    rem_tail_body<KB>(g.t, g.keys, n0, r0, g.sc, g.ctl, 0xFFFFFFFFu);
+}
+
+constexpr uint32_t GRP_ROUNDS = 3;  // grid rounds before the block-per-op tail
+
+template <int KB>
+void grp_rem_shape(const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream_t s) {
+    const unsigned g = grid_for(sum_n, 8);
+    k_grp_setup<<<nops, 256, 0, s>>>(ops, 0);
+    for (uint32_t r = 0; r < GRP_ROUNDS; r++) {
+        {
+            KtScope kt(KC_REM_MARK, s);
+            k_grp_rem_p1<KB><<<g, RBLOCK, 0, s>>>(ops, nops, r);
+        }
+        {
+            KtScope kt(KC_REM_CHECK, s);
+            k_grp_rem_p2<KB><<<g, RBLOCK, 0, s>>>(ops, nops, r);
+        }
+        {
+            KtScope kt(KC_REM_EXEC, s);
+            k_grp_rem_p3<KB><<<g, RBLOCK, 0, s>>>(ops, nops, r);
+        }
+    }
+    {
+        KtScope kt(KC_REM_TAIL, s);
+        k_grp_rem_tail<KB><<<nops, TAIL_THREADS, 0, s>>>(ops, GRP_ROUNDS);
+    }
+    k_grp_finish<<<(nops + 255) / 256, 256, 0, s>>>(ops, nops, 0);
+    count_launches(2 + 3 * GRP_ROUNDS + 1 + 1);
+}
+
+template <int KB>
 void rounds_shape(const TableView& t, const uint8_t* keys, uint32_t n0, uint32_t r0, uint32_t nrounds,
                   uint32_t grid_ops, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
     const unsigned g = grid_for(grid_ops, 8);
@@ -251,6 +347,19 @@ cudaError_t launch_rem_rounds(const TableView& t, Shape sh, const uint8_t* keys,
         case SHAPE_32_64:
         case SHAPE_32_32: rounds_shape<32>(t, keys, n0, r0, nrounds, grid_ops, sc, ctl, s); break;
         default: rounds_shape<0>(t, keys, n0, r0, nrounds, grid_ops, sc, ctl, s); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grp_rem(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream_t s) {
+    if (nops == 0) return cudaSuccess;
+    switch (sh) {
+        case SHAPE_8_8:
+        case SHAPE_8_32: grp_rem_shape<8>(ops, nops, sum_n, s); break;
+        case SHAPE_32_128:
+        case SHAPE_32_64:
+        case SHAPE_32_32: grp_rem_shape<32>(ops, nops, sum_n, s); break;
+        default: grp_rem_shape<0>(ops, nops, sum_n, s); break;
     }
     return cudaGetLastError();
 }

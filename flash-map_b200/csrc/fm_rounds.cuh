@@ -147,6 +147,106 @@ __device__ __forceinline__ uint32_t block_compact(uint32_t j, bool take, uint32_
     return total;
 }
 
+// ---- grouped launches ------------------------------------------------------
+
+// Exclusive prefix of the ops' item counts into s_pre[0..nops] (block-wide;
+// every thread calls it; count(o) is read once per op).  Returns the total.
+template <class Count>
+__device__ __forceinline__ uint32_t group_prefix(uint32_t nops, Count count, uint32_t* s_pre) {
+    if (threadIdx.x < 32) {
+        uint32_t carry = 0;
+        for (uint32_t b = 0; b < nops; b += 32) {
+            const uint32_t o = b + threadIdx.x;
+            uint32_t v = o < nops ? count(o) : 0u;
+            uint32_t incl = v;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t x = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+                if ((int)threadIdx.x >= d) incl += x;
+            }
+            if (o < nops) s_pre[o] = carry + incl - v;
+            carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
+        }
+        if (threadIdx.x == 0) s_pre[nops] = carry;
+    }
+    __syncthreads();
+    return s_pre[nops];
+}
+
+// The op holding flat item `flat` (largest o with s_pre[o] <= flat).
+__device__ __forceinline__ uint32_t group_find(const uint32_t* s_pre, uint32_t nops, uint32_t flat) {
+    uint32_t lo = 0, hi = nops;  // s_pre[lo] <= flat < s_pre[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_pre[mid] <= flat) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Append of `j` to op o's list, aggregated over the lanes of a warp working
+// on the same op (one atomic per op per warp).
+__device__ __forceinline__ void append_peer(uint32_t* list, uint32_t* counter, uint32_t j, bool take, uint32_t o) {
+    const uint32_t active = __activemask();
+    const uint32_t peers = __match_any_sync(active, o);
+    const uint32_t m = __ballot_sync(peers, take);
+    if (!take) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(m));
+    base = __shfl_sync(m, base, leader);
+    list[base + __popc(m & ((1u << lane) - 1u))] = j;
+}
+
+// Adds v to op o's spread counter, aggregated over the warp's lanes on o.
+__device__ __forceinline__ void add_peer(Ctl* ctl, uint32_t v, uint32_t o) {
+    const uint32_t active = __activemask();
+    const uint32_t peers = __match_any_sync(active, o);
+    const uint32_t sum = __reduce_add_sync(peers, v);
+    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1) && sum)
+        atomicAdd(&ctl->count_part[blockIdx.x % COUNT_PARTS][0], (unsigned long long)sum);
+}
+
+namespace {
+
+// Per op: reset the call's control fields, then the precheck of
+// gpu.rs:198-206 against the table's count at this point of the batch.
+__global__ void k_grp_setup(const GroupOp* __restrict__ ops, int is_insert) {
+    const GroupOp& g = ops[blockIdx.x];
+    uint32_t* w = reinterpret_cast<uint32_t*>(g.ctl);
+    for (uint32_t i = threadIdx.x; i < CTL_CALL_BYTES / 4; i += blockDim.x) w[i] = 0u;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t n0 = g.n;
+        int st = STATUS_OK;
+        if (is_insert && g.counted && *g.len + g.n > g.t.mask + 1) {
+            n0 = 0;
+            st = STATUS_TABLE_FULL;
+        }
+        g.ctl->n0 = n0;
+        *g.status = st;
+        *g.result = 0;
+    }
+}
+
+// Per op: the result, the table's count and the status.
+__global__ void k_grp_finish(const GroupOp* __restrict__ ops, uint32_t nops, int is_insert) {
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nops) return;
+    const GroupOp& g = ops[o];
+    if (*g.status != STATUS_OK) return;  // rejected by the precheck
+    const unsigned long long c = g.ctl->total_count();
+    *g.result = c;
+    if (is_insert) *g.len += g.counted ? c : (unsigned long long)g.n;
+    else *g.len -= c;
+    const uint32_t err = g.ctl->err;
+    if (err & (ERR_SCRATCH | ERR_NO_PROGRESS)) *g.status = STATUS_KERNEL;
+    else if (err & ERR_WALK_LIMIT) *g.status = STATUS_PROBE_LIMIT;
+}
+
+}  // namespace
+
 // Iteration count of a uniform grid-stride loop (every thread of a warp runs
 // the same number of iterations, so warp collectives stay legal).
 __device__ __forceinline__ uint32_t grid_iters(uint32_t n) {

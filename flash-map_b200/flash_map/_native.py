@@ -22,8 +22,24 @@ EXPORTS = (
     "fm_bulk_get_values_device", "fm_bulk_insert_device", "fm_bulk_insert_device_uncounted",
     "fm_bulk_remove_device", "fm_recount", "fm_last_error", "fm_launch_count", "fm_snapshot", "fm_load",
     "fm_bulk_insert_device_noalloc", "fm_kernel_timing", "fm_kernel_times", "fm_kernel_times_reset",
-    "fm_kernel_class_name",
+    "fm_kernel_class_name", "fm_batch_create", "fm_batch_capture", "fm_batch_run", "fm_batch_wait",
+    "fm_batch_waves", "fm_batch_destroy",
 )
+
+
+class FmOp(C.Structure):
+    """struct fm_op of include/flashmap_b200.h."""
+    _fields_ = [
+        ("table", C.c_void_p),
+        ("kind", C.c_uint32),
+        ("n", C.c_uint64),
+        ("d_keys", C.c_void_p),
+        ("d_values", C.c_void_p),
+        ("d_out_values", C.c_void_p),
+        ("d_out_found", C.c_void_p),
+        ("result", C.c_uint64),
+        ("status", C.c_int),
+    ]
 
 _lock = threading.Lock()
 _lib = None
@@ -82,6 +98,18 @@ def _declare(L) -> None:
     L.fm_kernel_times_reset.argtypes = [vp]
     L.fm_kernel_class_name.restype = C.c_char_p
     L.fm_kernel_class_name.argtypes = [u32]
+    L.fm_batch_create.restype = i32
+    L.fm_batch_create.argtypes = [C.POINTER(FmOp), u32, C.POINTER(vp)]
+    L.fm_batch_capture.restype = i32
+    L.fm_batch_capture.argtypes = [vp, vp]
+    L.fm_batch_run.restype = i32
+    L.fm_batch_run.argtypes = [vp, vp]
+    L.fm_batch_wait.restype = i32
+    L.fm_batch_wait.argtypes = [vp, C.POINTER(FmOp)]
+    L.fm_batch_waves.restype = u32
+    L.fm_batch_waves.argtypes = [vp]
+    L.fm_batch_destroy.restype = None
+    L.fm_batch_destroy.argtypes = [vp]
 
 
 def load_library(path: str = LIB_PATH):

@@ -150,6 +150,43 @@ int fm_kernel_times(fm_table* t, double* total_ms, uint64_t* launches, uint32_t 
 int fm_kernel_times_reset(fm_table* t);
 const char* fm_kernel_class_name(uint32_t cls);
 
+/* Batched form (no counterpart in gpu.rs; the batching row of the design).
+ * A queue of bulk operations over any number of tables of one device, with
+ * device-resident keys, values and outputs, executed with the result of
+ * calling fm_bulk_get_device / fm_bulk_insert_device / fm_bulk_remove_device
+ * one by one in queue order (each insert's TableFull precheck sees the
+ * table's count after the ops before it).  The ops are planned into waves of
+ * independent ops (distinct tables; consecutive gets of one table share a
+ * wave); each wave runs grouped kernels that serve all its ops of one kind
+ * and record shape per launch, with no host synchronisation between waves.
+ * fm_batch_capture records the whole batch into a CUDA graph that later
+ * fm_batch_run calls replay.  Between fm_batch_run and fm_batch_wait the
+ * batch's tables must not be used by other calls.  Per-op results (new /
+ * removed key counts) and status codes (FM_OK, FM_ERR_TABLE_FULL,
+ * FM_ERR_PROBE_LIMIT, ...) are written back into the op array by
+ * fm_batch_wait, which also updates each table's len. */
+#define FM_OP_GET 0u
+#define FM_OP_INSERT 1u
+#define FM_OP_REMOVE 2u
+typedef struct fm_op {
+    fm_table* table;
+    uint32_t kind;          /* FM_OP_GET / FM_OP_INSERT / FM_OP_REMOVE */
+    uint64_t n;             /* keys */
+    const void* d_keys;     /* n * K bytes, device */
+    const void* d_values;   /* insert: n * V bytes, device */
+    void* d_out_values;     /* get: n * V bytes, device (NULL: not wanted) */
+    uint8_t* d_out_found;   /* get: n bytes, device (NULL: not wanted) */
+    uint64_t result;        /* out: new keys (insert) / removed keys (remove) */
+    int status;             /* out: FM_OK or the op's error code */
+} fm_op;
+typedef struct fm_batch fm_batch;
+int fm_batch_create(const fm_op* ops, uint32_t nops, fm_batch** out);
+int fm_batch_capture(fm_batch* b, void* stream);
+int fm_batch_run(fm_batch* b, void* stream);
+int fm_batch_wait(fm_batch* b, fm_op* ops);
+uint32_t fm_batch_waves(const fm_batch* b);
+void fm_batch_destroy(fm_batch* b);
+
 /* Raw table access for layout checks and for loading a prefilled table:
  * flags (capacity u32), keys (capacity*K bytes), values (capacity*V bytes),
  * all host pointers; any may be NULL to skip it. */

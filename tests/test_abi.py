@@ -13,7 +13,7 @@ HEADER = os.path.join(ROOT, "include", "flashmap_b200.h")
 
 def declared_symbols():
     src = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|void|uint64_t|double|const char\*)\s+(fm_\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|void|uint32_t|uint64_t|double|const char\*)\s+(fm_\w+)\s*\(", src, re.M)))
 
 
 def test_header_declares_the_gpu_rs_surface():

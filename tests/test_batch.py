@@ -1,0 +1,170 @@
+"""Batched form: a queue of bulk ops over many tables, run as waves of grouped
+kernels (eagerly and replayed from a CUDA graph), must equal the sequential
+oracle replaying the same queue one op at a time in queue order: every get
+output, every insert/remove count and status (TableFull for oversized
+inserts), every table's final len and slot layout."""
+import numpy as np
+import pytest
+
+from fm_testutil import OracleAdapter, gpu_map
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(8, 8), (32, 128), (32, 32), (8, 32)]
+
+
+def _keys(rng, n, ks):
+    return rng.integers(0, 256, (n, ks), dtype=np.uint8)
+
+
+def make_queue(seed, ntables=8, nops=70, cap_bits=(10, 14), sizes=(16, 6000)):
+    import flash_map as F
+
+    rng = np.random.default_rng(seed)
+    tables = []
+    for i in range(ntables):
+        ks, vs = SHAPES[i % len(SHAPES)]
+        cap = 1 << int(rng.integers(cap_bits[0], cap_bits[1] + 1))
+        g = gpu_map(cap, ks, vs)
+        o = OracleAdapter(cap, ks, vs)
+        n = int(cap * rng.uniform(0.5, 0.85))
+        k, v = _keys(rng, n, ks), _keys(rng, n, vs)
+        assert g.bulk_insert(k, v) == o.bulk_insert(k, v)
+        tables.append({"g": g, "o": o, "ks": ks, "vs": vs, "known": [k]})
+    queue = []
+    for i in range(nops):
+        ti = int(rng.integers(ntables))
+        t = tables[ti]
+        kind = int(rng.choice([F.batch.GET, F.batch.INSERT, F.batch.REMOVE], p=[0.4, 0.4, 0.2]))
+        n = int(np.exp(rng.uniform(np.log(sizes[0]), np.log(sizes[1]))))
+        if i == 5:
+            n = 0  # an empty op
+        known = np.concatenate(t["known"])
+        if kind == F.batch.INSERT:
+            k = _keys(rng, n, t["ks"])
+            if n >= 10:
+                d = rng.choice(n, n // 10, replace=False)
+                k[d] = k[rng.integers(0, n, len(d))]  # in-batch duplicates
+                e = rng.choice(n, n // 10, replace=False)
+                k[e] = known[rng.integers(0, len(known), len(e))]  # updates of present keys
+            v = _keys(rng, n, t["vs"])
+            t["known"].append(k)
+        else:
+            npres = int(n * 0.8)
+            k = np.concatenate([known[rng.integers(0, len(known), npres)], _keys(rng, n - npres, t["ks"])])
+            k = k[rng.permutation(n)] if n else k
+            v = None
+        queue.append((ti, kind, k, v))
+    return tables, queue
+
+
+def run_batch(tables, queue, graph):
+    import torch
+
+    import flash_map as F
+
+    ops, outs = [], []
+    for ti, kind, k, v in queue:
+        t = tables[ti]
+        n = len(k)
+        dk = torch.from_numpy(np.ascontiguousarray(k)).cuda() if n else torch.empty((1, t["ks"]), dtype=torch.uint8,
+                                                                                      device="cuda")
+        dv = torch.from_numpy(np.ascontiguousarray(v)).cuda() if v is not None and n else None
+        ov = of = None
+        if kind == F.batch.GET:
+            ov = torch.full((max(n, 1), t["vs"]), 0xAB, dtype=torch.uint8, device="cuda")
+            of = torch.full((max(n, 1),), 0xAB, dtype=torch.uint8, device="cuda")
+        ops.append(F.BatchOp(kind, t["g"], n, dk, dv, ov, of))
+        outs.append((ov, of))
+    b = F.FlashMapBatch(ops)
+    assert b.waves >= 1
+    s = torch.cuda.Stream()
+    if graph:
+        b.capture(s)
+    b.run(s)
+    res = b.wait()
+    b.close()
+    torch.cuda.synchronize()
+    return res, [(None if ov is None else ov.cpu().numpy(), None if of is None else of.cpu().numpy())
+                 for ov, of in outs]
+
+
+def oracle_replay(tables, queue):
+    import oracle as O
+
+    import flash_map as F
+
+    res, outs = [], []
+    for ti, kind, k, v in queue:
+        o = tables[ti]["o"]
+        if len(k) == 0:
+            res.append((0, 0))
+            outs.append(None)
+            continue
+        if kind == F.batch.GET:
+            outs.append(o.bulk_get(k))
+            res.append((0, 0))
+        elif kind == F.batch.INSERT:
+            outs.append(None)
+            try:
+                res.append((o.bulk_insert(k, v), 0))
+            except O.TableFull:
+                res.append((0, 5))
+        else:
+            outs.append(None)
+            res.append((o.bulk_remove(k), 0))
+    return res, outs
+
+
+@pytest.mark.parametrize("graph", [False, True])
+@pytest.mark.parametrize("seed", [1, 2])
+def test_batch_matches_sequential_replay(seed, graph):
+    import flash_map as F
+
+    tables, queue = make_queue(seed)
+    g_res, g_out = run_batch(tables, queue, graph)
+    o_res, o_out = oracle_replay(tables, queue)
+    full = 0
+    for i, ((ti, kind, k, v), gr, orr) in enumerate(zip(queue, g_res, o_res)):
+        assert gr == orr, f"op {i} kind {kind} n {len(k)}: gpu {gr} oracle {orr}"
+        full += orr[1] == 5
+        if kind == F.batch.GET and len(k):
+            ov, of = g_out[i]
+            ev, ef = o_out[i]
+            assert np.array_equal(of.astype(bool), ef), f"op {i}: found differs"
+            assert np.array_equal(ov, ev), f"op {i}: values differ"
+    assert full >= 1  # the mix holds oversized inserts
+    for t in tables:
+        assert t["g"].len() == t["o"].len()
+        gf, gk, gv = t["g"].snapshot()
+        of_, ok, ov = t["o"].snapshot()
+        assert np.array_equal(gf, of_) and np.array_equal(gk, ok) and np.array_equal(gv, ov)
+
+
+def test_batch_single_table_chain_of_dependent_ops():
+    """Every op on one table: one wave per op (gets in a row share a wave),
+    each insert seeing the previous ops' effects."""
+    import flash_map as F
+
+    rng = np.random.default_rng(7)
+    cap = 1 << 12
+    g = gpu_map(cap, 8, 8)
+    o = OracleAdapter(cap, 8, 8)
+    tables = [{"g": g, "o": o, "ks": 8, "vs": 8, "known": []}]
+    queue = []
+    pool = rng.integers(0, 256, (3000, 8), dtype=np.uint8)
+    for i in range(20):
+        kind = [F.batch.INSERT, F.batch.GET, F.batch.GET, F.batch.REMOVE][i % 4]
+        k = pool[rng.integers(0, len(pool), 400)]
+        v = rng.integers(0, 256, (400, 8), dtype=np.uint8) if kind == F.batch.INSERT else None
+        queue.append((0, kind, k, v))
+    g_res, g_out = run_batch(tables, queue, False)
+    o_res, o_out = oracle_replay(tables, queue)
+    assert g_res == o_res
+    for i, (ti, kind, k, v) in enumerate(queue):
+        if kind == F.batch.GET:
+            assert np.array_equal(g_out[i][1].astype(bool), o_out[i][1])
+            assert np.array_equal(g_out[i][0], o_out[i][0])
+    gf, gk, gv = g.snapshot()
+    of_, ok, ov = o.snapshot()
+    assert np.array_equal(gf, of_) and np.array_equal(gk, ok) and np.array_equal(gv, ov)
