@@ -296,6 +296,16 @@ int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t
             if (now == 0) break;
             if (now >= left)  // every round runs at least the lowest pending op
                 return fail(FM_ERR_PROBE_LIMIT, "round made no progress");
+            if (insert && (uint64_t)now * 8 > (uint64_t)left * 7) {
+                // under 1/8 of the ops per pass (ops crowded onto few free
+                // slots, a near-full table): the rest one at a time in index
+                // order, which a round boundary allows
+                e = fm::launch_ins_serial(v, sh, kk, vv, m, r, t->sc, t->d_ctl, s);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "serial insert", e);
+                break;
+            }
             left = now;
         }
         total += t->h_ctl->total_count();
@@ -494,7 +504,8 @@ int fm_bulk_get(fm_table* t, const void* keys, uint64_t n, void* out_values, uin
         uint8_t* df = c->d_buf[sl] + off_f;
         if ((e = cudaMemcpyAsync(dq, hk + base * t->ksz, m * t->ksz, cudaMemcpyHostToDevice, st)) != cudaSuccess)
             rc = cuda_fail(FM_ERR_TRANSFER, "htod keys", e);
-        if (!rc && (e = fm::launch_get(t->view(), t->shape, dq, m, dv, df, st)) != cudaSuccess)
+        if (!rc && (e = fm::launch_get_cfg(t->view(), t->shape, dq, m, dv, df,
+                                           fm::tuned_get_cfg(t->shape, fm_load_factor(t)), st)) != cudaSuccess)
             rc = cuda_fail(FM_ERR_KERNEL_LAUNCH, "bulk_get", e);
         if (!rc && t->vsz &&
             (e = cudaMemcpyAsync(hv + base * t->vsz, dv, m * t->vsz, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
@@ -630,8 +641,9 @@ int fm_bulk_get_device(fm_table* t, const void* d_keys, uint64_t n, void* d_out_
     if (!d_keys || (!d_out_values && t->vsz)) return fail(FM_ERR_INVALID_ARG, "NULL buffer");
     DeviceGuard dg(t->device);
     TimerScope ts(t);
-    cudaError_t e = fm::launch_get(t->view(), t->shape_for({d_keys, d_out_values}), (const uint8_t*)d_keys, n,
-                                   (uint8_t*)d_out_values, d_out_found, (cudaStream_t)stream);
+    const fm::Shape sh = t->shape_for({d_keys, d_out_values});
+    cudaError_t e = fm::launch_get_cfg(t->view(), sh, (const uint8_t*)d_keys, n, (uint8_t*)d_out_values, d_out_found,
+                                       fm::tuned_get_cfg(sh, fm_load_factor(t)), (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "bulk_get_device", e);
     return FM_OK;
 }
@@ -742,6 +754,26 @@ int fm_load(fm_table* t, const uint32_t* flags, const void* keys, const void* va
     if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "load", e);
     t->len.store(len);
+    return FM_OK;
+}
+
+int fm_copy(fm_table* dst, const fm_table* src, void* stream) {
+    if (!dst || !src) return fail(FM_ERR_INVALID_ARG, "table is NULL");
+    if (dst == src) return FM_OK;
+    if (dst->cap != src->cap || dst->ksz != src->ksz || dst->vsz != src->vsz || dst->device != src->device)
+        return fail(FM_ERR_INVALID_ARG, "tables differ in capacity, record sizes or device");
+    std::lock_guard<std::mutex> g(dst->mu);
+    DeviceGuard dg(dst->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemcpyAsync(dst->d_flags, src->d_flags, src->cap * 4, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess && src->ksz)
+        e = cudaMemcpyAsync(dst->d_keys, src->d_keys, src->cap * src->ksz, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess && src->vsz)
+        e = cudaMemcpyAsync(dst->d_vals, src->d_vals, src->cap * src->vsz, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess)  // dmax, tomb_claimed
+        e = cudaMemcpyAsync(&dst->d_ctl->dmax, &src->d_ctl->dmax, 8, cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "copy", e);
+    dst->len.store(src->len.load());
     return FM_OK;
 }
 
@@ -949,9 +981,10 @@ extern "C" int fm_bulk_insert_device_noalloc(fm_table* t, const void* d_keys, co
 // Each wave launches one grouped lookup kernel per record shape and one
 // grouped round pipeline per shape for its inserts and for its removes
 // (precheck against the table's count at that point of the batch, grid
-// rounds, a block-per-op tail that runs to completion, result write-back):
-// no host synchronisation between waves, so the whole batch can be captured
-// in one CUDA graph and replayed.
+// rounds, a block-per-op tail that runs to completion, result write-back).
+// An eager run drives each group's grid rounds from the host, two at a time,
+// and records how many it needed; a capture launches the recorded counts with
+// no host synchronisation, so the whole batch replays from one CUDA graph.
 // ---------------------------------------------------------------------------
 
 static_assert(fm::STATUS_TABLE_FULL == FM_ERR_TABLE_FULL && fm::STATUS_PROBE_LIMIT == FM_ERR_PROBE_LIMIT &&
@@ -972,6 +1005,8 @@ struct fm_batch {
         size_t prefix_off = 0;          // gets: uint64 prefix[n+1]
         uint64_t total = 0;             // gets: queries; mutating: sum of sizes
         fm::GetCfg cfg;
+        uint32_t rounds = 0;            // mutating: grid rounds the last eager run needed (0: none yet)
+        bool serial = false;            // inserts: the eager run finished them one at a time
     };
     std::vector<Group> groups;          // in execution order
     uint32_t waves = 0;
@@ -982,6 +1017,8 @@ struct fm_batch {
     unsigned long long* d_res = nullptr;   // per op
     int* d_status = nullptr;               // per op
     uint8_t* h_io = nullptr;               // pinned: len[tables], res[ops], status[ops]
+    uint32_t* d_pend = nullptr;            // largest pending count (eager runs)
+    uint32_t* h_pend = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     unsigned long long launches_per_run = 0;
@@ -1006,6 +1043,16 @@ bool batch_aligned(const fm_op& o) {
 // can move when a table's scratch grows between runs).
 int batch_fill(fm_batch* b) {
     for (size_t i = 0; i < b->tables.size(); i++) b->h_len()[i] = b->tables[i]->len.load();
+    // Scratch first, sized for each table's largest mutating op: growing it
+    // reallocates, so no descriptor may be filled before the last growth.
+    std::vector<uint64_t> need(b->tables.size(), 0);
+    for (size_t i = 0; i < b->ops.size(); i++)
+        if (b->ops[i].kind != FM_OP_GET) need[b->table_of[i]] = std::max(need[b->table_of[i]], b->ops[i].n);
+    for (size_t i = 0; i < b->tables.size(); i++) {
+        if (!need[i]) continue;
+        int rc = ensure_scratch(b->tables[i], need[i]);
+        if (rc) return rc;
+    }
     for (auto& g : b->groups) {
         if (g.kind == FM_OP_GET) {
             auto* d = reinterpret_cast<fm::GroupGet*>(b->h_desc + g.desc_off);
@@ -1036,8 +1083,6 @@ int batch_fill(fm_batch* b) {
                 const uint32_t oi = g.members[k];
                 const fm_op& o = b->ops[oi];
                 fm_table* t = o.table;
-                int rc = ensure_scratch(t, o.n);
-                if (rc) return rc;
                 d[k].t = t->view();
                 d[k].keys = (const uint8_t*)o.d_keys;
                 d[k].vals = (const uint8_t*)o.d_values;
@@ -1057,24 +1102,58 @@ int batch_fill(fm_batch* b) {
 }
 
 // Enqueues the batch on stream s: descriptor and count upload, the waves,
-// result download.
-int batch_enqueue(fm_batch* b, cudaStream_t s) {
+// result download.  adaptive (eager runs): each insert/remove group runs grid
+// rounds two at a time until at most TAIL_MAX ops are pending (a 4-byte
+// readback per pair) and records how many it needed; otherwise (capture) the
+// recorded count is used (3 when there is none), so the stream carries no
+// host synchronisation.  Either way the block-per-op tail completes every op.
+int batch_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
     cudaError_t e = cudaMemcpyAsync(b->d_desc, b->h_desc, b->desc_bytes, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->d_len, b->h_len(), b->tables.size() * 8, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "batch upload", e);
-    for (const auto& g : b->groups) {
+    for (auto& g : b->groups) {
         const uint32_t n = (uint32_t)g.members.size();
         if (g.kind == FM_OP_GET) {
             e = fm::launch_grp_get(g.shape, reinterpret_cast<const fm::GroupGet*>(b->d_desc + g.desc_off),
                                    reinterpret_cast<const uint64_t*>(b->d_desc + g.prefix_off), n, g.total, g.cfg, s);
-        } else if (g.kind == FM_OP_INSERT) {
-            e = fm::launch_grp_ins(g.shape, reinterpret_cast<const fm::GroupOp*>(b->d_desc + g.desc_off), n, g.total,
-                                   s);
-        } else {
-            e = fm::launch_grp_rem(g.shape, reinterpret_cast<const fm::GroupOp*>(b->d_desc + g.desc_off), n, g.total,
-                                   s);
+            if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch wave", e);
+            continue;
         }
+        const auto* d = reinterpret_cast<const fm::GroupOp*>(b->d_desc + g.desc_off);
+        auto* L = g.kind == FM_OP_INSERT ? &fm::launch_grp_ins : &fm::launch_grp_rem;
+        e = L(g.shape, d, n, g.total, fm::GRP_BEGIN, 0, 0, s);
+        uint32_t r = 0;
+        if (adaptive) {
+            // every round runs the lowest pending op of each group: bounded
+            const uint64_t bound = 2 * g.total + 4;
+            uint64_t prev = g.total;
+            while (e == cudaSuccess) {
+                e = L(g.shape, d, n, g.total, fm::GRP_ROUNDS, r, 2, s);
+                r += 2;
+                if (e == cudaSuccess) e = fm::launch_grp_pending(d, n, r, b->d_pend, s);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_pend, b->d_pend, 4, cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                // done, few enough for the tail, or under 1/8 progress (the
+                // tail then finishes the rest one at a time)
+                if (e != cudaSuccess || *b->h_pend <= fm::TAIL_MAX || r >= bound) break;
+                if (g.kind == FM_OP_INSERT && (uint64_t)*b->h_pend * 8 > (uint64_t)prev * 7) {
+                    // under 1/8 of the ops per pass (ops crowded onto few free
+                    // slots): the rest one at a time in index order
+                    g.serial = true;
+                    break;
+                }
+                prev = *b->h_pend;
+            }
+            g.rounds = r;
+            if (e == cudaSuccess && g.serial) e = L(g.shape, d, n, g.total, fm::GRP_SERIAL, r, 0, s);
+        } else {
+            const uint32_t nr = g.rounds ? g.rounds : 3u;
+            e = L(g.shape, d, n, g.total, fm::GRP_ROUNDS, 0, nr, s);
+            r = nr;
+            if (e == cudaSuccess && g.serial) e = L(g.shape, d, n, g.total, fm::GRP_SERIAL, r, 0, s);
+        }
+        if (e == cudaSuccess) e = L(g.shape, d, n, g.total, fm::GRP_END, r, 0, s);
         if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch wave", e);
     }
     e = cudaMemcpyAsync(b->h_len(), b->d_len, b->tables.size() * 8, cudaMemcpyDeviceToHost, s);
@@ -1165,6 +1244,8 @@ int fm_batch_create(const fm_op* ops, uint32_t nops, fm_batch** out) {
     if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_res, nops * 8);
     if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_status, nops * 4);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_io, b->io_bytes());
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_pend, 4);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_pend, 4);
     if (e == cudaSuccess) e = cudaMemset(b->d_res, 0, nops * 8);
     if (e == cudaSuccess) e = cudaMemset(b->d_status, 0, nops * 4);
     if (e != cudaSuccess) {
@@ -1191,7 +1272,7 @@ int fm_batch_capture(fm_batch* b, void* stream) {
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "begin capture", e);
     const unsigned long long l0 = fm::launch_count();
-    rc = batch_enqueue(b, s);
+    rc = batch_enqueue(b, s, false);
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(s, &g);
     if (rc) {
@@ -1223,7 +1304,7 @@ int fm_batch_run(fm_batch* b, void* stream) {
     } else {
         TimerScope ts(b->tables.size() == 1 ? b->tables[0] : nullptr);
         rc = batch_fill(b);
-        if (!rc) rc = batch_enqueue(b, s);
+        if (!rc) rc = batch_enqueue(b, s, true);
         if (rc) return rc;
     }
     b->last_stream = s;
@@ -1266,7 +1347,151 @@ void fm_batch_destroy(fm_batch* b) {
     cudaFree(b->d_status);
     if (b->h_desc) cudaFreeHost(b->h_desc);
     if (b->h_io) cudaFreeHost(b->h_io);
+    cudaFree(b->d_pend);
+    if (b->h_pend) cudaFreeHost(b->h_pend);
     delete b;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Autotuner for the lookup kernels (no counterpart in the reference).  For
+// each compile-time record shape and load bucket it fills a sample table of
+// 2^20 slots to the bucket's load with seeded keys, times every candidate --
+// lanes per query in {1, 4, 8, 16, 32} x resident blocks per SM in
+// {8, 16, 32, 64} -- on 2^20 queries (half present) with CUDA events, keeps
+// the fastest, and uses it for every later lookup (plain and batched) on a
+// table of that shape whose load falls in the bucket.  Results can be saved
+// to and loaded from a text file (one "shape bucket lanes blocks_per_sm"
+// line each).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct ShapeKV {
+    fm::Shape sh;
+    uint32_t k, v;
+};
+const ShapeKV kTuneShapes[] = {{fm::SHAPE_8_8, 8, 8},
+                               {fm::SHAPE_32_128, 32, 128},
+                               {fm::SHAPE_32_64, 32, 64},
+                               {fm::SHAPE_32_32, 32, 32},
+                               {fm::SHAPE_8_32, 8, 32}};
+const double kBucketLoad[fm::LOAD_BUCKETS] = {0.5, 0.7, 0.88};
+
+int tune_load(const char* path) {
+    FILE* f = fopen(path, "r");
+    if (!f) return 0;
+    int sh, b, lanes, bps, n = 0;
+    while (fscanf(f, "%d %d %d %d", &sh, &b, &lanes, &bps) == 4) {
+        if (sh < 0 || sh > fm::SHAPE_GENERIC || b < 0 || b >= fm::LOAD_BUCKETS) continue;
+        fm::GetCfg c;
+        c.lanes = lanes;
+        c.blocks_per_sm = bps;
+        fm::set_tuned_get_cfg((fm::Shape)sh, b, c);
+        ++n;
+    }
+    fclose(f);
+    return n;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fm_autotune(int device, const char* cache_path) {
+    if (cache_path && tune_load(cache_path) > 0) return FM_OK;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || device < 0 || device >= ndev) return fail(FM_ERR_CUDA_INIT, "no such CUDA device");
+    DeviceGuard dg(device);
+    const uint64_t cap = 1ull << 20, nq = 1ull << 20;
+    const int lanes[] = {1, 4, 8, 16, 32};
+    const int bpss[] = {8, 16, 32, 64};
+    std::string out;
+    cudaStream_t s = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    uint8_t *dk = nullptr, *dv = nullptr, *dq = nullptr, *dout = nullptr, *dfound = nullptr;
+    int rc = FM_OK;
+    if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&a)) != cudaSuccess || (e = cudaEventCreate(&b)) != cudaSuccess)
+        return cuda_fail(FM_ERR_CUDA_INIT, "autotune", e);
+    for (const ShapeKV& sk : kTuneShapes) {
+        const uint64_t nfill = (uint64_t)(cap * kBucketLoad[fm::LOAD_BUCKETS - 1]) + 8;
+        if ((e = cudaMalloc(&dk, nfill * sk.k)) != cudaSuccess || (e = cudaMalloc(&dv, nfill * sk.v)) != cudaSuccess ||
+            (e = cudaMalloc(&dq, nq * sk.k)) != cudaSuccess || (e = cudaMalloc(&dout, nq * sk.v)) != cudaSuccess ||
+            (e = cudaMalloc(&dfound, nq)) != cudaSuccess) {
+            rc = cuda_fail(FM_ERR_GPU_ALLOC, "autotune buffers", e);
+            break;
+        }
+        fm::launch_fill_random(dk, nfill * sk.k, 11, s);
+        fm::launch_fill_random(dv, nfill * sk.v, 12, s);
+        fm_table* t = nullptr;
+        if ((rc = fm_create(cap, sk.k, sk.v, FM_HASH_IDENTITY, device, &t)) != FM_OK) break;
+        uint64_t filled = 0;
+        for (int bk = 0; bk < fm::LOAD_BUCKETS && rc == FM_OK; bk++) {
+            const uint64_t target = (uint64_t)(cap * kBucketLoad[bk]);
+            uint64_t added = 0;
+            rc = fm_bulk_insert_device(t, dk + filled * sk.k, dv + filled * sk.v, target - filled, &added, s);
+            if (rc) break;
+            filled = target;
+            // queries: half present (inserted keys, strided), half fresh
+            fm::launch_fill_random(dq, nq * sk.k, 13 + bk, s);
+            const uint64_t half = nq / 2 < filled ? nq / 2 : filled;
+            cudaMemcpy2DAsync(dq, 2 * sk.k, dk, sk.k * (filled / half), sk.k, half, cudaMemcpyDeviceToDevice, s);
+            float best = 1e30f;
+            fm::GetCfg bestc;
+            for (int l : lanes) {
+                for (int bps : bpss) {
+                    fm::GetCfg c;
+                    c.lanes = l;
+                    c.blocks_per_sm = bps;
+                    float ms = 1e30f;
+                    for (int rep = 0; rep < 3; rep++) {
+                        cudaEventRecord(a, s);
+                        fm::launch_get_cfg(t->view(), t->shape, dq, nq, dout, dfound, c, s);
+                        cudaEventRecord(b, s);
+                        if ((e = cudaEventSynchronize(b)) != cudaSuccess) break;
+                        float x = 0.f;
+                        cudaEventElapsedTime(&x, a, b);
+                        if (rep > 0 && x < ms) ms = x;  // the first run warms up
+                    }
+                    if (e != cudaSuccess) break;
+                    if (ms < best) best = ms, bestc = c;
+                }
+            }
+            if (e != cudaSuccess) {
+                rc = cuda_fail(FM_ERR_KERNEL_LAUNCH, "autotune", e);
+                break;
+            }
+            fm::set_tuned_get_cfg(sk.sh, bk, bestc);
+            out += std::to_string((int)sk.sh) + " " + std::to_string(bk) + " " + std::to_string(bestc.lanes) + " " +
+                   std::to_string(bestc.blocks_per_sm) + "\n";
+        }
+        fm_destroy(t);
+        cudaFree(dk), cudaFree(dv), cudaFree(dq), cudaFree(dout), cudaFree(dfound);
+        dk = dv = dq = dout = dfound = nullptr;
+        if (rc) break;
+    }
+    cudaFree(dk), cudaFree(dv), cudaFree(dq), cudaFree(dout), cudaFree(dfound);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaStreamDestroy(s);
+    if (rc) return rc;
+    if (cache_path) {
+        FILE* f = fopen(cache_path, "w");
+        if (f) {
+            fputs(out.c_str(), f);
+            fclose(f);
+        }
+    }
+    return FM_OK;
+}
+
+int fm_tuned_get_config(uint32_t key_size, uint32_t value_size, double load, int* lanes, int* blocks_per_sm) {
+    const fm::GetCfg c = fm::tuned_get_cfg(fm::pick_shape(key_size, value_size), load);
+    if (lanes) *lanes = c.lanes;
+    if (blocks_per_sm) *blocks_per_sm = c.blocks_per_sm;
+    return FM_OK;
 }
 
 }  // extern "C"

@@ -222,6 +222,17 @@ __global__ void __launch_bounds__(BLOCK) k_grp_get(const GroupGet* __restrict__ 
     }
 }
 
+// Seeded pseudo-random bytes (splitmix64 of the word index), for the
+// autotuner's sample tables and queries.
+__global__ void k_fill_random(uint64_t* __restrict__ out, uint64_t words, uint64_t seed) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        out[i] = z ^ (z >> 31);
+    }
+}
+
 // Tuned lookup configurations, per shape and load bucket (0: not measured).
 GetCfg g_tuned[SHAPE_GENERIC + 1][LOAD_BUCKETS];
 
@@ -350,6 +361,11 @@ cudaError_t launch_grp_get(Shape sh, const GroupGet* ops, const uint64_t* prefix
 #define FM_CALL(K, V) grp_get_shape<K, V>(ops, prefix, nops, total, cfg, s)
     FM_GET_SWITCH(sh, FM_CALL)
 #undef FM_CALL
+}
+
+cudaError_t launch_fill_random(void* out, uint64_t bytes, uint64_t seed, cudaStream_t s) {
+    k_fill_random<<<grid_for(bytes / 8, 8), BLOCK, 0, s>>>((uint64_t*)out, bytes / 8, seed);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_count(const TableView& t, Ctl* ctl, cudaStream_t s) {

@@ -538,37 +538,6 @@ __device__ __forceinline__ void publish_rare(Ctl* ctl, uint32_t maxd, bool tomb,
     }
 }
 
-// Applies the ops of `list` (n ops; nullptr = the identity over n ops) one at a
-// time in index order on thread 0 of one block -- the sequential semantics,
-// for rounds that found the table full.  Their registrations must already be
-// clear.  Block-uniform call; s_buf holds blockDim.x words, s_woff 33.
-template <int KB, int VB>
-__device__ void serial_process(const TableView& t, const uint8_t* keys, const uint8_t* vals, const uint32_t* list,
-                               uint32_t n, uint32_t n0, const OpScratch& sc, ExecAcc& a, uint32_t* s_buf,
-                               uint32_t* s_woff) {
-    const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
-    const uint32_t vsz = VB ? (uint32_t)VB : t.vsz;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sc.op_flag[list ? list[i] : i] = 3;
-    __syncthreads();
-    for (uint32_t base = 0; base < n0; base += blockDim.x) {
-        const uint32_t j = base + threadIdx.x;
-        const bool take = j < n0 && sc.op_flag[j] == 3;
-        const uint32_t c = block_compact(j, take, s_buf, s_woff);
-        if (threadIdx.x == 0) {
-            for (uint32_t k = 0; k < c; k++) {
-                const uint32_t jj = s_buf[k];
-                sc.op_flag[jj] = 0;
-                if constexpr (KB == 0 || VB == 0)
-                    a.claimed += exec_insert_generic(t, keys + (uint64_t)jj * ksz, vals + (uint64_t)jj * vsz, a);
-                else
-                    a.claimed += exec_insert<KB, VB>(t, keys + (uint64_t)jj * ksz, vals + (uint64_t)jj * vsz, a);
-            }
-        }
-        __syncthreads();
-    }
-}
-
-
 // ---- tile-cooperative execute (compile-time shapes) -----------------------
 //
 // A tile of T lanes runs one insert whose walk is too long for one thread.
@@ -600,14 +569,21 @@ constexpr int TMAXCH = 256;  // eviction slots held per tile
 constexpr int TMAXC = 128;   // possible updates of one window (>= 4T)
 constexpr uint32_t NOSRC = 0xFFFFFFFFu;
 
-struct TileChain {
-    uint32_t pos[TMAXCH];   // eviction slots of the current chunk
-    uint32_t p[TMAXCH];     // depth stored at each of them
+template <int MAXCH_>
+struct ChainBuf {
+    static constexpr int MAXCH = MAXCH_;
+    uint32_t pos[MAXCH];    // eviction slots of the current chunk
+    uint32_t p[MAXCH];      // depth stored at each of them
     uint32_t cpos[TMAXC];   // possible updates of the current window: slot,
     uint32_t cstage[TMAXC]; //   evictions before it,
     uint32_t csrc[TMAXC];   //   slot holding the carried key (NOSRC: the new key)
     uint32_t src_base;      // slot evicted just before the chunk's first stage
 };
+using TileChain = ChainBuf<TMAXCH>;
+// The one-op-at-a-time path's buffer (dynamic shared memory, 67 KB): chains
+// of up to SMAXCH - 128 evictions need no second walk.
+constexpr int SMAXCH = 8192;
+using SerialChain = ChainBuf<SMAXCH>;
 
 template <int T>
 __device__ __forceinline__ uint64_t find_free_tile(const TableView& t, uint64_t h, const Tile<T>& tl) {
@@ -671,10 +647,11 @@ __device__ __forceinline__ long long tile_max(long long v, const Tile<T>& tl) {
 // dest(m) = P_m (m < k) or the end slot (m == k) from source(m) = P_(m-1), the
 // slot `src_base` for m == chunk_base > 0, or the new entry for m == 0.  MB
 // moves per round trip, every lane holding up to CPL chunks.
-template <int KB, int VB, int T, int CPL>
+template <int KB, int VB, int CPL, class Crew, class C>
 __device__ __forceinline__ void tile_moves(const TableView& t, const RegKey<KB>& key, const uint8_t* vin,
-                                           const TileChain& s, uint32_t chunk_base, int hi, int lo, uint32_t k,
-                                           int kind, uint64_t end_slot, uint32_t src_base, const Tile<T>& tl) {
+                                           const C& s, uint32_t chunk_base, int hi, int lo, uint32_t k,
+                                           int kind, uint64_t end_slot, uint32_t src_base, const Crew& tl) {
+    constexpr int T = Crew::W;
     using CO = ChunkOf<KB, VB>;
     using Ch = typename CO::type;
     constexpr int CK = CO::CK, NK = CO::NK, NC = CO::NC;
@@ -729,11 +706,12 @@ __device__ __forceinline__ void tile_moves(const TableView& t, const RegKey<KB>&
 //         (stages from chunk_base) in s.pos; returns 1 claim, 2 update,
 //         3 drop, 5 (never in a non-serial round) walk past the bound.
 //   otherwise: records the eviction slots of stages [lo, hi) and stops.
-template <int KB, int T>
-__device__ int tile_walk(const TableView& t, const RegKey<KB>& key, TileChain& s, const Tile<T>& tl, bool find,
+template <int KB, int T, class C>
+__device__ int tile_walk(const TableView& t, const RegKey<KB>& key, C& s, const Tile<T>& tl, bool find,
                          uint32_t lo, uint32_t hi, uint32_t& k, uint32_t& chunk_base, uint32_t& src_base,
                          uint64_t& end_slot, uint64_t& end_p, bool& end_tomb) {
-    static_assert(TMAXC >= 4 * T && TMAXCH >= 8 * T, "a window's updates and evictions must fit the buffers");
+    constexpr int MAXCH = C::MAXCH;
+    static_assert(TMAXC >= 4 * T && MAXCH >= 8 * T, "a window's updates and evictions must fit the buffers");
     const uint64_t mask = t.mask;
     const uint64_t h = key.hash(KB, t.hash_mode) & mask;
     long long M = (long long)h;  // the carried entry's home (unwrapped positions)
@@ -752,7 +730,7 @@ __device__ int tile_walk(const TableView& t, const RegKey<KB>& key, TileChain& s
             kind = 5;
             break;
         }
-        if (find && g - chunk_base > (uint32_t)(TMAXCH - 4 * T)) {  // room for this window's evictions
+        if (find && g - chunk_base > (uint32_t)(MAXCH - 4 * T)) {  // room for this window's evictions
             src_base = last_ev;
             chunk_base = g;
         }
@@ -817,7 +795,7 @@ __device__ int tile_walk(const TableView& t, const RegKey<KB>& key, TileChain& s
         for (int i = 0; i < 4; i++) {
             const uint64_t pos = base + i;
             if ((evb >> i) & 1u) {
-                if (stg >= chunk_base && stg < (find ? chunk_base + TMAXCH : hi)) {
+                if (stg >= chunk_base && stg < (find ? chunk_base + MAXCH : hi)) {
                     s.pos[stg - chunk_base] = (uint32_t)(pos & mask);
                     s.p[stg - chunk_base] = pend[i];
                 }
@@ -900,41 +878,39 @@ __device__ int tile_walk(const TableView& t, const RegKey<KB>& key, TileChain& s
 }
 
 // One insert by a tile (capacity >= 4T, rounds that are not serial).
-template <int KB, int VB, int T>
-__device__ __forceinline__ void exec_tile(const TableView& t, const RegKey<KB>& key,
-                                          const uint8_t* __restrict__ vals_in, uint32_t j, const Tile<T>& tl,
-                                          TileChain& s, ExecAcc& a) {
+template <int KB, int VB, int T, class C = TileChain>
+__device__ __forceinline__ int exec_tile(const TableView& t, const RegKey<KB>& key,
+                                         const uint8_t* __restrict__ vals_in, uint32_t j, const Tile<T>& tl,
+                                         C& s, ExecAcc& a) {
     constexpr int CPL = 4;
+    constexpr int MAXCH = C::MAXCH;
     const uint8_t* vin = vals_in + (uint64_t)j * VB;
     uint32_t k = 0, chunk_base = 0, src_base = NOSRC;
     uint64_t end_slot = 0, end_p = 0;
     bool end_tomb = false;
     const int kind =
-        tile_walk<KB, T>(t, key, s, tl, true, 0, 0, k, chunk_base, src_base, end_slot, end_p, end_tomb);
-    if (kind == 5) {
-        a.limit = true;
-        return;
-    }
+        tile_walk<KB, T, C>(t, key, s, tl, true, 0, 0, k, chunk_base, src_base, end_slot, end_p, end_tomb);
+    if (kind == 5) return 5;  // no free slot within a pass: nothing written
     uint32_t md = 0;
     // last chunk: moves from the end (or the last eviction) down to chunk_base
     {
         const int hi = (kind == 3) ? (int)k - 1 : (int)k;
-        tile_moves<KB, VB, T, CPL>(t, key, vin, s, chunk_base, hi, (int)chunk_base, k, kind, end_slot, src_base, tl);
+        tile_moves<KB, VB, CPL>(t, key, vin, s, chunk_base, hi, (int)chunk_base, k, kind, end_slot, src_base, tl);
         for (uint32_t m = chunk_base + tl.lane; m < k; m += T) {
             t.flags[s.pos[m - chunk_base]] = mk_flag(ST_OCC, s.p[m - chunk_base]);
             md = max(md, min(s.p[m - chunk_base], DIST_MASK));
         }
         tl.sync();
     }
-    // earlier stages, TMAXCH at a time from the top, each found again by a
+    // earlier stages, MAXCH at a time from the top, each found again by a
     // walk from home
     for (uint32_t top = chunk_base; top > 0;) {
-        const uint32_t lo = top > (uint32_t)TMAXCH ? top - TMAXCH : 0u;
+        const uint32_t lo = top > (uint32_t)MAXCH ? top - MAXCH : 0u;
         uint32_t k2, cb2, sb2;
         uint64_t es2, ep2;
         bool et2;
-        tile_walk<KB, T>(t, key, s, tl, false, lo, top, k2, cb2, sb2, es2, ep2, et2);
-        tile_moves<KB, VB, T, CPL>(t, key, vin, s, lo, (int)top - 1, (int)lo, k, kind, end_slot, sb2, tl);
+        tile_walk<KB, T, C>(t, key, s, tl, false, lo, top, k2, cb2, sb2, es2, ep2, et2);
+        tile_moves<KB, VB, CPL>(t, key, vin, s, lo, (int)top - 1, (int)lo, k, kind, end_slot, sb2, tl);
         for (uint32_t m = tl.lane; m < top - lo; m += T) {
             t.flags[s.pos[m]] = mk_flag(ST_OCC, s.p[m]);
             md = max(md, min(s.p[m], DIST_MASK));
@@ -949,6 +925,134 @@ __device__ __forceinline__ void exec_tile(const TableView& t, const RegKey<KB>& 
         a.tomb = a.tomb || end_tomb;
     }
     a.maxd = max(a.maxd, md);
+    return kind;
+}
+
+// The walk's outcome, broadcast from warp 0 to the block.
+struct SerialOut {
+    int kind;
+    uint32_t k, chunk_base, src_base;
+    uint64_t end_slot, end_p;
+    int tomb;
+};
+
+constexpr int SERIAL_THREADS = 512;
+
+// One insert by a whole block of SERIAL_THREADS threads (compile-time sizes,
+// capacity >= 128): warp 0 walks the chain into the large buffer, then every
+// thread moves records (204 account-shape records per round trip) and writes
+// flags.  A chain longer than the buffer takes the chunked warp path; a walk
+// that finds no free slot within a pass (overfull table) the scalar walk.
+// Block-uniform call.
+template <int KB, int VB>
+__device__ void exec_serial_block(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t j,
+                                  SerialChain& s, SerialOut& so, ExecAcc& a) {
+    RegKey<KB> key;
+    key.load(keys + (uint64_t)j * KB, KB);
+    const uint8_t* vin = vals + (uint64_t)j * VB;
+    if (threadIdx.x < 32) {
+        const Tile<32> tl;
+        uint32_t k = 0, cb = 0, sb = NOSRC;
+        uint64_t es = 0, ep = 0;
+        bool et = false;
+        const int kind = tile_walk<KB, 32, SerialChain>(t, key, s, tl, true, 0, 0, k, cb, sb, es, ep, et);
+        if (tl.lane == 0) {
+            so.kind = kind;
+            so.k = k;
+            so.chunk_base = cb;
+            so.src_base = sb;
+            so.end_slot = es;
+            so.end_p = ep;
+            so.tomb = et ? 1 : 0;
+        }
+    }
+    __syncthreads();
+    const int kind = so.kind;
+    if (kind == 5 || so.chunk_base != 0) {
+        if (threadIdx.x < 32) {
+            const Tile<32> tl;
+            int kk = 5;
+            if (kind != 5) kk = exec_tile<KB, VB, 32, SerialChain>(t, key, vals, j, tl, s, a);
+            if (kk == 5 && tl.lane == 0) a.claimed += exec_insert_key<KB, VB>(t, key, vin, a);
+        }
+        __syncthreads();
+        return;
+    }
+    const uint32_t k = so.k;
+    const int hi = kind == 3 ? (int)k - 1 : (int)k;
+    const BlockCrew<SERIAL_THREADS> crew;
+    tile_moves<KB, VB, 4>(t, key, vin, s, 0, hi, 0, k, kind, so.end_slot, so.src_base, crew);
+    uint32_t md = 0;
+    for (uint32_t m = threadIdx.x; m < k; m += blockDim.x) {
+        t.flags[s.pos[m]] = mk_flag(ST_OCC, s.p[m]);
+        md = max(md, min(s.p[m], DIST_MASK));
+    }
+    if (threadIdx.x == 0 && kind == 1) {
+        t.flags[so.end_slot] = mk_flag(ST_OCC, so.end_p);
+        md = max(md, (uint32_t)min(so.end_p, (uint64_t)DIST_MASK));
+        a.claimed += 1;
+        a.tomb = a.tomb || so.tomb != 0;
+    }
+    a.maxd = max(a.maxd, md);
+    __syncthreads();  // the next op reads these writes
+}
+
+// Applies the ops of `list` (n ops; nullptr = the identity over n ops) one at
+// a time in index order -- the sequential semantics, for rounds that found an
+// op with no free slot or a flow wrapping the table.  With compile-time
+// record sizes each op runs on warp 0 as a tile walk (128 slots per round
+// trip); an op whose walk finds no free slot within a pass over the table
+// (a table overfilled by uncounted inserts) writes nothing there and reruns
+// as the scalar walk, which applies the step limit.  Run-time sizes use the
+// scalar walk on thread 0.  Registrations must already be clear.
+// Block-uniform call; s_buf holds blockDim.x words, s_woff 33, s_chain one
+// tile chain buffer (compile-time sizes; may be null for the scalar walk).
+// With s_big (a block of SERIAL_THREADS threads) each op runs on the whole
+// block instead (exec_serial_block).
+template <int KB, int VB>
+__device__ void serial_process(const TableView& t, const uint8_t* keys, const uint8_t* vals, const uint32_t* list,
+                               uint32_t n, uint32_t n0, const OpScratch& sc, ExecAcc& a, uint32_t* s_buf,
+                               uint32_t* s_woff, TileChain* s_chain, SerialChain* s_big = nullptr,
+                               SerialOut* s_out = nullptr) {
+    const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
+    const uint32_t vsz = VB ? (uint32_t)VB : t.vsz;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sc.op_flag[list ? list[i] : i] = 3;
+    __syncthreads();
+    for (uint32_t base = 0; base < n0; base += blockDim.x) {
+        const uint32_t j = base + threadIdx.x;
+        const bool take = j < n0 && sc.op_flag[j] == 3;
+        const uint32_t c = block_compact(j, take, s_buf, s_woff);
+        if constexpr (KB == 0 || VB == 0) {
+            if (threadIdx.x == 0) {
+                for (uint32_t k = 0; k < c; k++) {
+                    const uint32_t jj = s_buf[k];
+                    sc.op_flag[jj] = 0;
+                    a.claimed += exec_insert_generic(t, keys + (uint64_t)jj * ksz, vals + (uint64_t)jj * vsz, a);
+                }
+            }
+        } else if (s_big && t.mask >= 4 * 32 - 1) {
+            for (uint32_t k = 0; k < c; k++) {
+                const uint32_t jj = s_buf[k];
+                if (threadIdx.x == 0) sc.op_flag[jj] = 0;
+                exec_serial_block<KB, VB>(t, keys, vals, jj, *s_big, *s_out, a);
+            }
+        } else {
+            if (threadIdx.x < 32) {
+                const Tile<32> tl;
+                for (uint32_t k = 0; k < c; k++) {
+                    const uint32_t jj = s_buf[k];
+                    if (tl.lane == 0) sc.op_flag[jj] = 0;
+                    RegKey<KB> key;
+                    key.load(keys + (uint64_t)jj * KB, KB);
+                    int kind = 5;
+                    if (s_chain && t.mask >= 4 * 32 - 1) kind = exec_tile<KB, VB, 32>(t, key, vals, jj, tl, *s_chain, a);
+                    if (kind == 5 && tl.lane == 0) a.claimed += exec_insert_key<KB, VB>(t, key, vals + (uint64_t)jj * VB, a);
+                    tl.sync();  // the next op reads this one's writes
+                }
+            }
+        }
+        __syncthreads();
+    }
 }
 
 
@@ -1030,7 +1134,7 @@ __device__ __forceinline__ bool finish_tile(const TableView& t, const uint8_t* k
     const bool run = !serial && lead != 0 && blk > j;
     if (run) {
         if (t.mask >= 4 * T - 1) {
-            exec_tile<KB, VB, T>(t, key, vals, j, tl, s, a);
+            if (exec_tile<KB, VB, T>(t, key, vals, j, tl, s, a) == 5) a.limit = true;
         } else {
             if (tl.lane == 0) a.claimed += exec_insert_key<KB, VB>(t, key, vals + (uint64_t)j * VB, a);
         }
@@ -1073,7 +1177,7 @@ __global__ void __launch_bounds__(RBLOCK, 3) k_ins_p4(TableView t, const uint8_t
             RegKey<KB> key;
             key.load(keys + (uint64_t)j * KB, KB);
             if (t.mask >= 4 * P4_T - 1) {
-                exec_tile<KB, VB, P4_T>(t, key, vals, j, tl, s_chain[ti], a);
+                if (exec_tile<KB, VB, P4_T>(t, key, vals, j, tl, s_chain[ti], a) == 5) a.limit = true;
             } else {
                 if (tl.lane == 0) a.claimed += exec_insert_key<KB, VB>(t, key, vals + (uint64_t)j * VB, a);
             }
@@ -1161,7 +1265,7 @@ __device__ __forceinline__ void ins_tail_body(const TableView& t, const uint8_t*
                 sc.op_word[j] = IDLE;
             }
             __syncthreads();
-            serial_process<KB, VB>(t, keys, vals, in, n, n0, sc, a, s_buf, s_woff);
+            serial_process<KB, VB>(t, keys, vals, in, n, n0, sc, a, s_buf, s_woff, T > 1 ? &s_chain[0] : nullptr);
             ++rounds;
             break;
         }
@@ -1183,6 +1287,15 @@ __device__ __forceinline__ void ins_tail_body(const TableView& t, const uint8_t*
         if (nn == 0) break;
         if (nn >= n) {  // every non-serial round runs its smallest op
             if (threadIdx.x == 0) atomicOr(&s_err, ERR_NO_PROGRESS);
+            break;
+        }
+        if (rounds >= 4 && (uint64_t)nn * 8 > (uint64_t)n * 7) {
+            // under 1/8 of the ops per round (ops crowded onto few free slots,
+            // a near-full table): the rest in index order, one at a time
+            __syncthreads();
+            serial_process<KB, VB>(t, keys, vals, pend_of(sc, r), nn, n0, sc, a, s_buf, s_woff,
+                                   T > 1 ? &s_chain[0] : nullptr);
+            ++rounds;
             break;
         }
         n = nn;
@@ -1215,24 +1328,38 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_ins_tail(TableView t, const ui
 // Host-launched fallback for a serial round whose pending count is above
 // TAIL_MAX: applies round r's ops in index order.
 template <int KB, int VB>
-__global__ void __launch_bounds__(1024) k_ins_serial(TableView t, const uint8_t* __restrict__ keys,
-                                                     const uint8_t* __restrict__ vals, uint32_t n0, uint32_t r,
-                                                     OpScratch sc, Ctl* ctl) {
-    __shared__ uint32_t s_buf[1024];
+__global__ void __launch_bounds__(SERIAL_THREADS) k_ins_serial(TableView t, const uint8_t* __restrict__ keys,
+                                                               const uint8_t* __restrict__ vals, uint32_t n0,
+                                                               uint32_t r, OpScratch sc, Ctl* ctl) {
+    __shared__ uint32_t s_buf[SERIAL_THREADS];
     __shared__ uint32_t s_woff[33];
+    __shared__ TileChain s_chain;
+    __shared__ SerialOut s_out;
+    extern __shared__ __align__(16) unsigned char s_dyn[];  // SerialChain (compile-time sizes)
     const RoundOps ops = round_ops(sc, ctl, r, n0);
     ExecAcc a;
-    serial_process<KB, VB>(t, keys, vals, ops.list, ops.n, n0, sc, a, s_buf, s_woff);
+    serial_process<KB, VB>(t, keys, vals, ops.list, ops.n, n0, sc, a, s_buf, s_woff, &s_chain,
+                           (KB && VB) ? reinterpret_cast<SerialChain*>(s_dyn) : nullptr, &s_out);
+    __syncthreads();
+    if (a.claimed) atomicAdd(&ctl->count, (unsigned long long)a.claimed);
+    if (a.maxd > *(volatile uint32_t*)&ctl->dmax) atomicMax(&ctl->dmax, a.maxd);
+    if (a.tomb) ctl->tomb_claimed = 1u;
+    if (a.limit) atomicOr(&ctl->err, ERR_WALK_LIMIT);
     __syncthreads();
     if (threadIdx.x == 0) {
-        if (a.claimed) atomicAdd(&ctl->count, (unsigned long long)a.claimed);
-        if (a.maxd > ctl->dmax) ctl->dmax = a.maxd;
-        if (a.tomb) ctl->tomb_claimed = 1u;
-        if (a.limit) atomicOr(&ctl->err, ERR_WALK_LIMIT);
         ctl->npend[r & 1] = 0;
         ctl->npend[(r + 1) & 1] = 0;
         atomicAdd(&ctl->rounds, 1u);
     }
+}
+
+// Dynamic shared memory of a serial kernel (its attribute is set before each
+// launch: a host-side call).
+template <class K>
+size_t serial_smem(K kernel, bool big) {
+    if (!big) return 0;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SerialChain));
+    return sizeof(SerialChain);
 }
 
 constexpr int INS_T = 32;  // lanes per insert in the single-block tail
@@ -1329,7 +1456,7 @@ __global__ void __launch_bounds__(RBLOCK, 3) k_grp_ins_p4(const GroupOp* __restr
         key.load(g.keys + (uint64_t)j * KB, KB);
         ExecAcc a;
         if (g.t.mask >= 4 * 32 - 1) {
-            exec_tile<KB, VB, 32>(g.t, key, g.vals, j, tl, s_chain[w], a);
+            if (exec_tile<KB, VB, 32>(g.t, key, g.vals, j, tl, s_chain[w], a) == 5) a.limit = true;
         } else {
             if (tl.lane == 0) a.claimed += exec_insert_key<KB, VB>(g.t, key, g.vals + (uint64_t)j * VB, a);
         }
@@ -1352,13 +1479,64 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_grp_ins_tail(const GroupOp* __
     ins_tail_body<KB, VB, T>(g.t, g.keys, g.vals, n0, r0, g.n, g.sc, g.ctl, 0xFFFFFFFFu);
 }
 
-constexpr uint32_t GRP_ROUNDS = 3;  // grid rounds before the block-per-op tail
-
+// Serial completion of a grouped call, one block per op: the op's pending
+// ops of round r one at a time in index order (ops with none return).
 template <int KB, int VB>
-void grp_ins_shape(const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream_t s) {
+__global__ void __launch_bounds__(SERIAL_THREADS) k_grp_ins_serial(const GroupOp* __restrict__ ops, uint32_t r) {
+    __shared__ uint32_t s_buf[SERIAL_THREADS];
+    __shared__ uint32_t s_woff[33];
+    __shared__ TileChain s_chain;
+    __shared__ SerialOut s_out;
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    const GroupOp& g = ops[blockIdx.x];
+    const uint32_t n0 = *(volatile const uint32_t*)&g.ctl->n0;
+    const uint32_t n = grp_pending(ops, blockIdx.x, r);
+    if (n == 0) return;  // block-uniform
+    ExecAcc a;
+    serial_process<KB, VB>(g.t, g.keys, g.vals, r == 0 ? nullptr : pend_of(g.sc, r), n, n0, g.sc, a, s_buf, s_woff,
+                           &s_chain, (KB && VB) ? reinterpret_cast<SerialChain*>(s_dyn) : nullptr, &s_out);
+    __syncthreads();
+    Ctl* ctl = g.ctl;
+    if (a.claimed) atomicAdd(&ctl->count, (unsigned long long)a.claimed);
+    if (a.maxd > *(volatile uint32_t*)&ctl->dmax) atomicMax(&ctl->dmax, a.maxd);
+    if (a.tomb) ctl->tomb_claimed = 1u;
+    if (a.limit) atomicOr(&ctl->err, ERR_WALK_LIMIT);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ctl->npend[r & 1] = 0;
+        ctl->npend[(r + 1) & 1] = 0;
+    }
+}
+
+// Phases of a grouped insert call: GRP_BEGIN (control reset and precheck),
+// GRP_ROUNDS grid rounds r0 .. r0+nrounds-1, GRP_END (block-per-op tail to
+// completion from round r0, then the result write-back).
+template <int KB, int VB>
+void grp_ins_shape(const GroupOp* ops, uint32_t nops, uint64_t sum_n, int phase, uint32_t r0, uint32_t nrounds,
+                   cudaStream_t s) {
     const unsigned g = grid_for(sum_n, 8);
-    k_grp_setup<<<nops, 256, 0, s>>>(ops, 1);
-    for (uint32_t r = 0; r < GRP_ROUNDS; r++) {
+    if (phase == GRP_BEGIN) {
+        k_grp_setup<<<nops, 256, 0, s>>>(ops, 1);
+        count_launches(1);
+        return;
+    }
+    if (phase == GRP_SERIAL) {
+        KtScope kt(KC_INS_SERIAL, s);
+        const size_t smem = serial_smem(k_grp_ins_serial<KB, VB>, KB && VB);
+        k_grp_ins_serial<KB, VB><<<nops, SERIAL_THREADS, smem, s>>>(ops, r0);
+        count_launches(1);
+        return;
+    }
+    if (phase == GRP_END) {
+        {
+            KtScope kt(KC_INS_TAIL, s);
+            k_grp_ins_tail<KB, VB, (KB && VB) ? INS_T : 1><<<nops, TAIL_THREADS, 0, s>>>(ops, r0);
+        }
+        k_grp_finish<<<(nops + 255) / 256, 256, 0, s>>>(ops, nops, 1);
+        count_launches(2);
+        return;
+    }
+    for (uint32_t r = r0; r < r0 + nrounds; r++) {
         {
             KtScope kt(KC_INS_FIND, s);
             k_grp_ins_p1<KB><<<g, RBLOCK, 0, s>>>(ops, nops, r);
@@ -1376,12 +1554,14 @@ void grp_ins_shape(const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream
             k_grp_ins_p4<KB, VB><<<g, RBLOCK, 0, s>>>(ops, nops, r);
         }
     }
-    {
-        KtScope kt(KC_INS_TAIL, s);
-        k_grp_ins_tail<KB, VB, (KB && VB) ? INS_T : 1><<<nops, TAIL_THREADS, 0, s>>>(ops, GRP_ROUNDS);
-    }
-    k_grp_finish<<<(nops + 255) / 256, 256, 0, s>>>(ops, nops, 1);
-    count_launches(2 + GRP_ROUNDS * ((KB != 0 && VB != 0) ? 4 : 3) + 1 + 1);
+    count_launches(nrounds * ((KB != 0 && VB != 0) ? 4 : 3));
+}
+
+// Largest pending count of round r over the ops (one thread).
+__global__ void k_grp_pending(const GroupOp* __restrict__ ops, uint32_t nops, uint32_t r, uint32_t* out) {
+    uint32_t m = 0;
+    for (uint32_t o = 0; o < nops; o++) m = max(m, grp_pending(ops, o, r));
+    *out = m;
 }
 
 template <int KB, int VB>
@@ -1424,7 +1604,8 @@ template <int KB, int VB>
 void serial_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, uint32_t r,
                   const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
     KtScope kt(KC_INS_SERIAL, s);
-    k_ins_serial<KB, VB><<<1, 1024, 0, s>>>(t, keys, vals, n0, r, sc, ctl);
+    const size_t smem = serial_smem(k_ins_serial<KB, VB>, KB && VB);
+    k_ins_serial<KB, VB><<<1, SERIAL_THREADS, smem, s>>>(t, keys, vals, n0, r, sc, ctl);
     count_launches(1);
 }
 
@@ -1457,11 +1638,18 @@ cudaError_t launch_ins_tail(const TableView& t, Shape sh, const uint8_t* keys, c
     return cudaGetLastError();
 }
 
-cudaError_t launch_grp_ins(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream_t s) {
+cudaError_t launch_grp_ins(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, int phase, uint32_t r0,
+                           uint32_t nrounds, cudaStream_t s) {
     if (nops == 0) return cudaSuccess;
-#define FM_CALL(K, V) grp_ins_shape<K, V>(ops, nops, sum_n, s)
+#define FM_CALL(K, V) grp_ins_shape<K, V>(ops, nops, sum_n, phase, r0, nrounds, s)
     FM_SHAPE_SWITCH(sh, FM_CALL)
 #undef FM_CALL
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grp_pending(const GroupOp* ops, uint32_t nops, uint32_t r, uint32_t* out, cudaStream_t s) {
+    k_grp_pending<<<1, 1, 0, s>>>(ops, nops, r, out);
+    count_launches(1);
     return cudaGetLastError();
 }
 

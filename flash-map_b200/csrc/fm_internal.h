@@ -143,14 +143,28 @@ void set_tuned_get_cfg(Shape sh, int load_bucket, GetCfg cfg);
 constexpr int LOAD_BUCKETS = 3;  // load < 0.6, < 0.8, >= 0.8
 inline int load_bucket(double load) { return load < 0.6 ? 0 : (load < 0.8 ? 1 : 2); }
 
+// Fills `bytes` (a multiple of 8) with seeded pseudo-random words.
+cudaError_t launch_fill_random(void* out, uint64_t bytes, uint64_t seed, cudaStream_t s);
+
 // Grouped launchers (all ops of one call share the shape).  `prefix` holds
 // the nops+1 exclusive prefix sums of the gets' sizes (device memory).
 cudaError_t launch_grp_get(Shape sh, const GroupGet* ops, const uint64_t* prefix, uint32_t nops, uint64_t total,
                            GetCfg cfg, cudaStream_t s);
-// Precheck, grid rounds, block-per-op tail to completion, and the result
-// write-back, stream-ordered with no host synchronisation.
-cudaError_t launch_grp_ins(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream_t s);
-cudaError_t launch_grp_rem(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream_t s);
+// A grouped insert / remove call in three stream-ordered phases: GRP_BEGIN
+// (control reset, precheck against the table's count in the batch),
+// GRP_ROUNDS (grid rounds r0 .. r0+nrounds-1, each a no-op for ops with
+// nothing pending), GRP_END (block-per-op tail that finishes every op from
+// round r0 -- fast when at most TAIL_MAX ops are left -- and the result
+// write-back).  sum_n (the ops' total size) sizes the grids.
+// GRP_SERIAL (inserts): every op's ops pending at round r0 one at a time in
+// index order, one block per op (for rounds that stopped making progress).
+enum { GRP_BEGIN = 0, GRP_ROUNDS = 1, GRP_END = 2, GRP_SERIAL = 3 };
+cudaError_t launch_grp_ins(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, int phase, uint32_t r0,
+                           uint32_t nrounds, cudaStream_t s);
+cudaError_t launch_grp_rem(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, int phase, uint32_t r0,
+                           uint32_t nrounds, cudaStream_t s);
+// *out = the largest pending count of round r over the ops (insert or remove).
+cudaError_t launch_grp_pending(const GroupOp* ops, uint32_t nops, uint32_t r, uint32_t* out, cudaStream_t s);
 
 // Optional device timing per kernel class: while a table's timing is on, the
 // library records a CUDA event pair around each launch made for it on the

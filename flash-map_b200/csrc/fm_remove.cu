@@ -287,13 +287,25 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_grp_rem_tail(const GroupOp* __
     rem_tail_body<KB>(g.t, g.keys, n0, r0, g.sc, g.ctl, 0xFFFFFFFFu);
 }
 
-constexpr uint32_t GRP_ROUNDS = 3;  // grid rounds before the block-per-op tail
-
 template <int KB>
-void grp_rem_shape(const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream_t s) {
+void grp_rem_shape(const GroupOp* ops, uint32_t nops, uint64_t sum_n, int phase, uint32_t r0, uint32_t nrounds,
+                   cudaStream_t s) {
     const unsigned g = grid_for(sum_n, 8);
-    k_grp_setup<<<nops, 256, 0, s>>>(ops, 0);
-    for (uint32_t r = 0; r < GRP_ROUNDS; r++) {
+    if (phase == GRP_BEGIN) {
+        k_grp_setup<<<nops, 256, 0, s>>>(ops, 0);
+        count_launches(1);
+        return;
+    }
+    if (phase == GRP_END) {
+        {
+            KtScope kt(KC_REM_TAIL, s);
+            k_grp_rem_tail<KB><<<nops, TAIL_THREADS, 0, s>>>(ops, r0);
+        }
+        k_grp_finish<<<(nops + 255) / 256, 256, 0, s>>>(ops, nops, 0);
+        count_launches(2);
+        return;
+    }
+    for (uint32_t r = r0; r < r0 + nrounds; r++) {
         {
             KtScope kt(KC_REM_MARK, s);
             k_grp_rem_p1<KB><<<g, RBLOCK, 0, s>>>(ops, nops, r);
@@ -307,12 +319,7 @@ void grp_rem_shape(const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream
             k_grp_rem_p3<KB><<<g, RBLOCK, 0, s>>>(ops, nops, r);
         }
     }
-    {
-        KtScope kt(KC_REM_TAIL, s);
-        k_grp_rem_tail<KB><<<nops, TAIL_THREADS, 0, s>>>(ops, GRP_ROUNDS);
-    }
-    k_grp_finish<<<(nops + 255) / 256, 256, 0, s>>>(ops, nops, 0);
-    count_launches(2 + 3 * GRP_ROUNDS + 1 + 1);
+    count_launches(3 * nrounds);
 }
 
 template <int KB>
@@ -351,15 +358,16 @@ cudaError_t launch_rem_rounds(const TableView& t, Shape sh, const uint8_t* keys,
     return cudaGetLastError();
 }
 
-cudaError_t launch_grp_rem(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, cudaStream_t s) {
+cudaError_t launch_grp_rem(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, int phase, uint32_t r0,
+                           uint32_t nrounds, cudaStream_t s) {
     if (nops == 0) return cudaSuccess;
     switch (sh) {
         case SHAPE_8_8:
-        case SHAPE_8_32: grp_rem_shape<8>(ops, nops, sum_n, s); break;
+        case SHAPE_8_32: grp_rem_shape<8>(ops, nops, sum_n, phase, r0, nrounds, s); break;
         case SHAPE_32_128:
         case SHAPE_32_64:
-        case SHAPE_32_32: grp_rem_shape<32>(ops, nops, sum_n, s); break;
-        default: grp_rem_shape<0>(ops, nops, sum_n, s); break;
+        case SHAPE_32_32: grp_rem_shape<32>(ops, nops, sum_n, phase, r0, nrounds, s); break;
+        default: grp_rem_shape<0>(ops, nops, sum_n, phase, r0, nrounds, s); break;
     }
     return cudaGetLastError();
 }

@@ -27,6 +27,7 @@ template <int T>
 struct Tile {
     static_assert(T == 4 || T == 8 || T == 16 || T == 32, "tile width");
     static constexpr uint32_t TM = (T == 32) ? 0xFFFFFFFFu : ((1u << T) - 1u);
+    static constexpr int W = T;  // lanes
     uint32_t lane;   // 0..T-1
     uint32_t base;   // first lane of the tile in its warp
     uint32_t wmask;  // the tile's lanes as a warp mask
@@ -41,6 +42,15 @@ struct Tile {
         return __shfl_sync(wmask, v, base + src);
     }
     __device__ __forceinline__ void sync() const { __syncwarp(wmask); }
+};
+
+// The whole block as one crew of W threads (tile_moves over a block).
+template <int W_>
+struct BlockCrew {
+    static constexpr int W = W_;
+    uint32_t lane;
+    __device__ __forceinline__ BlockCrew() : lane(threadIdx.x) {}
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
 };
 
 // Pending list of round r (a select, so the scratch struct stays in registers).

@@ -23,7 +23,7 @@ EXPORTS = (
     "fm_bulk_remove_device", "fm_recount", "fm_last_error", "fm_launch_count", "fm_snapshot", "fm_load",
     "fm_bulk_insert_device_noalloc", "fm_kernel_timing", "fm_kernel_times", "fm_kernel_times_reset",
     "fm_kernel_class_name", "fm_batch_create", "fm_batch_capture", "fm_batch_run", "fm_batch_wait",
-    "fm_batch_waves", "fm_batch_destroy",
+    "fm_batch_waves", "fm_batch_destroy", "fm_autotune", "fm_tuned_get_config", "fm_copy",
 )
 
 
@@ -110,6 +110,12 @@ def _declare(L) -> None:
     L.fm_batch_waves.argtypes = [vp]
     L.fm_batch_destroy.restype = None
     L.fm_batch_destroy.argtypes = [vp]
+    L.fm_copy.restype = i32
+    L.fm_copy.argtypes = [vp, vp, vp]
+    L.fm_autotune.restype = i32
+    L.fm_autotune.argtypes = [i32, C.c_char_p]
+    L.fm_tuned_get_config.restype = i32
+    L.fm_tuned_get_config.argtypes = [u32, u32, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int)]
 
 
 def load_library(path: str = LIB_PATH):
@@ -131,6 +137,22 @@ def load_library(path: str = LIB_PATH):
 def launch_count() -> int:
     """Kernels launched by the library in this process (instrumentation)."""
     return load_library().fm_launch_count()
+
+
+def autotune(device: int = 0, cache_path: str = None) -> None:
+    """Time the lookup kernel configurations on `device` and use the fastest
+    per record shape and load (fm_autotune)."""
+    from .errors import raise_for_status
+
+    rc = load_library().fm_autotune(device, cache_path.encode() if cache_path else None)
+    raise_for_status(rc, last_error())
+
+
+def tuned_get_config(key_size: int, value_size: int, load: float):
+    """(lanes per query, blocks per SM) the lookups of such a table use."""
+    lanes, bps = C.c_int(0), C.c_int(0)
+    load_library().fm_tuned_get_config(key_size, value_size, load, C.byref(lanes), C.byref(bps))
+    return lanes.value, bps.value
 
 
 def last_error() -> str:

@@ -225,6 +225,11 @@ class FlashMap:
         self._check(self._L.fm_recount(self._h, C.byref(out)))
         return out.value
 
+    def copy_from(self, other: "FlashMap", stream=None) -> None:
+        """Device-side copy of `other` (same capacity and record sizes) into
+        this table: slots, len and probe facts (fm_copy)."""
+        self._check(self._L.fm_copy(self._h, other._h, _stream_ptr(stream)))
+
     # -- per-kernel device timing (instrumentation) -------------------------
     def kernel_timing(self, on: bool = True, reset: bool = False) -> None:
         """Record CUDA events around this table's kernel launches while on."""

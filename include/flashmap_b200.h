@@ -150,7 +150,7 @@ int fm_kernel_times(fm_table* t, double* total_ms, uint64_t* launches, uint32_t 
 int fm_kernel_times_reset(fm_table* t);
 const char* fm_kernel_class_name(uint32_t cls);
 
-/* Batched form (no counterpart in gpu.rs; the batching row of the design).
+/* Batched form (no counterpart in gpu.rs).
  * A queue of bulk operations over any number of tables of one device, with
  * device-resident keys, values and outputs, executed with the result of
  * calling fm_bulk_get_device / fm_bulk_insert_device / fm_bulk_remove_device
@@ -158,9 +158,15 @@ const char* fm_kernel_class_name(uint32_t cls);
  * table's count after the ops before it).  The ops are planned into waves of
  * independent ops (distinct tables; consecutive gets of one table share a
  * wave); each wave runs grouped kernels that serve all its ops of one kind
- * and record shape per launch, with no host synchronisation between waves.
- * fm_batch_capture records the whole batch into a CUDA graph that later
- * fm_batch_run calls replay.  Between fm_batch_run and fm_batch_wait the
+ * and record shape per launch.  Without a graph, fm_batch_run drives each
+ * wave's insert/remove rounds from the host (a 4-byte readback per two
+ * rounds, as the plain calls do) and records how many rounds each wave
+ * needed.  fm_batch_capture records the whole batch into a CUDA graph with
+ * those round counts (3 per wave before any eager run) and no host
+ * synchronisation; later fm_batch_run calls replay it.  A replay whose data
+ * needs more rounds than recorded still gives the same results, more slowly
+ * (the remaining ops finish in a single block per op) -- run the batch
+ * eagerly once on representative data before capturing.  Between fm_batch_run and fm_batch_wait the
  * batch's tables must not be used by other calls.  Per-op results (new /
  * removed key counts) and status codes (FM_OK, FM_ERR_TABLE_FULL,
  * FM_ERR_PROBE_LIMIT, ...) are written back into the op array by
@@ -186,6 +192,22 @@ int fm_batch_run(fm_batch* b, void* stream);
 int fm_batch_wait(fm_batch* b, fm_op* ops);
 uint32_t fm_batch_waves(const fm_batch* b);
 void fm_batch_destroy(fm_batch* b);
+
+/* Device-side copy of a whole table (no counterpart in gpu.rs): dst takes
+ * src's slots, len and persistent probe facts; both must have the same
+ * capacity and record sizes.  Stream-ordered on `stream`.  Keeps a checkpoint
+ * of a table on the GPU to roll back to. */
+int fm_copy(fm_table* dst, const fm_table* src, void* stream);
+
+/* Lookup autotuner (no counterpart in gpu.rs).  Times every lookup kernel
+ * configuration -- lanes per query (1, 4, 8, 16, 32) x resident blocks per SM
+ * (8, 16, 32, 64) -- per compile-time record shape (8/8, 32/128, 32/64, 32/32,
+ * 8/32) and load bucket (< 0.6, < 0.8, >= 0.8) on sample tables of 2^20 slots,
+ * and makes the fastest the configuration of every later lookup (plain and
+ * batched) in the process.  With cache_path, a file of earlier results is
+ * loaded instead when it exists, and new results are written to it. */
+int fm_autotune(int device, const char* cache_path);
+int fm_tuned_get_config(uint32_t key_size, uint32_t value_size, double load, int* lanes, int* blocks_per_sm);
 
 /* Raw table access for layout checks and for loading a prefilled table:
  * flags (capacity u32), keys (capacity*K bytes), values (capacity*V bytes),

@@ -168,3 +168,35 @@ def test_batch_single_table_chain_of_dependent_ops():
     gf, gk, gv = g.snapshot()
     of_, ok, ov = o.snapshot()
     assert np.array_equal(gf, of_) and np.array_equal(gk, ok) and np.array_equal(gv, ov)
+
+
+def test_batch_ops_larger_than_any_earlier_call():
+    """Fresh tables whose queued ops are far larger than any call they have
+    seen: the per-table scratch grows to the largest op before any wave's
+    descriptors are written (the small op queued first must not keep a stale
+    scratch address)."""
+    import flash_map as F
+
+    rng = np.random.default_rng(9)
+    tables, queue = [], []
+    for ks, vs in [(8, 8), (32, 128)]:
+        cap = 1 << 17
+        g = gpu_map(cap, ks, vs)
+        o = OracleAdapter(cap, ks, vs)
+        tables.append({"g": g, "o": o, "ks": ks, "vs": vs, "known": []})
+    for ti, t in enumerate(tables):
+        for n in (100, 60_000, 3_000):
+            queue.append((ti, F.batch.INSERT, _keys(rng, n, t["ks"]), _keys(rng, n, t["vs"])))
+        queue.append((ti, F.batch.REMOVE, queue[-2][2][: 20_000], None))
+        queue.append((ti, F.batch.GET, queue[-3][2], None))
+    g_res, g_out = run_batch(tables, queue, False)
+    o_res, o_out = oracle_replay(tables, queue)
+    assert g_res == o_res
+    for i, (ti, kind, k, v) in enumerate(queue):
+        if kind == F.batch.GET:
+            assert np.array_equal(g_out[i][1].astype(bool), o_out[i][1])
+            assert np.array_equal(g_out[i][0], o_out[i][0])
+    for t in tables:
+        gf, gk, gv = t["g"].snapshot()
+        of_, ok, ov = t["o"].snapshot()
+        assert np.array_equal(gf, of_) and np.array_equal(gk, ok) and np.array_equal(gv, ov)

@@ -408,7 +408,7 @@ def test_many_possible_updates(shape, run):
         assert_same_layout(g, o)
 
 
-@pytest.mark.parametrize("load", [0.9, 0.97])
+@pytest.mark.parametrize("load", [0.9, 0.97, 0.995])
 def test_high_load_fill_and_churn(load):
     """u64 pairs filled to a high load in calls of 2% of the capacity (eviction
     chains of hundreds of entries, many possible updates per walk), then
