@@ -588,6 +588,92 @@ def batched_leg(torch, F, native, dev, steps, warmup, scale=1):
     }
 
 
+# ---------------------------------------------------------------------------
+# Served form: Poisson request stream against a device-resident table
+# ---------------------------------------------------------------------------
+SERVE_RATE, SERVE_REQS = 2000.0, 500
+
+
+def served_leg(torch, F, dev, scale=1):
+    """The serving workload: FlashMap<[u8;32],[u8;128]> with_capacity(50M)
+    (2^26 slots) prefilled with 30M random entries; requests arrive as a
+    Poisson stream at 2,000/s, each insert / get / remove with probability
+    0.3 / 0.6 / 0.1 and a size log-uniform in 64..1M keys, get and remove keys
+    80% present (Zipf s=0.9 over a 4M-key sample of the present keys); 20 GB
+    staging budget.  500 requests (a quarter second of arrivals), served with
+    continuous batching and, from the same start state (a device copy), by
+    the plain one-call-per-request server.  Request inputs are slices of
+    pinned host pools (inserts: fresh keys; gets/removes: the skewed mix)."""
+    from flash_map.serve import FlashMapServer, PlainServer, Request, latency_summary
+
+    rng = np.random.default_rng(6)
+    g = torch.Generator(device=dev)
+    g.manual_seed(6)
+    cap_req, prefill = 50_000_000 // scale, 30_000_000 // scale
+    m = F.FlashMap(cap_req, KB, VB, F.HashStrategy.Identity, dev.index or 0)
+    pk = torch.randint(0, 256, (prefill, KB), dtype=torch.uint8, device=dev, generator=g)
+    pv = torch.randint(0, 256, (prefill, VB), dtype=torch.uint8, device=dev, generator=g)
+    for b in range(0, prefill, 4_000_000):
+        n = min(4_000_000, prefill - b)
+        m.bulk_insert_device(pk[b:b + n], pv[b:b + n], n)
+    backup = F.FlashMap(cap_req, KB, VB, F.HashStrategy.Identity, dev.index or 0)
+    backup.copy_from(m)
+    sample = pk[: min(4_000_000, prefill)].cpu().numpy()
+    del pk, pv
+    n_req = SERVE_REQS
+    kinds = rng.choice([1, 0, 2], size=n_req, p=[0.3, 0.6, 0.1])
+    sizes = np.exp(rng.uniform(np.log(64), np.log(1_000_000 // scale), n_req)).astype(np.int64)
+    arrivals = np.cumsum(rng.exponential(1.0 / SERVE_RATE, n_req))
+    n_ins = int(sizes[kinds == 1].sum())
+    n_look = int(sizes[kinds != 1].sum())
+    ins_k = torch.randint(0, 256, (n_ins, KB), dtype=torch.uint8).pin_memory().numpy()
+    ins_v = torch.randint(0, 256, (n_ins, VB), dtype=torch.uint8).pin_memory().numpy()
+    # lookup pool: 80% present with Zipf(0.9) ranks (inverse CDF of r^-0.9), 20% fresh
+    pool_n = min(n_look, 24_000_000 // scale)
+    ranks = np.minimum((rng.random(pool_n) ** 10 * len(sample)).astype(np.int64), len(sample) - 1)
+    look = sample[ranks]
+    fresh = rng.random(pool_n) < 0.2
+    look[fresh] = rng.integers(0, 256, (int(fresh.sum()), KB), dtype=np.uint8)
+    look = torch.from_numpy(look).pin_memory().numpy()
+    out_v = torch.empty((1_000_000 // scale + 1, VB), dtype=torch.uint8).pin_memory()
+    out_f = torch.empty((1_000_000 // scale + 1,), dtype=torch.uint8).pin_memory()
+
+    def requests():
+        reqs, io, lo = [], 0, 0
+        for i in range(n_req):
+            n = int(sizes[i])
+            if kinds[i] == 1:
+                reqs.append(Request(1, ins_k[io:io + n], ins_v[io:io + n], float(arrivals[i])))
+                io += n
+            else:
+                if lo + n > pool_n:
+                    lo = 0
+                reqs.append(Request(int(kinds[i]), look[lo:lo + n], None, float(arrivals[i])))
+                lo += n
+        return reqs
+
+    torch.cuda.synchronize()
+    total_keys = int(sizes.sum())
+    out = {"workload": f"{n_req} requests, Poisson {SERVE_RATE:.0f}/s, insert/get/remove 0.3/0.6/0.1, sizes "
+                       f"log-uniform 64..{1_000_000 // scale}, 80% present Zipf(0.9) on get/remove, table "
+                       f"with_capacity({cap_req}) prefilled with {prefill}, 20 GB staging budget",
+           "keys": total_keys}
+    reqs_s = requests()
+    srv = FlashMapServer(m, budget=20 << 30, out_pool=lambda n, v: (out_v[:n], out_f[:n]))
+    wall = srv.serve(reqs_s, realtime=True)
+    out["served"] = dict(latency_summary(reqs_s), mops=round(total_keys / wall / 1e6, 3), wall_s=round(wall, 3),
+                         batches=srv.batches, mean_requests_per_batch=round(n_req / max(srv.batches, 1), 2))
+    m.copy_from(backup)
+    torch.cuda.synchronize()
+    reqs_p = requests()
+    wall_p = PlainServer(m, out_pool=lambda n, v: (out_v[:n].numpy(), out_f[:n].numpy())).serve(reqs_p, realtime=True)
+    out["plain"] = dict(latency_summary(reqs_p), mops=round(total_keys / wall_p / 1e6, 3), wall_s=round(wall_p, 3))
+    out["identical_results"] = all((a.result, a.status) == (b.result, b.status) for a, b in zip(reqs_s, reqs_p))
+    m.close()
+    backup.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -598,6 +684,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-as-written", action="store_true", help="skip the load-0.477 variant")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form workload")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-form workload")
     ap.add_argument("--nvtx", action="store_true",
                     help="mark one insert call and the bulk_get of the kernel-timing step with NVTX ranges")
     ap.add_argument("--scale", type=int, default=1,
@@ -688,6 +775,9 @@ def main():
         line["batched"] = batched_leg(torch, F, _native, dev, max(1, min(args.steps, 3)), 1, args.scale)
         line["batched"]["autotuned_get"] = {"u64": _native.tuned_get_config(8, 8, 0.7),
                                             "account": _native.tuned_get_config(KB, VB, 0.7)}
+
+    if not args.no_served:
+        line["served"] = served_leg(torch, F, dev, args.scale)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb, bpo = cpu_baseline_leg(main_w)

@@ -991,7 +991,60 @@ static_assert(fm::STATUS_TABLE_FULL == FM_ERR_TABLE_FULL && fm::STATUS_PROBE_LIM
                   fm::STATUS_KERNEL == FM_ERR_KERNEL_LAUNCH,
               "device status codes");
 
+// Device and pinned host memory of a batch, carved from one block each and
+// kept for reuse when the batch is destroyed (allocating pinned memory costs
+// milliseconds and freeing device memory synchronises the device, which a
+// server creating a batch per step would pay every step).
+struct BatchArena {
+    int device = -1;
+    uint8_t* d = nullptr;
+    size_t dcap = 0;
+    uint8_t* h = nullptr;
+    size_t hcap = 0;
+};
+
+namespace {
+std::mutex g_arena_mu;
+std::vector<BatchArena> g_arenas;  // free arenas
+constexpr size_t ARENA_KEEP = 8;
+
+BatchArena arena_take(int device, size_t dneed, size_t hneed, cudaError_t* err) {
+    {
+        std::lock_guard<std::mutex> g(g_arena_mu);
+        for (size_t i = 0; i < g_arenas.size(); i++) {
+            if (g_arenas[i].device == device && g_arenas[i].dcap >= dneed && g_arenas[i].hcap >= hneed) {
+                BatchArena a = g_arenas[i];
+                g_arenas.erase(g_arenas.begin() + i);
+                *err = cudaSuccess;
+                return a;
+            }
+        }
+    }
+    BatchArena a;
+    a.device = device;
+    a.dcap = dneed + dneed / 2;
+    a.hcap = hneed + hneed / 2;
+    *err = cudaMalloc((void**)&a.d, a.dcap);
+    if (*err == cudaSuccess) *err = cudaMallocHost((void**)&a.h, a.hcap);
+    return a;
+}
+
+void arena_give(BatchArena a) {
+    if (!a.d && !a.h) return;
+    {
+        std::lock_guard<std::mutex> g(g_arena_mu);
+        if (g_arenas.size() < ARENA_KEEP) {
+            g_arenas.push_back(a);
+            return;
+        }
+    }
+    if (a.d) cudaFree(a.d);
+    if (a.h) cudaFreeHost(a.h);
+}
+}  // namespace
+
 struct fm_batch {
+    BatchArena arena;
     int device = 0;
     std::vector<fm_op> ops;
     std::vector<fm_table*> tables;      // distinct tables, batch order
@@ -1111,6 +1164,8 @@ int batch_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
     cudaError_t e = cudaMemcpyAsync(b->d_desc, b->h_desc, b->desc_bytes, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->d_len, b->h_len(), b->tables.size() * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_res, 0, b->ops.size() * 8, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_status, 0, b->ops.size() * 4, s);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "batch upload", e);
     for (auto& g : b->groups) {
         const uint32_t n = (uint32_t)g.members.size();
@@ -1238,20 +1293,24 @@ int fm_batch_create(const fm_op* ops, uint32_t nops, fm_batch** out) {
     }
     b->desc_bytes = off ? off : 256;
     DeviceGuard dg(b->device);
-    cudaError_t e = cudaMalloc((void**)&b->d_desc, b->desc_bytes);
-    if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_desc, b->desc_bytes);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_len, b->tables.size() * 8);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_res, nops * 8);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_status, nops * 4);
-    if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_io, b->io_bytes());
-    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_pend, 4);
-    if (e == cudaSuccess) e = cudaMallocHost((void**)&b->h_pend, 4);
-    if (e == cudaSuccess) e = cudaMemset(b->d_res, 0, nops * 8);
-    if (e == cudaSuccess) e = cudaMemset(b->d_status, 0, nops * 4);
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t o_len = al(b->desc_bytes), o_res = o_len + al(b->tables.size() * 8), o_st = o_res + al(nops * 8),
+                 o_pend = o_st + al(nops * 4), dneed = o_pend + 256;
+    const size_t h_io = al(b->desc_bytes), h_pend = h_io + al(b->io_bytes()), hneed = h_pend + 256;
+    cudaError_t e = cudaSuccess;
+    b->arena = arena_take(b->device, dneed, hneed, &e);
     if (e != cudaSuccess) {
         fm_batch_destroy(b);
         return cuda_fail(FM_ERR_GPU_ALLOC, "batch buffers", e);
     }
+    b->d_desc = b->arena.d;
+    b->d_len = reinterpret_cast<unsigned long long*>(b->arena.d + o_len);
+    b->d_res = reinterpret_cast<unsigned long long*>(b->arena.d + o_res);
+    b->d_status = reinterpret_cast<int*>(b->arena.d + o_st);
+    b->d_pend = reinterpret_cast<uint32_t*>(b->arena.d + o_pend);
+    b->h_desc = b->arena.h;
+    b->h_io = b->arena.h + h_io;
+    b->h_pend = reinterpret_cast<uint32_t*>(b->arena.h + h_pend);
     memset(b->h_desc, 0, b->desc_bytes);
     memset(b->h_io, 0, b->io_bytes());
     *out = b;
@@ -1341,14 +1400,7 @@ void fm_batch_destroy(fm_batch* b) {
     if (b->pending && b->last_stream) cudaStreamSynchronize(b->last_stream);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
-    cudaFree(b->d_desc);
-    cudaFree(b->d_len);
-    cudaFree(b->d_res);
-    cudaFree(b->d_status);
-    if (b->h_desc) cudaFreeHost(b->h_desc);
-    if (b->h_io) cudaFreeHost(b->h_io);
-    cudaFree(b->d_pend);
-    if (b->h_pend) cudaFreeHost(b->h_pend);
+    arena_give(b->arena);
     delete b;
 }
 
