@@ -271,7 +271,7 @@ REMOVE_KERNELS = ("k_rem_p1", "k_rem_p2", "k_rem_p3", "k_rem_tail")
 # the same load factor and call size (the traffic summary under
 # profiles/ gives the command and the per-kernel figures); traffic grows with
 # the ops processed.
-NCU_TRAFFIC_PER_OP = {"insert": 1275.6, "get": 330.4, "remove": 846.3}
+NCU_TRAFFIC_PER_OP = {"insert": 1238.7, "get": 330.3, "remove": 840.7}
 
 
 class DeviceRun:
@@ -329,12 +329,14 @@ class DeviceRun:
 
     def kernel_pass(self, nvtx=False):
         """One more step with the library's per-kernel CUDA events on.  With
-        nvtx, the last full insert call of the step (the highest load) and
-        its bulk_get sit in NVTX ranges "insert_call" and "get_call" (for ncu
-        --nvtx-include)."""
+        nvtx, the step sits in the NVTX range "step", and within it the last
+        full insert call (the highest load) and the bulk_get in "insert_call"
+        and "get_call" (for ncu --nvtx-include)."""
         self.m.kernel_timing(True, reset=True)
         if nvtx:
             w, m, s, nv = self.w, self.m, self.stream, self.torch.cuda.nvtx
+            self.torch.cuda.synchronize()
+            nv.range_push("step")
             m.clear()
             mid = (w.pairs // CALL - 1) * CALL
             for b in range(0, w.pairs, CALL):
@@ -350,6 +352,8 @@ class DeviceRun:
             self.torch.cuda.synchronize()
             nv.range_pop()
             m.bulk_remove_device(self.rem, w.removes, s)
+            self.torch.cuda.synchronize()
+            nv.range_pop()
         else:
             self.step()
         self.torch.cuda.synchronize()
