@@ -28,6 +28,8 @@
 // Grid kernels aggregate list appends and counts per block so no address
 // takes more than one atomic per block.
 #include <climits>
+#include <limits>
+#include <cstdlib>
 #include <type_traits>
 
 #include "fm_rounds.cuh"
@@ -97,13 +99,31 @@ __device__ __forceinline__ uint32_t walk_op(const TableView& t, uint32_t j, uint
         // At most the capacity-1 slots after F; coming back to F means the
         // flow wraps the whole table.
         uint64_t F2 = NONE64;
-        while (walked < mask) {
-            const uint64_t s = pos & mask;
-            ++pos;
-            ++walked;
-            if (is_free(t.flags[s])) {
-                F2 = s;
-                break;
+        if (mask >= 7) {  // aligned 8-slot windows, one 32-byte sector each
+            for (uint64_t wb = pos & ~7ull; F2 == NONE64 && walked < mask; wb += 8) {
+                const uint4* fp = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
+                const uint4 a = fp[0], b = fp[1];
+                const uint32_t f8[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+                for (int l = 0; l < 8; l++) {
+                    if (F2 != NONE64 || wb + l < pos || walked >= mask) continue;
+                    ++walked;
+                    if (is_free(f8[l])) F2 = wb + l;
+                }
+            }
+            if (F2 != NONE64) {
+                pos = F2 + 1;
+                F2 &= mask;
+            }
+        } else {
+            while (walked < mask) {
+                const uint64_t s = pos & mask;
+                ++pos;
+                ++walked;
+                if (is_free(t.flags[s])) {
+                    F2 = s;
+                    break;
+                }
             }
         }
         if (F2 == NONE64) return 1u;
@@ -569,14 +589,15 @@ constexpr int TMAXCH = 256;  // eviction slots held per tile
 constexpr int TMAXC = 128;   // possible updates of one window (>= 4T)
 constexpr uint32_t NOSRC = 0xFFFFFFFFu;
 
-template <int MAXCH_>
+template <int MAXCH_, int MAXC_ = TMAXC>
 struct ChainBuf {
     static constexpr int MAXCH = MAXCH_;
+    static constexpr int MAXC = MAXC_;
     uint32_t pos[MAXCH];    // eviction slots of the current chunk
     uint32_t p[MAXCH];      // depth stored at each of them
-    uint32_t cpos[TMAXC];   // possible updates of the current window: slot,
-    uint32_t cstage[TMAXC]; //   evictions before it,
-    uint32_t csrc[TMAXC];   //   slot holding the carried key (NOSRC: the new key)
+    uint32_t cpos[MAXC];    // possible updates of the current window: slot,
+    uint32_t cstage[MAXC];  //   evictions before it,
+    uint32_t csrc[MAXC];    //   slot holding the carried key (NOSRC: the new key)
     uint32_t src_base;      // slot evicted just before the chunk's first stage
 };
 using TileChain = ChainBuf<TMAXCH>;
@@ -632,11 +653,11 @@ __device__ __forceinline__ uint32_t tile_sum(uint32_t v, const Tile<T>& tl) {
     }
     return v;
 }
-template <int T>
-__device__ __forceinline__ long long tile_max(long long v, const Tile<T>& tl) {
+template <int T, class P>
+__device__ __forceinline__ P tile_max(P v, const Tile<T>& tl) {
 #pragma unroll
     for (int d = 1; d < T; d <<= 1) {
-        const long long o = __shfl_up_sync(tl.wmask, v, d, T);
+        const P o = __shfl_up_sync(tl.wmask, v, d, T);
         if ((int)tl.lane >= d) v = max(v, o);
     }
     return v;
@@ -706,15 +727,20 @@ __device__ __forceinline__ void tile_moves(const TableView& t, const RegKey<KB>&
 //         (stages from chunk_base) in s.pos; returns 1 claim, 2 update,
 //         3 drop, 5 (never in a non-serial round) walk past the bound.
 //   otherwise: records the eviction slots of stages [lo, hi) and stops.
-template <int KB, int T, class C>
-__device__ int tile_walk(const TableView& t, const RegKey<KB>& key, C& s, const Tile<T>& tl, bool find,
-                         uint32_t lo, uint32_t hi, uint32_t& k, uint32_t& chunk_base, uint32_t& src_base,
-                         uint64_t& end_slot, uint64_t& end_p, bool& end_tomb) {
+// Positions are kept relative to the first window's base in the signed type
+// P: int (32-bit scans) for tables below 2^30 slots, 64-bit above.
+template <int KB, int T, class C, class P>
+__device__ int tile_walk_p(const TableView& t, const RegKey<KB>& key, C& s, const Tile<T>& tl, bool find,
+                           uint32_t lo, uint32_t hi, uint32_t& k, uint32_t& chunk_base, uint32_t& src_base,
+                           uint64_t& end_slot, uint64_t& end_p, bool& end_tomb) {
     constexpr int MAXCH = C::MAXCH;
-    static_assert(TMAXC >= 4 * T && MAXCH >= 8 * T, "a window's updates and evictions must fit the buffers");
+    static_assert(C::MAXC >= 4 * T && MAXCH >= 8 * T, "a window's updates and evictions must fit the buffers");
     const uint64_t mask = t.mask;
+    constexpr P PMIN = std::numeric_limits<P>::min();
     const uint64_t h = key.hash(KB, t.hash_mode) & mask;
-    long long M = (long long)h;  // the carried entry's home (unwrapped positions)
+    const uint64_t wb0 = h & ~(uint64_t)(4 * T - 1);  // origin of the relative positions
+    const P hr = (P)(h - wb0);
+    P M = hr;  // the carried entry's home
     uint32_t g = 0;              // evictions so far
     uint32_t last_ev = NOSRC;    // slot of the last eviction
     int kind = 0;
@@ -738,27 +764,26 @@ __device__ int tile_walk(const TableView& t, const RegKey<KB>& key, C& s, const 
         const uint4 fw = *reinterpret_cast<const uint4*>(t.flags + (base & mask));
         const uint32_t f[4] = {fw.x, fw.y, fw.z, fw.w};
         // homes of the occupied slots on the walk, and the running maximum
-        long long hh[4];
-        long long lm = LLONG_MIN;
+        const P br = (P)(base - wb0);
+        P hh[4];
+        P lm = PMIN;
 #pragma unroll
         for (int i = 0; i < 4; i++) {
-            const uint64_t pos = base + i;
-            hh[i] = (pos >= h && st_of(f[i]) == ST_OCC) ? (long long)pos - (long long)dist_of(f[i]) : LLONG_MIN;
+            hh[i] = (br + i >= hr && st_of(f[i]) == ST_OCC) ? br + i - (P)dist_of(f[i]) : PMIN;
             lm = max(lm, hh[i]);
         }
-        const long long incl = tile_max<T>(lm, tl);
-        long long mx = __shfl_up_sync(tl.wmask, incl, 1, T);
+        const P incl = tile_max<T, P>(lm, tl);
+        P mx = __shfl_up_sync(tl.wmask, incl, 1, T);
         mx = tl.lane == 0 ? M : max(M, mx);
         // classify: end (free or drop), eviction, possible update
         uint32_t endb = 0, evb = 0, cdb = 0, pend[4];
-        long long mi[4];
+        P mi[4];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
-            const uint64_t pos = base + i;
             mi[i] = mx;
-            const uint64_t depth = (uint64_t)((long long)pos - mx);
+            const uint64_t depth = (uint64_t)(br + i - mx);
             pend[i] = (uint32_t)depth;
-            if (pos >= h) {
+            if (br + i >= hr) {
                 const uint32_t st = st_of(f[i]);
                 if (depth > mask || st == ST_EMPTY || st == ST_TOMB) endb |= 1u << i;
                 else if (hh[i] > mx) evb |= 1u << i;
@@ -778,9 +803,9 @@ __device__ int tile_walk(const TableView& t, const RegKey<KB>& key, C& s, const 
         const uint32_t etot = tl.shfl(einc, T - 1);
         uint32_t gi = g + einc - ne;
         // the last eviction before each slot (for the possible updates' carried key)
-        long long lastpos = evb ? (long long)(base + 31 - __clz(evb)) : -1;
-        const long long linc = tile_max<T>(lastpos, tl);
-        long long lprev = __shfl_up_sync(tl.wmask, linc, 1, T);
+        P lastpos = evb ? br + (P)(31 - __clz(evb)) : (P)-1;
+        const P linc = tile_max<T, P>(lastpos, tl);
+        P lprev = __shfl_up_sync(tl.wmask, linc, 1, T);
         if (tl.lane == 0) lprev = -1;
         uint32_t co = 0;
         uint32_t nc_tot = 0;
@@ -800,12 +825,12 @@ __device__ int tile_walk(const TableView& t, const RegKey<KB>& key, C& s, const 
                     s.p[stg - chunk_base] = pend[i];
                 }
                 if (!find && stg + 1 == lo) s.src_base = (uint32_t)(pos & mask);
-                lprev = (long long)pos;
+                lprev = br + i;
                 ++stg;
             } else if (find && ((cdb >> i) & 1u)) {
                 s.cpos[co] = (uint32_t)(pos & mask);
                 s.cstage[co] = stg;
-                s.csrc[co] = lprev >= 0 ? (uint32_t)((uint64_t)lprev & mask)
+                s.csrc[co] = lprev >= 0 ? (uint32_t)((wb0 + (uint64_t)lprev) & mask)
                                         : (last_ev == NOSRC ? NOSRC : last_ev);
                 ++co;
             }
@@ -841,22 +866,21 @@ __device__ int tile_walk(const TableView& t, const RegKey<KB>& key, C& s, const 
         }
         // advance: evictions, last eviction slot, carried home
         if (etot) {
-            const long long lw = tl.shfl(linc, T - 1);
-            last_ev = (uint32_t)((uint64_t)lw & mask);
+            const P lw = tl.shfl(linc, T - 1);
+            last_ev = (uint32_t)((wb0 + (uint64_t)lw) & mask);
         }
         g += etot;
-        const long long mall = tl.shfl(incl, T - 1);
+        const P mall = tl.shfl(incl, T - 1);
         if (em) {
             // the end slot: its depth is position - running max before it
             const uint32_t dsel = myi == 0 ? pend[0] : (myi == 1 ? pend[1] : (myi == 2 ? pend[2] : pend[3]));
             const uint32_t fsel = myi == 0 ? f[0] : (myi == 1 ? f[1] : (myi == 2 ? f[2] : f[3]));
-            const uint64_t ep = (uint64_t)(long long)tl.shfl((long long)dsel, elane);
             const uint32_t ef = tl.shfl(fsel, elane);
             const uint64_t epos = wb + 4 * elane + tl.shfl(myi, elane);
             // depth as a full 64-bit value (pend holds its low 32 bits)
-            const long long mend = tl.shfl(myi == 0 ? mi[0] : (myi == 1 ? mi[1] : (myi == 2 ? mi[2] : mi[3])), elane);
-            const uint64_t edepth = (uint64_t)((long long)epos - mend);
-            (void)ep;
+            const P mend = tl.shfl(myi == 0 ? mi[0] : (myi == 1 ? mi[1] : (myi == 2 ? mi[2] : mi[3])), elane);
+            const uint64_t edepth = (uint64_t)((P)(epos - wb0) - mend);
+            (void)dsel;
             kind = (edepth > mask) ? 3 : 1;
             end_slot = epos & mask;
             end_p = edepth;
@@ -875,6 +899,17 @@ __device__ int tile_walk(const TableView& t, const RegKey<KB>& key, C& s, const 
     if (!find) src_base = s.src_base;
     tl.sync();
     return kind;
+}
+
+template <int KB, int T, class C>
+__device__ __forceinline__ int tile_walk(const TableView& t, const RegKey<KB>& key, C& s, const Tile<T>& tl,
+                                         bool find, uint32_t lo, uint32_t hi, uint32_t& k, uint32_t& chunk_base,
+                                         uint32_t& src_base, uint64_t& end_slot, uint64_t& end_p, bool& end_tomb) {
+    if (t.mask < (1ull << 30))
+        return tile_walk_p<KB, T, C, int>(t, key, s, tl, find, lo, hi, k, chunk_base, src_base, end_slot, end_p,
+                                          end_tomb);
+    return tile_walk_p<KB, T, C, long long>(t, key, s, tl, find, lo, hi, k, chunk_base, src_base, end_slot, end_p,
+                                            end_tomb);
 }
 
 // One insert by a tile (capacity >= 4T, rounds that are not serial).
@@ -1083,8 +1118,11 @@ __global__ void __launch_bounds__(RBLOCK) k_ins_p2(TableView t, uint32_t n0, uin
     }
 }
 
+#ifndef FM_P3_MIN_BLOCKS
+#define FM_P3_MIN_BLOCKS 3  // resident blocks per SM the thread-per-op pass is compiled for
+#endif
 template <int KB, int VB>
-__global__ void __launch_bounds__(RBLOCK, 3) k_ins_p3(TableView t, const uint8_t* __restrict__ keys,
+__global__ void __launch_bounds__(RBLOCK, FM_P3_MIN_BLOCKS) k_ins_p3(TableView t, const uint8_t* __restrict__ keys,
                                                    const uint8_t* __restrict__ vals, uint32_t n0, uint32_t r,
                                                    OpScratch sc, Ctl* ctl) {
     __shared__ AppendSmem s_app;
@@ -1151,21 +1189,27 @@ __device__ __forceinline__ bool finish_tile(const TableView& t, const uint8_t* k
 }
 
 // Phase 4: the inserts of round r whose walks were too long for one thread,
-// one P4_T-lane tile each.  Their segments are disjoint from each other and
-// from every op run in phase 3.
-constexpr int P4_T = 32;
+// one T-lane tile each (T = 8 or 16 share every warp instruction between 4
+// or 2 inserts; the closed-form walk keeps their control flow together).
+// Their segments are disjoint from each other and from every op run in
+// phase 3.
+template <int T>
+using P4Chain = ChainBuf<(8 * T > 64 ? 8 * T : 64), 4 * T>;
 
-template <int KB, int VB>
-__global__ void __launch_bounds__(RBLOCK, 3) k_ins_p4(TableView t, const uint8_t* __restrict__ keys,
+#ifndef FM_P4_MIN_BLOCKS
+#define FM_P4_MIN_BLOCKS 2  // resident blocks per SM the long-walk pass is compiled for (no spills at 2)
+#endif
+template <int KB, int VB, int T>
+__global__ void __launch_bounds__(RBLOCK, FM_P4_MIN_BLOCKS) k_ins_p4(TableView t, const uint8_t* __restrict__ keys,
                                                       const uint8_t* __restrict__ vals, uint32_t r, OpScratch sc,
                                                       Ctl* ctl) {
-    constexpr int NT = RBLOCK / P4_T;
-    __shared__ TileChain s_chain[NT];
+    constexpr int NT = RBLOCK / T;
+    __shared__ P4Chain<T> s_chain[NT];
     __shared__ uint32_t s_tmp[RBLOCK / 32];
     const uint32_t n = *(volatile const uint32_t*)&ctl->nlong[r & 1];
     if (n == 0) return;  // block-uniform
-    const Tile<P4_T> tl;
-    const uint32_t ti = threadIdx.x / P4_T;
+    const Tile<T> tl;
+    const uint32_t ti = threadIdx.x / T;
     const uint32_t ntiles = gridDim.x * NT;
     ExecAcc a;
     // uniform trip count per warp (all tiles of a warp loop together)
@@ -1176,8 +1220,8 @@ __global__ void __launch_bounds__(RBLOCK, 3) k_ins_p4(TableView t, const uint8_t
             const uint32_t j = sc.long_list[i];
             RegKey<KB> key;
             key.load(keys + (uint64_t)j * KB, KB);
-            if (t.mask >= 4 * P4_T - 1) {
-                if (exec_tile<KB, VB, P4_T>(t, key, vals, j, tl, s_chain[ti], a) == 5) a.limit = true;
+            if (t.mask >= 4 * T - 1) {
+                if (exec_tile<KB, VB, T, P4Chain<T>>(t, key, vals, j, tl, s_chain[ti], a) == 5) a.limit = true;
             } else {
                 if (tl.lane == 0) a.claimed += exec_insert_key<KB, VB>(t, key, vals + (uint64_t)j * VB, a);
             }
@@ -1186,6 +1230,19 @@ __global__ void __launch_bounds__(RBLOCK, 3) k_ins_p4(TableView t, const uint8_t
     }
     block_add_count(ctl, a.claimed, s_tmp);
     publish_rare(ctl, a.maxd, a.tomb, a.limit);
+}
+
+// Lanes per insert of the long-walk pass: 32, 16 or 8 (environment variable
+// FLASHMAP_P4_LANES, read once; default 32, the fastest measured on B200 at
+// load 0.8: 8 and 16 lanes share warp instructions between inserts but walk
+// more windows and move fewer records per round trip).
+int p4_lanes() {
+    static int lanes = [] {
+        const char* e = getenv("FLASHMAP_P4_LANES");
+        const int v = e ? atoi(e) : 32;
+        return (v == 8 || v == 16 || v == 32) ? v : 32;
+    }();
+    return lanes;
 }
 
 // ---- single-block tails ----------------------------------------------------
@@ -1586,7 +1643,10 @@ void rounds_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, 
         }
         if constexpr (KB != 0 && VB != 0) {
             KtScope kt(KC_INS_LONG, s);
-            k_ins_p4<KB, VB><<<g, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
+            const int l = p4_lanes();
+            if (l == 8) k_ins_p4<KB, VB, 8><<<g, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
+            else if (l == 16) k_ins_p4<KB, VB, 16><<<g, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
+            else k_ins_p4<KB, VB, 32><<<g, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
         }
     }
     count_launches((KB != 0 && VB != 0 ? 4 : 3) * nrounds);

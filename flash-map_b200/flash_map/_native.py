@@ -13,7 +13,8 @@ import threading
 from .errors import CudaInit
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_DIR, "libflashmap_b200.so")
+# The in-tree build; FLASHMAP_B200_LIB names another build of the same ABI.
+LIB_PATH = os.environ.get("FLASHMAP_B200_LIB") or os.path.join(PKG_DIR, "libflashmap_b200.so")
 
 # Every exported symbol of include/flashmap_b200.h.
 EXPORTS = (
