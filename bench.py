@@ -263,6 +263,18 @@ def gpu_inputs(torch, dev, w, seed=3):
     return keys, vals, q, rem
 
 
+def max_over_ranks(value, dist, device):
+    """The largest of every rank's value (all ranks call it; identity without
+    a process group)."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 INSERT_KERNELS = ("k_ins_p1", "k_ins_p2", "k_ins_p3", "k_ins_p4", "k_ins_tail", "k_ins_serial")
 REMOVE_KERNELS = ("k_rem_p1", "k_rem_p2", "k_rem_p3", "k_rem_tail")
 
@@ -392,11 +404,7 @@ class DeviceRun:
         for _ in range(n):
             step_host()
         torch.cuda.synchronize()
-        e2e_s = (time.perf_counter() - t0) / n
-        if dist is not None:
-            t = torch.tensor([e2e_s], device=self.q.device)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = max_over_ranks((time.perf_counter() - t0) / n, dist, self.q.device)
         calls = (w.pairs + CALL - 1) // CALL
         # the link these copies cross: pinned 256 MB copies each way
         hb = torch.empty(1 << 28, dtype=torch.uint8).pin_memory()
@@ -689,6 +697,7 @@ def main():
     ap.add_argument("--no-as-written", action="store_true", help="skip the load-0.477 variant")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form workload")
     ap.add_argument("--no-served", action="store_true", help="skip the served-form workload")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default lookup kernel configuration")
     ap.add_argument("--nvtx", action="store_true",
                     help="mark one insert call and the bulk_get of the kernel-timing step with NVTX ranges")
     ap.add_argument("--scale", type=int, default=1,
@@ -725,6 +734,8 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    if not args.no_autotune:
+        _native.autotune(local)  # lookup kernel configuration per record shape and load
     stream = torch.cuda.current_stream(dev)
     run = DeviceRun(torch, F, dev, stream, main_w, local)
     with Clocks(local) as clk:  # sampled from the warm-up on, through the timed steps
@@ -733,11 +744,7 @@ def main():
         torch.cuda.synchronize()
         run.check()  # correctness guard on the timed workload (not a parity test)
         t = run.timed(args.steps, barrier, _native)
-    total_ms = t["total_ms"]
-    if dist is not None:
-        tt = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = max_over_ranks(t["total_ms"], dist, dev)
     ms_step = total_ms / args.steps
     value = main_w.ops * world / (ms_step / 1e3) / 1e6
     kt = run.kernel_pass(args.nvtx)
@@ -750,6 +757,8 @@ def main():
         "config": dict(main_w.desc(), parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
         "ops": run.ops(t),
         "gpu_launches": int(t["launches"]),
+        "lookup_config": {"lanes_per_query_and_blocks_per_sm": _native.tuned_get_config(KB, VB, 0.8),
+                          "autotuned": not args.no_autotune},
         "kernels": kernel_summary(kt, main_w),
     }
     if e2e:
@@ -775,7 +784,6 @@ def main():
         del alt
 
     if not args.no_batched:
-        _native.autotune(local, "/tmp/fm_autotune.txt")
         line["batched"] = batched_leg(torch, F, _native, dev, max(1, min(args.steps, 3)), 1, args.scale)
         line["batched"]["autotuned_get"] = {"u64": _native.tuned_get_config(8, 8, 0.7),
                                             "account": _native.tuned_get_config(KB, VB, 0.7)}
