@@ -28,7 +28,10 @@ __device__ __forceinline__ uint64_t home_of(const TableView& t, const uint8_t* k
     return key.hash(ksz, t.hash_mode) & t.mask;
 }
 
-// Phase 1 for op j: probe, then mark every possible target.
+// Phase 1 for op j: probe, then mark every possible target.  With capacity
+// >= 8 the metadata is read in aligned 8-slot windows (two 16-byte loads, one
+// 32-byte sector) and scanned in registers; key compares happen only where
+// the stored distance equals the probe depth.
 template <int KB>
 __device__ __forceinline__ void scan_op(const TableView& t, const uint8_t* keys, uint32_t j, uint64_t dmax,
                                         const OpScratch& sc) {
@@ -37,45 +40,114 @@ __device__ __forceinline__ void scan_op(const TableView& t, const uint8_t* keys,
     RegKey<KB> key;
     const uint64_t h = home_of<KB>(t, keys, j, key);
     uint64_t tp = NONE64;  // probe depth of the current target
-    uint64_t p = 0;
+    uint64_t p = 0;        // probe depth where the probe stopped
     bool empty_hit = false;
-    for (; p <= mask; ++p) {
-        const uint64_t s = (h + p) & mask;
-        const uint32_t f = t.flags[s];
-        const uint32_t st = st_of(f);
-        if (st == ST_EMPTY) {
-            empty_hit = true;
-            break;
-        }
-        if (st == ST_OCC) {
-            if (p > dist_of(f)) break;  // Robin Hood exit (rayon_cpu.rs:298-302)
-            if (dist_matches(f, p) && key.eq(t.keys + s * ksz, ksz)) {
-                tp = p;
-                break;
-            }
-        }
-    }
-    uint64_t lim = (tp != NONE64 ? tp : 0) + dmax;
-    if (lim > mask) lim = mask;
     uint32_t npt = 0;
-    uint64_t wend;
+    uint64_t wend = NONE64;
     auto mark = [&](uint64_t q) {
         atomicMin(&t.seg_min[(h + q) & mask], j);
         if (npt < PT_MAX) sc.op_pt[(uint64_t)j * PT_MAX + npt] = (uint32_t)q;
         ++npt;
     };
-    if (empty_hit) {
-        wend = p == 0 ? NONE64 : min(p - 1, lim);  // home slot EMPTY: nothing to watch
+    if (mask >= 7) {
+        // 1. the probe
+        bool stop = false;
+        for (uint64_t wb = h & ~7ull; !stop; wb += 8) {
+            const uint4* fp = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
+            const uint4 a = fp[0], b = fp[1];
+            const uint32_t f8[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int l = 0; l < 8; l++) {
+                if (stop || wb + l < h) continue;
+                const uint64_t q = wb + l - h;
+                if (q > mask) {  // the whole table probed
+                    p = q;
+                    stop = true;
+                    continue;
+                }
+                const uint32_t f = f8[l];
+                const uint32_t st = st_of(f);
+                if (st == ST_EMPTY) {
+                    empty_hit = true;
+                    p = q;
+                    stop = true;
+                } else if (st == ST_OCC) {
+                    if (q > dist_of(f)) {  // Robin Hood exit (rayon_cpu.rs:298-302)
+                        p = q;
+                        stop = true;
+                    } else if (dist_matches(f, q) && key.eq(t.keys + ((h + q) & mask) * ksz, ksz)) {
+                        tp = q;
+                        p = q;
+                        stop = true;
+                    }
+                }
+            }
+        }
+        uint64_t lim = (tp != NONE64 ? tp : 0) + dmax;
+        if (lim > mask) lim = mask;
+        if (empty_hit) {
+            wend = p == 0 ? NONE64 : min(p - 1, lim);  // home slot EMPTY: nothing to watch
+        } else {
+            if (tp != NONE64) mark(tp);
+            wend = min(p, lim);
+            // 2. later copies of the key up to the bound (windows again)
+            const uint64_t q0 = (tp != NONE64 ? tp : p) + 1;
+            bool done = q0 > lim;
+            for (uint64_t wb = (h + q0) & ~7ull; !done; wb += 8) {
+                const uint4* fp = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
+                const uint4 a = fp[0], b = fp[1];
+                const uint32_t f8[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+                for (int l = 0; l < 8; l++) {
+                    if (done || wb + l < h + q0) continue;
+                    const uint64_t q = wb + l - h;
+                    if (q > lim) {
+                        done = true;
+                        continue;
+                    }
+                    const uint32_t f = f8[l];
+                    const uint32_t st = st_of(f);
+                    if (st == ST_EMPTY) {
+                        done = true;
+                        continue;
+                    }
+                    wend = q;
+                    if (st == ST_OCC && dist_matches(f, q) && key.eq(t.keys + ((h + q) & mask) * ksz, ksz)) mark(q);
+                }
+            }
+        }
     } else {
-        if (tp != NONE64) mark(tp);
-        wend = min(p, lim);
-        for (uint64_t q = (tp != NONE64 ? tp : p) + 1; q <= lim; ++q) {
-            const uint64_t s = (h + q) & mask;
+        for (; p <= mask; ++p) {
+            const uint64_t s = (h + p) & mask;
             const uint32_t f = t.flags[s];
             const uint32_t st = st_of(f);
-            if (st == ST_EMPTY) break;
-            wend = q;
-            if (st == ST_OCC && dist_matches(f, q) && key.eq(t.keys + s * ksz, ksz)) mark(q);
+            if (st == ST_EMPTY) {
+                empty_hit = true;
+                break;
+            }
+            if (st == ST_OCC) {
+                if (p > dist_of(f)) break;  // Robin Hood exit (rayon_cpu.rs:298-302)
+                if (dist_matches(f, p) && key.eq(t.keys + s * ksz, ksz)) {
+                    tp = p;
+                    break;
+                }
+            }
+        }
+        uint64_t lim = (tp != NONE64 ? tp : 0) + dmax;
+        if (lim > mask) lim = mask;
+        if (empty_hit) {
+            wend = p == 0 ? NONE64 : min(p - 1, lim);  // home slot EMPTY: nothing to watch
+        } else {
+            if (tp != NONE64) mark(tp);
+            wend = min(p, lim);
+            for (uint64_t q = (tp != NONE64 ? tp : p) + 1; q <= lim; ++q) {
+                const uint64_t s = (h + q) & mask;
+                const uint32_t f = t.flags[s];
+                const uint32_t st = st_of(f);
+                if (st == ST_EMPTY) break;
+                wend = q;
+                if (st == ST_OCC && dist_matches(f, q) && key.eq(t.keys + s * ksz, ksz)) mark(q);
+            }
         }
     }
     sc.op_slot[j] = tp != NONE64 ? ((h + tp) & mask) : NONE64;
@@ -83,7 +155,8 @@ __device__ __forceinline__ void scan_op(const TableView& t, const uint8_t* keys,
     sc.op_flag[j] = (uint8_t)min(npt, 255u);
 }
 
-// Phase 2 for op j: run unless an earlier op marked its window.
+// Phase 2 for op j: run unless an earlier op marked its window (read as
+// aligned 4-slot groups of marks with capacity >= 4).
 template <int KB>
 __device__ __forceinline__ bool check_op(const TableView& t, const uint8_t* keys, uint32_t j, const OpScratch& sc,
                                          uint32_t& removed) {
@@ -92,8 +165,19 @@ __device__ __forceinline__ bool check_op(const TableView& t, const uint8_t* keys
     if (wend != IDLE) {
         RegKey<KB> key;
         const uint64_t h = home_of<KB>(t, keys, j, key);
-        for (uint64_t q = 0; q <= wend; ++q)
-            if (t.seg_min[(h + q) & mask] < j) return false;
+        if (mask >= 3) {
+            const uint64_t last = h + wend;
+            for (uint64_t wb = h & ~3ull; wb <= last; wb += 4) {
+                const uint4 m = *reinterpret_cast<const uint4*>(t.seg_min + (wb & mask));
+                const uint32_t m4[4] = {m.x, m.y, m.z, m.w};
+#pragma unroll
+                for (int l = 0; l < 4; l++)
+                    if (wb + l >= h && wb + l <= last && m4[l] < j) return false;
+            }
+        } else {
+            for (uint64_t q = 0; q <= wend; ++q)
+                if (t.seg_min[(h + q) & mask] < j) return false;
+        }
     }
     const uint64_t ts = sc.op_slot[j];
     if (ts != NONE64) {
