@@ -1214,12 +1214,23 @@ __global__ void __launch_bounds__(RBLOCK, FM_P4_MIN_BLOCKS) k_ins_p4(TableView t
     ExecAcc a;
     // uniform trip count per warp (all tiles of a warp loop together)
     const uint32_t iters = (n + ntiles - 1) / ntiles;
+    const uint32_t first = blockIdx.x * NT + ti;
+    // two-deep prefetch: the next op's key and the op after's list entry
+    // load while this op walks (their round trips overlap the walk)
+    uint32_t jn = first < n ? sc.long_list[first] : 0u;
+    RegKey<KB> kn;
+    if (first < n) kn.load(keys + (uint64_t)jn * KB, KB);
+    uint32_t jnn = first + ntiles < n ? sc.long_list[first + ntiles] : 0u;
     for (uint32_t it = 0; it < iters; it++) {
-        const uint32_t i = blockIdx.x * NT + ti + it * ntiles;
+        const uint32_t i = first + it * ntiles;
+        const uint32_t j = jn;
+        const RegKey<KB> key = kn;
+        if (i + ntiles < n) {
+            jn = jnn;
+            kn.load(keys + (uint64_t)jn * KB, KB);
+            if (i + 2 * ntiles < n) jnn = sc.long_list[i + 2 * ntiles];
+        }
         if (i < n) {
-            const uint32_t j = sc.long_list[i];
-            RegKey<KB> key;
-            key.load(keys + (uint64_t)j * KB, KB);
             if (t.mask >= 4 * T - 1) {
                 if (exec_tile<KB, VB, T, P4Chain<T>>(t, key, vals, j, tl, s_chain[ti], a) == 5) a.limit = true;
             } else {
