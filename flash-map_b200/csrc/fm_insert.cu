@@ -1639,6 +1639,9 @@ void rounds_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, 
     // one op per thread: far more ops in flight than one per tile, which is
     // what chains of dependent random reads need
     const unsigned g = grid_for(grid_ops, 8);
+    // the long-walk pass: a warp per walk that a pending op may defer, up to
+    // the blocks that fit on the GPU at once
+    const unsigned g4 = grid_for((uint64_t)grid_ops * 32, FM_P4_MIN_BLOCKS);
     for (uint32_t r = r0; r < r0 + nrounds; r++) {
         {
             KtScope kt(KC_INS_FIND, s);
@@ -1655,9 +1658,9 @@ void rounds_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, 
         if constexpr (KB != 0 && VB != 0) {
             KtScope kt(KC_INS_LONG, s);
             const int l = p4_lanes();
-            if (l == 8) k_ins_p4<KB, VB, 8><<<g, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
-            else if (l == 16) k_ins_p4<KB, VB, 16><<<g, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
-            else k_ins_p4<KB, VB, 32><<<g, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
+            if (l == 8) k_ins_p4<KB, VB, 8><<<g4, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
+            else if (l == 16) k_ins_p4<KB, VB, 16><<<g4, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
+            else k_ins_p4<KB, VB, 32><<<g4, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
         }
     }
     count_launches((KB != 0 && VB != 0 ? 4 : 3) * nrounds);
