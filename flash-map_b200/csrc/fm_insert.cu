@@ -277,8 +277,14 @@ __device__ __forceinline__ void move_entry(const TableView& t, const uint8_t* ks
     }
 }
 
-constexpr int TH_MAXK = 3;  // evictions per op on the thread path
-constexpr int TH_MAXC = 2;  // possible updates per op on the thread path
+#ifndef FM_TH_MAXK
+#define FM_TH_MAXK 3
+#endif
+#ifndef FM_TH_MAXC
+#define FM_TH_MAXC 2
+#endif
+constexpr int TH_MAXK = FM_TH_MAXK;  // evictions per op on the thread path
+constexpr int TH_MAXC = FM_TH_MAXC;  // possible updates per op on the thread path
 
 // The sequential insert of one key by one thread, for the common short walk
 // (capacity >= 8, rounds that are not serial, so the walk ends at or before
