@@ -283,7 +283,7 @@ REMOVE_KERNELS = ("k_rem_p1", "k_rem_p2", "k_rem_p3", "k_rem_tail")
 # the same load factor and call size (the traffic summary under
 # profiles/ gives the command and the per-kernel figures); traffic grows with
 # the ops processed.
-NCU_TRAFFIC_PER_OP = {"insert": 1238.7, "get": 330.3, "remove": 840.7}
+NCU_TRAFFIC_PER_OP = {"insert": 1274.3, "get": 333.5, "remove": 850.5}
 
 
 class DeviceRun:
@@ -434,6 +434,14 @@ def kernel_summary(kt, w):
     total = sum(v[0] for v in kt.values()) or 1.0
     return {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / total, 4)}
             for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}
+
+
+def get_kernel_label():
+    from flash_map import _native
+
+    lanes, bps = _native.tuned_get_config(KB, VB, 0.8)
+    name = "k_get_thread<32,128>" if lanes == 1 else f"k_get<32,128,{lanes}>"
+    return f"{name} ({lanes} lane(s) per query, {bps} blocks per SM; one launch of all gets)"
 
 
 def roofline_for(kt, names, nops, bpo, peak, kind, label, traffic_per_op):
@@ -800,7 +808,7 @@ def main():
             "bulk_insert kernel set (k_ins_p1..p4 per round + k_ins_tail, every call of the step; the step's "
             "largest device-time share)", NCU_TRAFFIC_PER_OP["insert"])
         line["roofline_get"] = roofline_for(
-            kt, ("k_get",), main_w.gets, bpo["get"], peak, kind, "k_get_thread<32,128> (one launch of all gets)",
+            kt, ("k_get",), main_w.gets, bpo["get"], peak, kind, get_kernel_label(),
             NCU_TRAFFIC_PER_OP["get"])
         line["roofline_remove"] = roofline_for(
             kt, REMOVE_KERNELS, main_w.removes, bpo["remove"], peak, kind, "bulk_remove kernel set",
