@@ -9,8 +9,9 @@ reach a :class:`FlashMapServer` in arrival order.  Two threads run them:
 * the executor takes every admitted request that is ready, runs them as one
   :class:`~flash_map.FlashMapBatch` on the compute stream (arrival-order
   sequential semantics: each request's result is the one it would get alone
-  at its turn), downloads the get results, stamps completion times and
-  releases the budget.
+  at its turn) or, when only one is ready, as the plain device-pointer call,
+  downloads the get results, stamps completion times and releases the
+  budget.
 
 So requests that arrive while a batch is on the GPU are admitted as memory
 frees up, their uploads overlap the running batch, and they join the next
@@ -31,7 +32,7 @@ from typing import List, Optional
 import numpy as np
 
 from .batch import GET, INSERT, REMOVE, BatchOp, FlashMapBatch
-from .errors import TableFull
+from .errors import FM_ERR_PROBE_LIMIT, FM_ERR_TABLE_FULL, TableFull
 from .map import FlashMap
 
 
@@ -143,11 +144,15 @@ class FlashMapServer:
                 ready.clear()
             for r in group:
                 self.stream.wait_event(r._dev[4])
-            ops = [BatchOp(r.kind, self.t, r.n, r._dev[0], r._dev[1], r._dev[2], r._dev[3]) for r in group]
-            b = FlashMapBatch(ops)
-            b.run(self.stream)
-            res = b.wait()
-            b.close()
+            if len(group) == 1:
+                # a lone request: the plain device call, without batch set-up
+                res = [self._run_one(group[0])]
+            else:
+                ops = [BatchOp(r.kind, self.t, r.n, r._dev[0], r._dev[1], r._dev[2], r._dev[3]) for r in group]
+                b = FlashMapBatch(ops)
+                b.run(self.stream)
+                res = b.wait()
+                b.close()
             # results home: get outputs downloaded on the compute stream
             outs = []
             with torch.cuda.stream(self.stream):
@@ -179,6 +184,29 @@ class FlashMapServer:
             end = time.perf_counter()
         th.join()
         return end - t0
+
+
+    def _run_one(self, r: Request):
+        """A lone request: the device-pointer call on the compute stream, with
+        TableFull and the probe limit reported as the op's status, as a batch
+        reports them; any other failure raises."""
+        import ctypes as C
+
+        from .map import _dev_ptr
+
+        dk, dv, ov, of = r._dev[:4]
+        L, h, s = self.t._L, self.t._h, self.stream.cuda_stream
+        out = C.c_uint64(0)
+        if r.kind == GET:
+            rc = L.fm_bulk_get_device(h, _dev_ptr(dk), r.n, _dev_ptr(ov), _dev_ptr(of), s)
+        elif r.kind == INSERT:
+            rc = L.fm_bulk_insert_device(h, _dev_ptr(dk), _dev_ptr(dv), r.n, C.byref(out), s)
+        else:
+            rc = L.fm_bulk_remove_device(h, _dev_ptr(dk), r.n, C.byref(out), s)
+        if rc in (FM_ERR_TABLE_FULL, FM_ERR_PROBE_LIMIT):
+            return 0, rc
+        self.t._check(rc)
+        return int(out.value), 0
 
 
 class PlainServer:

@@ -200,3 +200,40 @@ def test_batch_ops_larger_than_any_earlier_call():
         gf, gk, gv = t["g"].snapshot()
         of_, ok, ov = t["o"].snapshot()
         assert np.array_equal(gf, of_) and np.array_equal(gk, ok) and np.array_equal(gv, ov)
+
+
+def test_batch_run_time_record_sizes():
+    """Record sizes without a compiled specialisation (12-byte keys, 20-byte
+    values) run the grouped kernels' generic path; results still equal the
+    queue-order replay."""
+    import flash_map as F
+
+    rng = np.random.default_rng(12)
+    tables = []
+    for cap in (1 << 12, 1 << 13):
+        tables.append({"g": gpu_map(cap, 12, 20), "o": OracleAdapter(cap, 12, 20), "ks": 12, "vs": 20, "known": []})
+    queue = []
+    for i in range(24):
+        ti = i % 2
+        t = tables[ti]
+        kind = [F.batch.INSERT, F.batch.GET, F.batch.REMOVE, F.batch.INSERT][i % 4]
+        n = int(rng.integers(50, 900))
+        if kind == F.batch.INSERT:
+            k = _keys(rng, n, 12)
+            t["known"].append(k)
+            queue.append((ti, kind, k, _keys(rng, n, 20)))
+        else:
+            pool = np.concatenate(t["known"]) if t["known"] else _keys(rng, 8, 12)
+            queue.append((ti, kind, pool[rng.integers(0, len(pool), n)], None))
+    for graph in (False,):
+        g_res, g_out = run_batch(tables, queue, graph)
+        o_res, o_out = oracle_replay(tables, queue)
+        assert g_res == o_res
+        for i, (ti, kind, k, v) in enumerate(queue):
+            if kind == F.batch.GET:
+                assert np.array_equal(g_out[i][1].astype(bool), o_out[i][1])
+                assert np.array_equal(g_out[i][0], o_out[i][0])
+    for t in tables:
+        gf, gk, gv = t["g"].snapshot()
+        of_, ok, ov = t["o"].snapshot()
+        assert np.array_equal(gf, of_) and np.array_equal(gk, ok) and np.array_equal(gv, ov)
