@@ -211,10 +211,11 @@ struct TimerScope {
 
 int ensure_scratch(fm_table* t, uint64_t n) {
     if (t->sc.cap_ops >= n) return FM_OK;
-    // pend[0], pend[1] (u32) | op_slot (u64) | op_word (u32) | op_flag (u8) | op_pt (PT_MAX u32)
+    // pend[0], pend[1] (u32) | op_slot (u64) | op_word (u32) | op_flag (u8) | op_pt (PT_MAX u32) |
+    // long_list (u32) per op, then the component buffer (per table)
     const uint64_t per_op = 4 + 4 + 8 + 4 + 1 + 4 * fm::PT_MAX + 4;
     const uint64_t want = n + n / 4 + 1024;
-    const size_t bytes = (size_t)(want * per_op + 7 * 256);
+    const size_t bytes = (size_t)(want * per_op + 8 * 256 + fm::cmp_bytes(t->mask));
     if (t->sc_base) cudaFree(t->sc_base);
     t->sc_base = nullptr;
     t->sc = OpScratch{};
@@ -233,6 +234,7 @@ int ensure_scratch(fm_table* t, uint64_t n) {
     t->sc.op_pt = (uint32_t*)carve(want * 4 * fm::PT_MAX);
     t->sc.op_flag = carve(want);
     t->sc.long_list = (uint32_t*)carve(want * 4);
+    t->sc.comp = carve(fm::cmp_bytes(t->mask));
     t->sc.cap_ops = want;
     t->sc_bytes = bytes;
     // op_word doubles as the insert inflow bound: idle value 0xFFFFFFFF.
@@ -287,7 +289,7 @@ int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t
             uint32_t now = t->h_ctl->npend[r & 1];
             if (insert && now > 0 && t->h_ctl->serial[(r - 1) & 1]) {
                 // the table is full: the remaining ops run one at a time in index order
-                e = fm::launch_ins_serial(v, sh, kk, vv, m, r, t->sc, t->d_ctl, s);
+                e = fm::launch_ins_comp(v, sh, kk, vv, m, r, now, t->sc, t->d_ctl, s);
                 if (e == cudaSuccess) e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(s);
                 if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "serial insert", e);
@@ -299,8 +301,8 @@ int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t
             if (insert && (uint64_t)now * 8 > (uint64_t)left * 7) {
                 // under 1/8 of the ops per pass (ops crowded onto few free
                 // slots, a near-full table): the rest one at a time in index
-                // order, which a round boundary allows
-                e = fm::launch_ins_serial(v, sh, kk, vv, m, r, t->sc, t->d_ctl, s);
+                // order within each component, which a round boundary allows
+                e = fm::launch_ins_comp(v, sh, kk, vv, m, r, now, t->sc, t->d_ctl, s);
                 if (e == cudaSuccess) e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(s);
                 if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "serial insert", e);
@@ -1060,6 +1062,7 @@ struct fm_batch {
         fm::GetCfg cfg;
         uint32_t rounds = 0;            // mutating: grid rounds the last eager run needed (0: none yet)
         bool serial = false;            // inserts: the eager run finished them one at a time
+        std::vector<uint32_t> comp;     // ... of these, the members run as components (more than TAIL_MAX left)
     };
     std::vector<Group> groups;          // in execution order
     uint32_t waves = 0;
@@ -1070,7 +1073,7 @@ struct fm_batch {
     unsigned long long* d_res = nullptr;   // per op
     int* d_status = nullptr;               // per op
     uint8_t* h_io = nullptr;               // pinned: len[tables], res[ops], status[ops]
-    uint32_t* d_pend = nullptr;            // largest pending count (eager runs)
+    uint32_t* d_pend = nullptr;            // pending counts (eager runs): GROUP_MAX + 1 words
     uint32_t* h_pend = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1201,12 +1204,29 @@ int batch_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
                 prev = *b->h_pend;
             }
             g.rounds = r;
-            if (e == cudaSuccess && g.serial) e = L(g.shape, d, n, g.total, fm::GRP_SERIAL, r, 0, s);
+            g.comp.clear();
+            if (e == cudaSuccess && g.serial) {
+                // members with many ops left run as components (the rest in
+                // the block-per-op serial launch)
+                e = fm::launch_grp_pending_each(d, n, r, b->d_pend, s);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_pend, b->d_pend, n * 4, cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                for (uint32_t k = 0; e == cudaSuccess && k < n; k++)
+                    if (b->h_pend[k] > fm::TAIL_MAX) g.comp.push_back(k);
+            }
         } else {
             const uint32_t nr = g.rounds ? g.rounds : 3u;
             e = L(g.shape, d, n, g.total, fm::GRP_ROUNDS, 0, nr, s);
             r = nr;
-            if (e == cudaSuccess && g.serial) e = L(g.shape, d, n, g.total, fm::GRP_SERIAL, r, 0, s);
+        }
+        if (e == cudaSuccess && g.serial) {
+            const auto* hd = reinterpret_cast<const fm::GroupOp*>(b->h_desc + g.desc_off);
+            for (uint32_t k : g.comp) {
+                if (e != cudaSuccess) break;
+                const fm::GroupOp& o = hd[k];
+                e = fm::launch_ins_comp(o.t, g.shape, o.keys, o.vals, fm::CMP_N0_CTL, r, o.n, o.sc, o.ctl, s);
+            }
+            if (e == cudaSuccess) e = L(g.shape, d, n, g.total, fm::GRP_SERIAL, r, 0, s);
         }
         if (e == cudaSuccess) e = L(g.shape, d, n, g.total, fm::GRP_END, r, 0, s);
         if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch wave", e);
@@ -1295,8 +1315,9 @@ int fm_batch_create(const fm_op* ops, uint32_t nops, fm_batch** out) {
     DeviceGuard dg(b->device);
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t o_len = al(b->desc_bytes), o_res = o_len + al(b->tables.size() * 8), o_st = o_res + al(nops * 8),
-                 o_pend = o_st + al(nops * 4), dneed = o_pend + 256;
-    const size_t h_io = al(b->desc_bytes), h_pend = h_io + al(b->io_bytes()), hneed = h_pend + 256;
+                 o_pend = o_st + al(nops * 4), dneed = o_pend + al(4 * (fm::GROUP_MAX + 1));
+    const size_t h_io = al(b->desc_bytes), h_pend = h_io + al(b->io_bytes()),
+                 hneed = h_pend + al(4 * (fm::GROUP_MAX + 1));
     cudaError_t e = cudaSuccess;
     b->arena = arena_take(b->device, dneed, hneed, &e);
     if (e != cudaSuccess) {

@@ -979,13 +979,13 @@ struct SerialOut {
 
 constexpr int SERIAL_THREADS = 512;
 
-// One insert by a whole block of SERIAL_THREADS threads (compile-time sizes,
+// One insert by a whole block of W threads (compile-time sizes,
 // capacity >= 128): warp 0 walks the chain into the large buffer, then every
 // thread moves records (204 account-shape records per round trip) and writes
 // flags.  A chain longer than the buffer takes the chunked warp path; a walk
 // that finds no free slot within a pass (overfull table) the scalar walk.
 // Block-uniform call.
-template <int KB, int VB>
+template <int KB, int VB, int W = SERIAL_THREADS>
 __device__ void exec_serial_block(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t j,
                                   SerialChain& s, SerialOut& so, ExecAcc& a) {
     RegKey<KB> key;
@@ -1021,7 +1021,7 @@ __device__ void exec_serial_block(const TableView& t, const uint8_t* keys, const
     }
     const uint32_t k = so.k;
     const int hi = kind == 3 ? (int)k - 1 : (int)k;
-    const BlockCrew<SERIAL_THREADS> crew;
+    const BlockCrew<W> crew;
     tile_moves<KB, VB, 4>(t, key, vin, s, 0, hi, 0, k, kind, so.end_slot, so.src_base, crew);
     uint32_t md = 0;
     for (uint32_t m = threadIdx.x; m < k; m += blockDim.x) {
@@ -1036,6 +1036,46 @@ __device__ void exec_serial_block(const TableView& t, const uint8_t* keys, const
     }
     a.maxd = max(a.maxd, md);
     __syncthreads();  // the next op reads these writes
+}
+
+// Applies the c ops of s_list in that order on this block, each as
+// serial_process (below) describes.  Block-uniform call; W = blockDim.x
+// when s_big is given.
+template <int KB, int VB, int W>
+__device__ void serial_apply(const TableView& t, const uint8_t* keys, const uint8_t* vals, const uint32_t* s_list,
+                             uint32_t c, const OpScratch& sc, ExecAcc& a, TileChain* s_chain, SerialChain* s_big,
+                             SerialOut* s_out) {
+    const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
+    const uint32_t vsz = VB ? (uint32_t)VB : t.vsz;
+    if constexpr (KB == 0 || VB == 0) {
+        if (threadIdx.x == 0) {
+            for (uint32_t k = 0; k < c; k++) {
+                const uint32_t jj = s_list[k];
+                sc.op_flag[jj] = 0;
+                a.claimed += exec_insert_generic(t, keys + (uint64_t)jj * ksz, vals + (uint64_t)jj * vsz, a);
+            }
+        }
+    } else if (s_big && t.mask >= 4 * 32 - 1) {
+        for (uint32_t k = 0; k < c; k++) {
+            const uint32_t jj = s_list[k];
+            if (threadIdx.x == 0) sc.op_flag[jj] = 0;
+            exec_serial_block<KB, VB, W>(t, keys, vals, jj, *s_big, *s_out, a);
+        }
+    } else {
+        if (threadIdx.x < 32) {
+            const Tile<32> tl;
+            for (uint32_t k = 0; k < c; k++) {
+                const uint32_t jj = s_list[k];
+                if (tl.lane == 0) sc.op_flag[jj] = 0;
+                RegKey<KB> key;
+                key.load(keys + (uint64_t)jj * KB, KB);
+                int kind = 5;
+                if (s_chain && t.mask >= 4 * 32 - 1) kind = exec_tile<KB, VB, 32>(t, key, vals, jj, tl, *s_chain, a);
+                if (kind == 5 && tl.lane == 0) a.claimed += exec_insert_key<KB, VB>(t, key, vals + (uint64_t)jj * VB, a);
+                tl.sync();  // the next op reads this one's writes
+            }
+        }
+    }
 }
 
 // Applies the ops of `list` (n ops; nullptr = the identity over n ops) one at
@@ -1055,43 +1095,13 @@ __device__ void serial_process(const TableView& t, const uint8_t* keys, const ui
                                uint32_t n, uint32_t n0, const OpScratch& sc, ExecAcc& a, uint32_t* s_buf,
                                uint32_t* s_woff, TileChain* s_chain, SerialChain* s_big = nullptr,
                                SerialOut* s_out = nullptr) {
-    const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
-    const uint32_t vsz = VB ? (uint32_t)VB : t.vsz;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sc.op_flag[list ? list[i] : i] = 3;
     __syncthreads();
     for (uint32_t base = 0; base < n0; base += blockDim.x) {
         const uint32_t j = base + threadIdx.x;
         const bool take = j < n0 && sc.op_flag[j] == 3;
         const uint32_t c = block_compact(j, take, s_buf, s_woff);
-        if constexpr (KB == 0 || VB == 0) {
-            if (threadIdx.x == 0) {
-                for (uint32_t k = 0; k < c; k++) {
-                    const uint32_t jj = s_buf[k];
-                    sc.op_flag[jj] = 0;
-                    a.claimed += exec_insert_generic(t, keys + (uint64_t)jj * ksz, vals + (uint64_t)jj * vsz, a);
-                }
-            }
-        } else if (s_big && t.mask >= 4 * 32 - 1) {
-            for (uint32_t k = 0; k < c; k++) {
-                const uint32_t jj = s_buf[k];
-                if (threadIdx.x == 0) sc.op_flag[jj] = 0;
-                exec_serial_block<KB, VB>(t, keys, vals, jj, *s_big, *s_out, a);
-            }
-        } else {
-            if (threadIdx.x < 32) {
-                const Tile<32> tl;
-                for (uint32_t k = 0; k < c; k++) {
-                    const uint32_t jj = s_buf[k];
-                    if (tl.lane == 0) sc.op_flag[jj] = 0;
-                    RegKey<KB> key;
-                    key.load(keys + (uint64_t)jj * KB, KB);
-                    int kind = 5;
-                    if (s_chain && t.mask >= 4 * 32 - 1) kind = exec_tile<KB, VB, 32>(t, key, vals, jj, tl, *s_chain, a);
-                    if (kind == 5 && tl.lane == 0) a.claimed += exec_insert_key<KB, VB>(t, key, vals + (uint64_t)jj * VB, a);
-                    tl.sync();  // the next op reads this one's writes
-                }
-            }
-        }
+        serial_apply<KB, VB, SERIAL_THREADS>(t, keys, vals, s_buf, c, sc, a, s_chain, s_big, s_out);
         __syncthreads();
     }
 }
@@ -1436,6 +1446,437 @@ size_t serial_smem(K kernel, bool big) {
     return sizeof(SerialChain);
 }
 
+// ---- components: the one-at-a-time order spread over the GPU ---------------
+//
+// When rounds stall (ops crowded onto few free slots of a near-full table),
+// the remaining ops must run in index order -- but only ops that can reach
+// the same slots need that order.  An insert reads and writes only [home, F']
+// with F' the first free slot at or after its home when it runs, and fills
+// F' when its key is new.  With d(s) the pending ops whose first free slot is
+// s now, a carry walk over the table in slot order bounds the free slots they
+// fill: a free slot passes on c' = max(0, c + d(s) - 1) of the c ops that
+// arrive at it, an occupied slot passes c on.  A free slot with d(s) > 0 and
+// no arriving carry starts a component, which ends at the first free slot
+// that passes on 0.  A component's ops fill free slots within it only and read
+// nothing below their homes, so components touch disjoint slots and may run
+// at the same time.  Counting updates as demand only raises carries (merging
+// components), which keeps this true.  Each component's ops run in index
+// order on one block; components go to the resident blocks by a hash of
+// their start.
+//
+// The walk is a scan of the functions c -> max(a, c + b), which compose
+// associatively: per chunk of CMP_CHUNK slots (32 per thread), then one block
+// over the chunks.  The carry into slot 0 comes round the ring: with the
+// ring's composition (A, B) and B < 0 (fewer demanding ops than free slots)
+// it is A.  Otherwise (B >= 0, or an op with no free slot at all) every op
+// goes to block 0, which is the plain one-at-a-time order.
+constexpr int CMP_THREADS = 256;
+constexpr uint32_t CMP_PER_T = (uint32_t)CMP_CHUNK / CMP_THREADS;  // slots per thread
+constexpr long long CMP_NEG = -(1ll << 60);
+constexpr uint32_t CMP_UNK = 0xFFFFFFFEu;  // demand slot whose component starts in an earlier chunk
+constexpr uint32_t CMP_OPS_PER_T = 16;
+constexpr uint32_t CMP_OPS_PER_BLOCK = CMP_THREADS * CMP_OPS_PER_T;  // op indices per compaction block
+constexpr int CMP_EXEC_THREADS = 256;
+static_assert(CMP_PER_T == 32, "cmp_load reads 32 slots per thread");
+
+struct CFn {  // c -> max(a, c + b)
+    long long a, b;
+};
+__device__ __forceinline__ CFn cfn_id() { return CFn{CMP_NEG, 0}; }
+// f, then g
+__device__ __forceinline__ CFn cfn_then(const CFn& f, const CFn& g) {
+    return CFn{max(g.a, f.a + g.b), f.b + g.b};
+}
+__device__ __forceinline__ long long cfn_apply(const CFn& f, long long c) { return max(f.a, c + f.b); }
+
+struct CmpHdr {
+    uint32_t fallback;  // 1: every op to block 0
+    uint32_t np;        // ops in the ordered list
+};
+
+// The call's op count: the argument, or the grouped call's count in its
+// control block (CMP_N0_CTL).
+__device__ __forceinline__ uint32_t cmp_n0(uint32_t n0, const Ctl* ctl) {
+    return n0 != CMP_N0_CTL ? n0 : *(volatile const uint32_t*)&ctl->n0;
+}
+
+// The component buffer: header, then per chunk its function, the carry into
+// it, its last component start + 1 and the last start before it + 1 (0: none).
+struct CmpView {
+    CmpHdr* hdr;
+    CFn* fn;
+    long long* carry;
+    uint32_t* last;
+    uint32_t* prev;
+    uint32_t nch;
+    __device__ __forceinline__ CmpView(uint8_t* base, uint64_t mask) {
+        nch = (uint32_t)cmp_chunks(mask);
+        hdr = reinterpret_cast<CmpHdr*>(base);
+        fn = reinterpret_cast<CFn*>(base + 256);
+        carry = reinterpret_cast<long long*>(fn + nch);
+        last = reinterpret_cast<uint32_t*>(carry + nch);
+        prev = last + nch;
+    }
+};
+
+// Metadata and demand of the 32 slots from s0 (a multiple of 32); slots past
+// the table read as occupied.
+__device__ __forceinline__ void cmp_load(const TableView& t, uint64_t s0, uint32_t (&fl)[CMP_PER_T],
+                                         uint32_t (&dm)[CMP_PER_T]) {
+    if (s0 + CMP_PER_T - 1 <= t.mask) {
+        const uint4* pf = reinterpret_cast<const uint4*>(t.flags + s0);
+        const uint4* pc = reinterpret_cast<const uint4*>(t.seg_cnt + s0);
+#pragma unroll
+        for (int q = 0; q < (int)CMP_PER_T / 4; q++) {
+            const uint4 f = pf[q], c = pc[q];
+            fl[4 * q] = f.x, fl[4 * q + 1] = f.y, fl[4 * q + 2] = f.z, fl[4 * q + 3] = f.w;
+            dm[4 * q] = c.x, dm[4 * q + 1] = c.y, dm[4 * q + 2] = c.z, dm[4 * q + 3] = c.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < (int)CMP_PER_T; i++) {
+            const uint64_t s = s0 + i;
+            fl[i] = s <= t.mask ? t.flags[s] : ST_OCC;
+            dm[i] = s <= t.mask ? t.seg_cnt[s] : 0u;
+        }
+    }
+}
+
+__device__ __forceinline__ CFn cmp_thread_fn(const uint32_t (&fl)[CMP_PER_T], const uint32_t (&dm)[CMP_PER_T]) {
+    CFn f = cfn_id();
+#pragma unroll
+    for (int i = 0; i < (int)CMP_PER_T; i++)
+        if (is_free(fl[i])) f = cfn_then(f, CFn{0, (long long)dm[i] - 1});
+    return f;
+}
+
+// Exclusive in-order scan of one function per thread over the block; `total`
+// gets the block's composition.  s_w: 32 entries.
+__device__ CFn cmp_block_scan(CFn f, CFn* s_w, CFn& total) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    CFn inc = f;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        CFn g;
+        g.a = __shfl_up_sync(0xFFFFFFFFu, inc.a, off);
+        g.b = __shfl_up_sync(0xFFFFFFFFu, inc.b, off);
+        if ((int)lane >= off) inc = cfn_then(g, inc);
+    }
+    if (lane == 31) s_w[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        CFn v = lane < nw ? s_w[lane] : cfn_id();
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            CFn g;
+            g.a = __shfl_up_sync(0xFFFFFFFFu, v.a, off);
+            g.b = __shfl_up_sync(0xFFFFFFFFu, v.b, off);
+            if ((int)lane >= off) v = cfn_then(g, v);
+        }
+        s_w[lane] = v;  // inclusive over the warps
+    }
+    __syncthreads();
+    CFn ex;
+    ex.a = __shfl_up_sync(0xFFFFFFFFu, inc.a, 1);
+    ex.b = __shfl_up_sync(0xFFFFFFFFu, inc.b, 1);
+    if (lane == 0) ex = cfn_id();
+    if (warp > 0) ex = cfn_then(s_w[warp - 1], ex);
+    total = s_w[nw - 1];
+    __syncthreads();
+    return ex;
+}
+
+// Exclusive max-scan (ex: the largest value of the threads before) and the
+// block's largest value.  s_m: 32 entries.
+__device__ uint32_t cmp_block_max(uint32_t v, uint32_t* s_m, uint32_t& total) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t inc = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t g = __shfl_up_sync(0xFFFFFFFFu, inc, off);
+        if ((int)lane >= off) inc = max(inc, g);
+    }
+    if (lane == 31) s_m[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < nw ? s_m[lane] : 0u;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t g = __shfl_up_sync(0xFFFFFFFFu, w, off);
+            if ((int)lane >= off) w = max(w, g);
+        }
+        s_m[lane] = w;
+    }
+    __syncthreads();
+    uint32_t ex = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
+    if (lane == 0) ex = 0u;
+    if (warp > 0) ex = max(ex, s_m[warp - 1]);
+    total = s_m[nw - 1];
+    __syncthreads();
+    return ex;
+}
+
+// Exclusive sum-scan and the block's sum.  s_m: 32 entries.
+__device__ uint32_t cmp_block_sum(uint32_t v, uint32_t* s_m, uint32_t& total) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t inc = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t g = __shfl_up_sync(0xFFFFFFFFu, inc, off);
+        if ((int)lane >= off) inc += g;
+    }
+    if (lane == 31) s_m[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < nw ? s_m[lane] : 0u;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t g = __shfl_up_sync(0xFFFFFFFFu, w, off);
+            if ((int)lane >= off) w += g;
+        }
+        s_m[lane] = w;
+    }
+    __syncthreads();
+    uint32_t ex = inc - v;
+    if (warp > 0) ex += s_m[warp - 1];
+    total = s_m[nw - 1];
+    __syncthreads();
+    return ex;
+}
+
+// 1. Each pending op of round r: its first free slot (op_slot), its mark
+// (op_flag 3) and its demand on that slot (seg_cnt).
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_cmp_find(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
+                                                     uint32_t r, OpScratch sc, Ctl* ctl, uint32_t force) {
+    const RoundOps ops = round_ops(sc, ctl, r, cmp_n0(n0, ctl));
+    bool fb = force != 0u && blockIdx.x == 0 && threadIdx.x == 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ops.n; i += gridDim.x * blockDim.x) {
+        const uint32_t j = ops.op(i);
+        const uint64_t F = find_free<KB>(t, keys, j);
+        sc.op_slot[j] = F;
+        sc.op_flag[j] = 3;
+        if (F == NONE64) fb = true;
+        else atomicAdd(&t.seg_cnt[F], 1u);
+    }
+    if (fb) reinterpret_cast<CmpHdr*>(sc.comp)->fallback = 1u;
+}
+
+// 2. Each chunk's composition.
+__global__ void __launch_bounds__(CMP_THREADS) k_cmp_fn(TableView t, uint8_t* comp) {
+    __shared__ CFn s_w[32];
+    CmpView cv(comp, t.mask);
+    const uint64_t s0 = (uint64_t)blockIdx.x * CMP_CHUNK + (uint64_t)threadIdx.x * CMP_PER_T;
+    uint32_t fl[CMP_PER_T], dm[CMP_PER_T];
+    cmp_load(t, s0, fl, dm);
+    CFn total;
+    cmp_block_scan(cmp_thread_fn(fl, dm), s_w, total);
+    if (threadIdx.x == 0) cv.fn[blockIdx.x] = total;
+}
+
+// 3. One block: the carry into every chunk, from the carry round the ring.
+__global__ void __launch_bounds__(1024) k_cmp_carry(uint8_t* comp, uint64_t mask) {
+    __shared__ CFn s_w[32];
+    CmpView cv(comp, mask);
+    const uint32_t per = (cv.nch + blockDim.x - 1) / blockDim.x;
+    const uint32_t c0 = min(threadIdx.x * per, cv.nch), c1 = min(c0 + per, cv.nch);
+    CFn f = cfn_id();
+    for (uint32_t c = c0; c < c1; c++) f = cfn_then(f, cv.fn[c]);
+    CFn total;
+    const CFn ex = cmp_block_scan(f, s_w, total);
+    if (total.b >= 0 || total.a < 0) {  // block-uniform
+        if (threadIdx.x == 0) cv.hdr->fallback = 1u;
+        return;
+    }
+    long long carry = cfn_apply(ex, total.a);
+    for (uint32_t c = c0; c < c1; c++) {
+        cv.carry[c] = carry;
+        carry = cfn_apply(cv.fn[c], carry);
+    }
+}
+
+// 4. Component starts: every demand slot gets its component's start in
+// seg_min (CMP_UNK when it lies in an earlier chunk); each chunk its last start.
+__global__ void __launch_bounds__(CMP_THREADS) k_cmp_starts(TableView t, uint8_t* comp) {
+    __shared__ CFn s_w[32];
+    __shared__ uint32_t s_m[32];
+    CmpView cv(comp, t.mask);
+    if (*(volatile uint32_t*)&cv.hdr->fallback) return;  // block-uniform
+    const uint64_t s0 = (uint64_t)blockIdx.x * CMP_CHUNK + (uint64_t)threadIdx.x * CMP_PER_T;
+    uint32_t fl[CMP_PER_T], dm[CMP_PER_T];
+    cmp_load(t, s0, fl, dm);
+    CFn total;
+    const CFn ex = cmp_block_scan(cmp_thread_fn(fl, dm), s_w, total);
+    const long long cin = cfn_apply(ex, cv.carry[blockIdx.x]);
+    long long c = cin;
+    uint32_t last = 0;
+#pragma unroll
+    for (int i = 0; i < (int)CMP_PER_T; i++) {
+        if (is_free(fl[i])) {
+            if (dm[i] && c == 0) last = (uint32_t)(s0 + i) + 1u;
+            c = max(0ll, c + (long long)dm[i] - 1);
+        }
+    }
+    uint32_t tot;
+    uint32_t cur = cmp_block_max(last, s_m, tot);
+    c = cin;
+#pragma unroll
+    for (int i = 0; i < (int)CMP_PER_T; i++) {
+        if (is_free(fl[i])) {
+            if (dm[i]) {
+                if (c == 0) cur = (uint32_t)(s0 + i) + 1u;
+                t.seg_min[s0 + i] = cur ? cur - 1u : CMP_UNK;
+            }
+            c = max(0ll, c + (long long)dm[i] - 1);
+        }
+    }
+    if (threadIdx.x == 0) cv.last[blockIdx.x] = tot;
+}
+
+// 5. One block: the last start before every chunk, round the ring.
+__global__ void __launch_bounds__(1024) k_cmp_prev(uint8_t* comp, uint64_t mask) {
+    __shared__ uint32_t s_m[32];
+    CmpView cv(comp, mask);
+    if (*(volatile uint32_t*)&cv.hdr->fallback) return;
+    const uint32_t per = (cv.nch + blockDim.x - 1) / blockDim.x;
+    const uint32_t c0 = min(threadIdx.x * per, cv.nch), c1 = min(c0 + per, cv.nch);
+    uint32_t m = 0;
+    for (uint32_t c = c0; c < c1; c++) m = max(m, cv.last[c]);
+    uint32_t tot;
+    uint32_t ex = cmp_block_max(m, s_m, tot);
+    for (uint32_t c = c0; c < c1; c++) {
+        cv.prev[c] = ex ? ex : tot;
+        ex = max(ex, cv.last[c]);
+    }
+}
+
+// 6. Each pending op's block: a hash of its component's start (0 for all on
+// the fallback).
+__global__ void __launch_bounds__(RBLOCK) k_cmp_own(TableView t, uint32_t n0, uint32_t r, OpScratch sc, Ctl* ctl,
+                                                    uint32_t nblk) {
+    const RoundOps ops = round_ops(sc, ctl, r, cmp_n0(n0, ctl));
+    CmpView cv(sc.comp, t.mask);
+    const bool fb = *(volatile uint32_t*)&cv.hdr->fallback != 0u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ops.n; i += gridDim.x * blockDim.x) {
+        const uint32_t j = ops.op(i);
+        uint32_t o = 0;
+        if (!fb) {
+            const uint64_t F = sc.op_slot[j];
+            uint32_t v = t.seg_min[F];
+            if (v == CMP_UNK) v = cv.prev[F / CMP_CHUNK] - 1u;
+            o = (uint32_t)(((uint64_t)(v * 2654435761u) * nblk) >> 32);
+        }
+        sc.op_word[j] = o;
+    }
+}
+
+// 7. The marked ops in index order (long_list): counts per block of op
+// indices (kept in op_pt), one block's scan of them, then the writes.
+__device__ __forceinline__ uint32_t cmp_marks(const OpScratch& sc, uint32_t n0, uint32_t j0) {
+    uint32_t m = 0;
+    if (j0 + CMP_OPS_PER_T <= n0) {
+        const uint4 w = *reinterpret_cast<const uint4*>(sc.op_flag + j0);
+        const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int q = 0; q < 16; q++)
+            if (((ws[q >> 2] >> (8 * (q & 3))) & 0xFFu) == 3u) m |= 1u << q;
+    } else {
+        for (uint32_t q = 0; q < CMP_OPS_PER_T && j0 + q < n0; q++)
+            if (sc.op_flag[j0 + q] == 3) m |= 1u << q;
+    }
+    return m;
+}
+
+__global__ void __launch_bounds__(CMP_THREADS) k_cmp_count(OpScratch sc, uint32_t n0, const Ctl* ctl) {
+    __shared__ uint32_t s_m[32];
+    n0 = cmp_n0(n0, ctl);
+    const uint32_t j0 = blockIdx.x * CMP_OPS_PER_BLOCK + threadIdx.x * CMP_OPS_PER_T;
+    uint32_t tot;
+    cmp_block_sum(__popc(cmp_marks(sc, n0, j0)), s_m, tot);
+    if (threadIdx.x == 0) sc.op_pt[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(1024) k_cmp_offsets(OpScratch sc, uint32_t nb) {
+    __shared__ uint32_t s_m[32];
+    const uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
+    const uint32_t b0 = min(threadIdx.x * per, nb), b1 = min(b0 + per, nb);
+    uint32_t v = 0;
+    for (uint32_t b = b0; b < b1; b++) v += sc.op_pt[b];
+    uint32_t tot;
+    uint32_t ex = cmp_block_sum(v, s_m, tot);
+    for (uint32_t b = b0; b < b1; b++) {
+        const uint32_t c = sc.op_pt[b];
+        sc.op_pt[b] = ex;
+        ex += c;
+    }
+    if (threadIdx.x == 0) reinterpret_cast<CmpHdr*>(sc.comp)->np = tot;
+}
+
+__global__ void __launch_bounds__(CMP_THREADS) k_cmp_list(OpScratch sc, uint32_t n0, const Ctl* ctl) {
+    __shared__ uint32_t s_m[32];
+    n0 = cmp_n0(n0, ctl);
+    const uint32_t j0 = blockIdx.x * CMP_OPS_PER_BLOCK + threadIdx.x * CMP_OPS_PER_T;
+    uint32_t m = cmp_marks(sc, n0, j0);
+    uint32_t tot;
+    uint32_t at = sc.op_pt[blockIdx.x] + cmp_block_sum(__popc(m), s_m, tot);
+    while (m) {
+        const int q = __ffs(m) - 1;
+        m &= m - 1u;
+        sc.long_list[at++] = j0 + (uint32_t)q;
+    }
+}
+
+// 8. Every block runs the ops it owns in index order.
+template <int KB, int VB>
+__global__ void __launch_bounds__(CMP_EXEC_THREADS, 2) k_ins_comp(TableView t, const uint8_t* __restrict__ keys,
+                                                                  const uint8_t* __restrict__ vals, uint32_t r,
+                                                                  OpScratch sc, Ctl* ctl) {
+    __shared__ uint32_t s_buf[CMP_EXEC_THREADS];
+    __shared__ uint32_t s_woff[33];
+    __shared__ TileChain s_chain;
+    __shared__ SerialOut s_out;
+    extern __shared__ __align__(16) unsigned char s_dyn[];  // SerialChain (compile-time sizes)
+    const CmpHdr* hdr = reinterpret_cast<const CmpHdr*>(sc.comp);
+    const uint32_t np = *(volatile const uint32_t*)&hdr->np;
+    const bool fb = *(volatile const uint32_t*)&hdr->fallback != 0u;
+    ExecAcc a;
+    if (!fb || blockIdx.x == 0) {  // block-uniform
+        for (uint32_t base = 0; base < np; base += blockDim.x) {
+            const uint32_t i = base + threadIdx.x;
+            const uint32_t j = i < np ? sc.long_list[i] : 0u;
+            const bool take = i < np && sc.op_word[j] == blockIdx.x;
+            const uint32_t c = block_compact(j, take, s_buf, s_woff);
+            serial_apply<KB, VB, CMP_EXEC_THREADS>(t, keys, vals, s_buf, c, sc, a, &s_chain,
+                                                   (KB && VB) ? reinterpret_cast<SerialChain*>(s_dyn) : nullptr,
+                                                   &s_out);
+            __syncthreads();
+        }
+    }
+    if (a.claimed) atomicAdd(&ctl->count, (unsigned long long)a.claimed);
+    if (a.maxd > *(volatile uint32_t*)&ctl->dmax) atomicMax(&ctl->dmax, a.maxd);
+    if (a.tomb) ctl->tomb_claimed = 1u;
+    if (a.limit) atomicOr(&ctl->err, ERR_WALK_LIMIT);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->npend[r & 1] = 0;
+        ctl->npend[(r + 1) & 1] = 0;
+        atomicAdd(&ctl->rounds, 1u);
+    }
+}
+
+// 9. Registrations and inflow words back to idle.
+__global__ void __launch_bounds__(RBLOCK) k_cmp_clean(TableView t, OpScratch sc) {
+    const uint32_t np = *(volatile const uint32_t*)&reinterpret_cast<const CmpHdr*>(sc.comp)->np;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+        const uint32_t j = sc.long_list[i];
+        const uint64_t F = sc.op_slot[j];
+        if (F != NONE64) {
+            t.seg_min[F] = IDLE;
+            t.seg_cnt[F] = 0;
+        }
+        sc.op_word[j] = IDLE;
+    }
+}
+
 constexpr int INS_T = 32;  // lanes per insert in the single-block tail
 
 // ---- grouped rounds (batch waves) ------------------------------------------
@@ -1631,6 +2072,12 @@ void grp_ins_shape(const GroupOp* ops, uint32_t nops, uint64_t sum_n, int phase,
     count_launches(nrounds * ((KB != 0 && VB != 0) ? 4 : 3));
 }
 
+// Pending count of round r of every op.
+__global__ void k_grp_pending_each(const GroupOp* __restrict__ ops, uint32_t nops, uint32_t r, uint32_t* out) {
+    for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < nops; o += gridDim.x * blockDim.x)
+        out[o] = grp_pending(ops, o, r);
+}
+
 // Largest pending count of round r over the ops (one thread).
 __global__ void k_grp_pending(const GroupOp* __restrict__ ops, uint32_t nops, uint32_t r, uint32_t* out) {
     uint32_t m = 0;
@@ -1689,6 +2136,49 @@ void serial_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, 
     count_launches(1);
 }
 
+// The component path (k_cmp_* then k_ins_comp): npend bounds round r's
+// pending count (sizes the per-op grids) and, with n0 = CMP_N0_CTL, the
+// call's op count too.
+template <int KB, int VB>
+void comp_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, uint32_t r,
+                uint32_t npend, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+    KtScope kt(KC_INS_SERIAL, s);
+    const size_t smem = serial_smem(k_ins_comp<KB, VB>, KB && VB);
+    static int per_sm = 0;  // resident exec blocks per SM, per instantiation
+    if (per_sm == 0) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_ins_comp<KB, VB>, CMP_EXEC_THREADS, smem) !=
+                cudaSuccess ||
+            b < 1)
+            b = 1;
+        per_sm = b;
+    }
+    const uint32_t nblk = (uint32_t)(num_sms() * per_sm);
+    // start slots are kept as 32-bit words
+    const bool force = t.mask >= 0xFFFFFFF0ull;
+    const unsigned g = grid_for(npend, 8);
+    const unsigned nch = (unsigned)cmp_chunks(t.mask);
+    const uint32_t n0_max = n0 != CMP_N0_CTL ? n0 : npend;
+    const unsigned nb = (unsigned)(((uint64_t)n0_max + CMP_OPS_PER_BLOCK - 1) / CMP_OPS_PER_BLOCK);
+    cudaMemsetAsync(sc.comp, 0, sizeof(CmpHdr), s);
+    k_cmp_find<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, r, sc, ctl, force ? 1u : 0u);
+    unsigned launches = 1;
+    if (!force) {
+        k_cmp_fn<<<nch, CMP_THREADS, 0, s>>>(t, sc.comp);
+        k_cmp_carry<<<1, 1024, 0, s>>>(sc.comp, t.mask);
+        k_cmp_starts<<<nch, CMP_THREADS, 0, s>>>(t, sc.comp);
+        k_cmp_prev<<<1, 1024, 0, s>>>(sc.comp, t.mask);
+        launches += 4;
+    }
+    k_cmp_own<<<g, RBLOCK, 0, s>>>(t, n0, r, sc, ctl, nblk);
+    k_cmp_count<<<nb, CMP_THREADS, 0, s>>>(sc, n0, ctl);
+    k_cmp_offsets<<<1, 1024, 0, s>>>(sc, nb);
+    k_cmp_list<<<nb, CMP_THREADS, 0, s>>>(sc, n0, ctl);
+    k_ins_comp<KB, VB><<<nblk, CMP_EXEC_THREADS, smem, s>>>(t, keys, vals, r, sc, ctl);
+    k_cmp_clean<<<g, RBLOCK, 0, s>>>(t, sc);
+    count_launches(launches + 6);
+}
+
 }  // namespace
 
 #define FM_SHAPE_SWITCH(sh, CALL)                 \
@@ -1733,9 +2223,27 @@ cudaError_t launch_grp_pending(const GroupOp* ops, uint32_t nops, uint32_t r, ui
     return cudaGetLastError();
 }
 
+cudaError_t launch_grp_pending_each(const GroupOp* ops, uint32_t nops, uint32_t r, uint32_t* out, cudaStream_t s) {
+    k_grp_pending_each<<<(nops + 255) / 256, 256, 0, s>>>(ops, nops, r, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_ins_serial(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
                               uint32_t r, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
 #define FM_CALL(K, V) serial_shape<K, V>(t, keys, vals, n0, r, sc, ctl, s)
+    FM_SHAPE_SWITCH(sh, FM_CALL)
+#undef FM_CALL
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ins_comp(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
+                            uint32_t r, uint32_t npend, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+    if (!sc.comp) {
+        if (n0 == CMP_N0_CTL) return cudaErrorInvalidValue;
+        return launch_ins_serial(t, sh, keys, vals, n0, r, sc, ctl, s);
+    }
+#define FM_CALL(K, V) comp_shape<K, V>(t, keys, vals, n0, r, npend, sc, ctl, s)
     FM_SHAPE_SWITCH(sh, FM_CALL)
 #undef FM_CALL
     return cudaGetLastError();

@@ -63,8 +63,17 @@ struct OpScratch {
     uint8_t* op_flag;    // insert: leader bit; remove: potential-target count
     uint32_t* op_pt;     // remove: up to PT_MAX potential-target distances per op
     uint32_t* long_list; // insert: ops of this round deferred to the warp-per-op pass
+    uint8_t* comp;       // insert: component buffer (cmp_bytes of the table; null: none)
     uint64_t cap_ops;
 };
+
+// Component buffer of the one-at-a-time insert path: a 256-byte header, then
+// 32 bytes per chunk of CMP_CHUNK slots.  CMP_N0_CTL as a call's op count:
+// read it from the control block (grouped calls).
+constexpr uint64_t CMP_CHUNK = 8192;
+__host__ __device__ inline uint64_t cmp_chunks(uint64_t mask) { return (mask + CMP_CHUNK) / CMP_CHUNK; }
+__host__ __device__ inline uint64_t cmp_bytes(uint64_t mask) { return 256 + cmp_chunks(mask) * 32; }
+constexpr uint32_t CMP_N0_CTL = 0xFFFFFFFFu;
 constexpr int PT_MAX = 4;
 
 enum Shape { SHAPE_8_8 = 0, SHAPE_32_128, SHAPE_32_64, SHAPE_32_32, SHAPE_8_32, SHAPE_GENERIC };
@@ -92,6 +101,13 @@ cudaError_t launch_ins_tail(const TableView& t, Shape sh, const uint8_t* keys, c
 // found the table full, with more than TAIL_MAX ops pending).
 cudaError_t launch_ins_serial(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
                               uint32_t r, const OpScratch& sc, Ctl* ctl, cudaStream_t s);
+// The same over the whole GPU: round r's pending ops (at most npend) split
+// into components that touch disjoint slots, each run in index order on one
+// block.  n0 may be CMP_N0_CTL (grouped calls; npend then also bounds the
+// call size).  Without a component buffer (sc.comp null) it is
+// launch_ins_serial.
+cudaError_t launch_ins_comp(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
+                            uint32_t r, uint32_t npend, const OpScratch& sc, Ctl* ctl, cudaStream_t s);
 cudaError_t launch_rem_rounds(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, uint32_t r0,
                               uint32_t nrounds, uint32_t grid_ops, const OpScratch& sc, Ctl* ctl, cudaStream_t s);
 cudaError_t launch_rem_tail(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, uint32_t r,
@@ -165,6 +181,8 @@ cudaError_t launch_grp_rem(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t
                            uint32_t nrounds, cudaStream_t s);
 // *out = the largest pending count of round r over the ops (insert or remove).
 cudaError_t launch_grp_pending(const GroupOp* ops, uint32_t nops, uint32_t r, uint32_t* out, cudaStream_t s);
+// out[o] = the pending count of round r of op o.
+cudaError_t launch_grp_pending_each(const GroupOp* ops, uint32_t nops, uint32_t r, uint32_t* out, cudaStream_t s);
 
 // Optional device timing per kernel class: while a table's timing is on, the
 // library records a CUDA event pair around each launch made for it on the

@@ -1,0 +1,71 @@
+"""The component split of the one-at-a-time insert path, checked on the CPU
+oracle.
+
+When insert rounds stall, the pending ops are split into components by a
+carry walk over the free slots (EMPTY or TOMBSTONE) in slot order: a free
+slot s with d(s) ops whose first free slot is s passes on
+max(0, c + d(s) - 1) of the c ops arriving at it; a free slot with demand
+and no arriving carry starts a component, and every op belongs to the last
+start at or before its first free slot (round the ring).  The device runs
+the components at the same time, each in index order.  This restates the
+split in numpy and checks its claim on the oracle: applying the components
+one after another in reverse start order gives the same counts and the same
+table, slot for slot, as the batch in index order.
+"""
+import numpy as np
+import pytest
+
+from fm_testutil import OracleAdapter
+
+
+def component_of(flags, homes, cap):
+    st = flags & 0xF
+    fidx = np.nonzero((st == 0) | (st == 2))[0]
+    pos = np.searchsorted(fidx, homes)
+    F = fidx[np.where(pos < len(fidx), pos, 0)]  # first free slot at or after home, round the ring
+    d = np.zeros(cap, np.int64)
+    np.add.at(d, F, 1)
+    assert d[fidx].sum() < len(fidx), "no free slot to spare: the device takes the plain order"
+    # carry into every free slot; two turns settle the carry round the ring
+    c = 0
+    cin = np.zeros(len(fidx), np.int64)
+    for _ in range(2):
+        for i, s in enumerate(fidx):
+            cin[i] = c
+            c = max(0, c + d[s] - 1)
+    demand = d[fidx] > 0
+    starts = fidx[demand & (cin == 0)]
+    assert len(starts)
+    at = np.searchsorted(starts, F, side="right") - 1
+    return starts[at]  # -1 wraps to the last start
+
+
+@pytest.mark.parametrize("case", [(1 << 12, 0.8, 0.18, 0.0), (1 << 13, 0.85, 0.13, 0.0), (1 << 13, 0.9, 0.2, 0.3)])
+@pytest.mark.parametrize("seed", [0, 1])
+def test_components_commute(case, seed):
+    cap, load0, frac, rm = case
+    rng = np.random.default_rng(seed)
+    a, b = OracleAdapter(cap, 8, 8), OracleAdapter(cap, 8, 8)
+    pk = rng.integers(0, 256, (int(cap * load0), 8), dtype=np.uint8)
+    for m in (a, b):
+        m.bulk_insert(pk, pk)
+    if rm:
+        r = pk[rng.choice(len(pk), int(len(pk) * rm), replace=False)]
+        assert a.bulk_remove(r) == b.bulk_remove(r)
+    n = int(cap * frac)
+    k = rng.integers(0, 256, (n, 8), dtype=np.uint8)
+    k[rng.choice(n, n // 10)] = k[rng.integers(0, n, n // 10)]  # in-batch duplicates
+    k[rng.choice(n, n // 10)] = pk[rng.integers(0, len(pk), n // 10)]  # updates
+    v = rng.integers(0, 256, (n, 8), dtype=np.uint8)
+    homes = (k.view("<u8").reshape(-1) & np.uint64(cap - 1)).astype(np.int64)  # identity hash
+    comp = component_of(a.snapshot()[0].astype(np.int64), homes, cap)
+    starts = np.unique(comp)
+    assert len(starts) > 10  # a real split, not one component
+    whole = a.bulk_insert(k, v)
+    parts = 0
+    for c in starts[::-1]:
+        idx = np.nonzero(comp == c)[0]
+        parts += b.bulk_insert(k[idx], v[idx])
+    assert whole == parts
+    for x, y in zip(a.snapshot(), b.snapshot()):
+        assert np.array_equal(x, y)
