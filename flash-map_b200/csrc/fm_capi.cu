@@ -33,6 +33,9 @@ int cuda_fail(int code, const char* what, cudaError_t e) {
 // an idle segment slot, so a call is split into sequential chunks (which is
 // exactly the sequential semantics) of at most this many operations.
 constexpr uint64_t OP_CHUNK = 1ull << 30;
+#ifndef FM_DIRECT_LOAD
+#define FM_DIRECT_LOAD 0.97  // load from which an insert call skips the rounds
+#endif
 
 struct DeviceGuard {
     int prev = -1;
@@ -273,12 +276,24 @@ int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t
         if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "round setup", e);
         uint32_t r = 0;
         uint32_t left = m;
+        // a chunk that can take the table to FM_DIRECT_LOAD or beyond runs as
+        // components from the start: rounds stall there, and their tiles'
+        // short chain buffers walk chains of thousands of entries again and
+        // again
+        const bool direct = insert && (double)(t->len.load() + total + m) >= FM_DIRECT_LOAD * (double)t->cap;
         for (;;) {
+            if (direct) {
+                e = fm::launch_ins_comp(v, sh, kk, vv, m, 0, m, t->sc, t->d_ctl, s);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "component insert", e);
+                break;
+            }
             e = insert ? fm::launch_ins_rounds(v, sh, kk, vv, m, r, 2, left, t->sc, t->d_ctl, s)
                        : fm::launch_rem_rounds(v, sh, kk, m, r, 2, left, t->sc, t->d_ctl, s);
             r += 2;
             if (e == cudaSuccess)
-                e = insert ? fm::launch_ins_tail(v, sh, kk, vv, m, r, t->sc, t->d_ctl, s)
+                e = insert ? fm::launch_ins_tail(v, sh, kk, vv, m, r, t->sc, t->d_ctl, s, true)
                            : fm::launch_rem_tail(v, sh, kk, m, r, t->sc, t->d_ctl, s);
             if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, insert ? "insert rounds" : "remove rounds", e);
             e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
@@ -286,6 +301,15 @@ int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t
             if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "round readback", e);
             if (t->h_ctl->err & fm::ERR_SCRATCH) return fail(FM_ERR_KERNEL_LAUNCH, "stale segment registration");
             if (t->h_ctl->err & fm::ERR_NO_PROGRESS) return fail(FM_ERR_PROBE_LIMIT, "round made no progress");
+            if (insert && t->h_ctl->tail_handoff) {
+                // the tail stopped progressing: its round's ops run as components
+                const uint32_t rh = t->h_ctl->tail_handoff - 1;
+                e = fm::launch_ins_comp(v, sh, kk, vv, m, rh, t->h_ctl->npend[rh & 1], t->sc, t->d_ctl, s);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "component insert", e);
+                break;
+            }
             uint32_t now = t->h_ctl->npend[r & 1];
             if (insert && now > 0 && t->h_ctl->serial[(r - 1) & 1]) {
                 // the table is full: the remaining ops run one at a time in index order

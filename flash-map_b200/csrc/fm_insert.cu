@@ -1277,12 +1277,16 @@ int p4_lanes() {
 // One block runs every remaining round of the call (phases separated by block
 // barriers) when at most TAIL_MAX ops are pending, or returns at once.  A
 // serial round hands its ops to serial_process.  On completion both pending
-// counts are zero (the host's done marker).
+// counts are zero (the host's done marker).  With `handoff`, rounds that stop
+// progressing are handed back instead of run one at a time here: the tail
+// stops at a round boundary with that round's ops pending and records the
+// round in Ctl::tail_handoff (the host then runs them as components).
 
 template <int KB, int VB, int T>
 __device__ __forceinline__ void ins_tail_body(const TableView& t, const uint8_t* __restrict__ keys,
                                               const uint8_t* __restrict__ vals, uint32_t n0, uint32_t r0,
-                                              uint32_t nops, const OpScratch& sc, Ctl* ctl, uint32_t limit) {
+                                              uint32_t nops, const OpScratch& sc, Ctl* ctl, uint32_t limit,
+                                              bool handoff) {
     // tiles holding a chain buffer (T > 1): as many as the static shared
     // memory allows; the block's other warps idle in the tile phases
     constexpr int NT = T > 1 ? (TAIL_THREADS / T < 12 ? TAIL_THREADS / T : 12) : 1;
@@ -1300,6 +1304,7 @@ __device__ __forceinline__ void ins_tail_body(const TableView& t, const uint8_t*
     ExecAcc a;
     uint32_t r = r0;
     uint32_t rounds = 0;
+    uint32_t handed = 0;  // ops handed back at round r (handoff)
     // tiles (T > 1) or single threads (T == 1) as the unit of work
     const uint32_t unit = T > 1 ? threadIdx.x / T : threadIdx.x;
     const uint32_t nunits = T > 1 ? (uint32_t)NT : blockDim.x;
@@ -1349,6 +1354,10 @@ __device__ __forceinline__ void ins_tail_body(const TableView& t, const uint8_t*
                 sc.op_word[j] = IDLE;
             }
             __syncthreads();
+            if (handoff && in) {
+                handed = n;
+                break;
+            }
             serial_process<KB, VB>(t, keys, vals, in, n, n0, sc, a, s_buf, s_woff, T > 1 ? &s_chain[0] : nullptr);
             ++rounds;
             break;
@@ -1377,6 +1386,10 @@ __device__ __forceinline__ void ins_tail_body(const TableView& t, const uint8_t*
             // under 1/8 of the ops per round (ops crowded onto few free slots,
             // a near-full table): the rest in index order, one at a time
             __syncthreads();
+            if (handoff) {
+                handed = nn;
+                break;
+            }
             serial_process<KB, VB>(t, keys, vals, pend_of(sc, r), nn, n0, sc, a, s_buf, s_woff,
                                    T > 1 ? &s_chain[0] : nullptr);
             ++rounds;
@@ -1397,6 +1410,10 @@ __device__ __forceinline__ void ins_tail_body(const TableView& t, const uint8_t*
         } else {
             ctl->npend[r0 & 1] = 0;  // done marker read by the host
             ctl->npend[(r0 + 1) & 1] = 0;
+            if (handed) {
+                ctl->npend[r & 1] = handed;
+                ctl->tail_handoff = r + 1;
+            }
         }
         atomicAdd(&ctl->rounds, rounds);
     }
@@ -1405,8 +1422,9 @@ __device__ __forceinline__ void ins_tail_body(const TableView& t, const uint8_t*
 template <int KB, int VB, int T>
 __global__ void __launch_bounds__(TAIL_THREADS) k_ins_tail(TableView t, const uint8_t* __restrict__ keys,
                                                            const uint8_t* __restrict__ vals, uint32_t n0,
-                                                           uint32_t r0, uint32_t nops, OpScratch sc, Ctl* ctl) {
-    ins_tail_body<KB, VB, T>(t, keys, vals, n0, r0, nops, sc, ctl, TAIL_MAX);
+                                                           uint32_t r0, uint32_t nops, OpScratch sc, Ctl* ctl,
+                                                           bool handoff) {
+    ins_tail_body<KB, VB, T>(t, keys, vals, n0, r0, nops, sc, ctl, TAIL_MAX, handoff);
 }
 
 // Host-launched fallback for a serial round whose pending count is above
@@ -1991,7 +2009,7 @@ template <int KB, int VB, int T>
 __global__ void __launch_bounds__(TAIL_THREADS) k_grp_ins_tail(const GroupOp* __restrict__ ops, uint32_t r0) {
     const GroupOp& g = ops[blockIdx.x];
     const uint32_t n0 = *(volatile const uint32_t*)&g.ctl->n0;
-    ins_tail_body<KB, VB, T>(g.t, g.keys, g.vals, n0, r0, g.n, g.sc, g.ctl, 0xFFFFFFFFu);
+    ins_tail_body<KB, VB, T>(g.t, g.keys, g.vals, n0, r0, g.n, g.sc, g.ctl, 0xFFFFFFFFu, false);
 }
 
 // Serial completion of a grouped call, one block per op: the op's pending
@@ -2121,9 +2139,10 @@ void rounds_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, 
 
 template <int KB, int VB>
 void tail_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, uint32_t r,
-                uint32_t nops, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+                uint32_t nops, const OpScratch& sc, Ctl* ctl, bool handoff, cudaStream_t s) {
     KtScope kt(KC_INS_TAIL, s);
-    k_ins_tail<KB, VB, (KB && VB) ? INS_T : 1><<<1, TAIL_THREADS, 0, s>>>(t, keys, vals, n0, r, nops, sc, ctl);
+    k_ins_tail<KB, VB, (KB && VB) ? INS_T : 1><<<1, TAIL_THREADS, 0, s>>>(t, keys, vals, n0, r, nops, sc, ctl,
+                                                                          handoff);
     count_launches(1);
 }
 
@@ -2201,8 +2220,8 @@ cudaError_t launch_ins_rounds(const TableView& t, Shape sh, const uint8_t* keys,
 }
 
 cudaError_t launch_ins_tail(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
-                            uint32_t r, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
-#define FM_CALL(K, V) tail_shape<K, V>(t, keys, vals, n0, r, n0, sc, ctl, s)
+                            uint32_t r, const OpScratch& sc, Ctl* ctl, cudaStream_t s, bool handoff) {
+#define FM_CALL(K, V) tail_shape<K, V>(t, keys, vals, n0, r, n0, sc, ctl, handoff, s)
     FM_SHAPE_SWITCH(sh, FM_CALL)
 #undef FM_CALL
     return cudaGetLastError();

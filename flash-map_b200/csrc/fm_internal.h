@@ -28,7 +28,7 @@ struct Ctl {
     uint32_t rounds;         // rounds run by the call (statistics)
     uint32_t nlong[2];       // inserts deferred to the warp-per-op pass, per round parity
     uint32_t n0;             // grouped (batch) calls: the call's op count after the precheck
-    uint32_t pad_;
+    uint32_t tail_handoff;   // insert tail: 1 + the round it left pending for the host (0: none)
     unsigned long long count;  // new keys (insert) / removed keys (remove), single-block kernels
     unsigned long long count_part[COUNT_PARTS][4];  // the same from grid kernels, [i][0] used
     // Persistent table facts (survive across calls, reset by clear):
@@ -94,9 +94,11 @@ cudaError_t launch_ins_rounds(const TableView& t, Shape sh, const uint8_t* keys,
                               uint32_t r0, uint32_t nrounds, uint32_t grid_ops, const OpScratch& sc, Ctl* ctl,
                               cudaStream_t s);
 // Runs every remaining round starting at r in one block if the pending count
-// is at most TAIL_MAX; otherwise returns without touching anything.
+// is at most TAIL_MAX; otherwise returns without touching anything.  With
+// handoff, rounds that stop progressing are left pending for the host
+// (Ctl::tail_handoff) instead of run one at a time in the block.
 cudaError_t launch_ins_tail(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
-                            uint32_t r, const OpScratch& sc, Ctl* ctl, cudaStream_t s);
+                            uint32_t r, const OpScratch& sc, Ctl* ctl, cudaStream_t s, bool handoff = false);
 // Applies round r's pending ops one at a time in index order (a round that
 // found the table full, with more than TAIL_MAX ops pending).
 cudaError_t launch_ins_serial(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
