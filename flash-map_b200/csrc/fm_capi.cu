@@ -36,6 +36,9 @@ constexpr uint64_t OP_CHUNK = 1ull << 30;
 #ifndef FM_DIRECT_LOAD
 #define FM_DIRECT_LOAD 0.97  // load from which an insert call skips the rounds
 #endif
+#ifndef FM_HANDOFF_LOAD
+#define FM_HANDOFF_LOAD 0.9  // load from which the insert tail hands stalled rounds back
+#endif
 
 struct DeviceGuard {
     int prev = -1;
@@ -280,7 +283,11 @@ int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t
         // components from the start: rounds stall there, and their tiles'
         // short chain buffers walk chains of thousands of entries again and
         // again
-        const bool direct = insert && (double)(t->len.load() + total + m) >= FM_DIRECT_LOAD * (double)t->cap;
+        const double reach = (double)(t->len.load() + total + m) / (double)t->cap;
+        const bool direct = insert && reach >= FM_DIRECT_LOAD;
+        // below FM_HANDOFF_LOAD the tail's own one-at-a-time order is cheaper
+        // than a hand-back (a readback and a scan of the table)
+        const bool handoff = reach >= FM_HANDOFF_LOAD;
         for (;;) {
             if (direct) {
                 e = fm::launch_ins_comp(v, sh, kk, vv, m, 0, m, t->sc, t->d_ctl, s);
@@ -293,7 +300,7 @@ int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t
                        : fm::launch_rem_rounds(v, sh, kk, m, r, 2, left, t->sc, t->d_ctl, s);
             r += 2;
             if (e == cudaSuccess)
-                e = insert ? fm::launch_ins_tail(v, sh, kk, vv, m, r, t->sc, t->d_ctl, s, true)
+                e = insert ? fm::launch_ins_tail(v, sh, kk, vv, m, r, t->sc, t->d_ctl, s, handoff)
                            : fm::launch_rem_tail(v, sh, kk, m, r, t->sc, t->d_ctl, s);
             if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, insert ? "insert rounds" : "remove rounds", e);
             e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
@@ -1079,6 +1086,7 @@ struct fm_batch {
         uint32_t wave;
         uint32_t kind;
         fm::Shape shape;
+        uint32_t lane = 0;              // stream lane of its tables
         std::vector<uint32_t> members;  // op indices
         size_t desc_off = 0;            // GroupGet[] / GroupOp[] in the descriptor buffer
         size_t prefix_off = 0;          // gets: uint64 prefix[n+1]
@@ -1090,6 +1098,15 @@ struct fm_batch {
     };
     std::vector<Group> groups;          // in execution order
     uint32_t waves = 0;
+    // Tables are spread over up to BATCH_LANES streams forked from the
+    // caller's stream (balanced by their ops' sizes): a table's ops stay in
+    // order on its lane, and lanes run at the same time, so a long op on one
+    // table does not hold up the waves of the others.
+    static constexpr uint32_t BATCH_LANES = 8;
+    uint32_t nlanes = 1;
+    cudaStream_t lane_s[BATCH_LANES] = {};
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[BATCH_LANES] = {};
     size_t desc_bytes = 0;
     uint8_t* d_desc = nullptr;          // descriptors (device)
     uint8_t* h_desc = nullptr;          // descriptors (pinned host)
@@ -1194,8 +1211,20 @@ int batch_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_res, 0, b->ops.size() * 8, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_status, 0, b->ops.size() * 4, s);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "batch upload", e);
+    const cudaStream_t s0 = s;
+    // an upper bound of each table's count as the waves go (inserts add
+    // their size): inserts that can take a table to FM_DIRECT_LOAD run as
+    // components from the start, as plain calls do
+    std::vector<double> est(b->tables.size());
+    for (size_t i = 0; i < b->tables.size(); i++) est[i] = (double)b->h_len()[i];
+    if (b->nlanes > 1) {  // fork the lanes off the caller's stream
+        e = cudaEventRecord(b->ev_fork, s0);
+        for (uint32_t l = 0; e == cudaSuccess && l < b->nlanes; l++) e = cudaStreamWaitEvent(b->lane_s[l], b->ev_fork, 0);
+        if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch fork", e);
+    }
     for (auto& g : b->groups) {
         const uint32_t n = (uint32_t)g.members.size();
+        s = b->nlanes > 1 ? b->lane_s[g.lane] : s0;
         if (g.kind == FM_OP_GET) {
             e = fm::launch_grp_get(g.shape, reinterpret_cast<const fm::GroupGet*>(b->d_desc + g.desc_off),
                                    reinterpret_cast<const uint64_t*>(b->d_desc + g.prefix_off), n, g.total, g.cfg, s);
@@ -1205,6 +1234,21 @@ int batch_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
         const auto* d = reinterpret_cast<const fm::GroupOp*>(b->d_desc + g.desc_off);
         auto* L = g.kind == FM_OP_INSERT ? &fm::launch_grp_ins : &fm::launch_grp_rem;
         e = L(g.shape, d, n, g.total, fm::GRP_BEGIN, 0, 0, s);
+        if (g.kind == FM_OP_INSERT) {
+            const auto* hd = reinterpret_cast<const fm::GroupOp*>(b->h_desc + g.desc_off);
+            for (uint32_t k = 0; e == cudaSuccess && k < n; k++) {
+                const uint32_t ti = b->table_of[g.members[k]];
+                const double cap = (double)b->tables[ti]->cap;
+                est[ti] += (double)hd[k].n;
+                if (est[ti] < FM_DIRECT_LOAD * cap) continue;
+                est[ti] = std::min(est[ti], cap);
+                // the member's ops as components, then a zero op count so the
+                // group's rounds pass it by (its counts stay for the finish)
+                e = fm::launch_ins_comp(hd[k].t, g.shape, hd[k].keys, hd[k].vals, fm::CMP_N0_CTL, 0, hd[k].n, hd[k].sc,
+                                        hd[k].ctl, s);
+                if (e == cudaSuccess) e = cudaMemsetAsync(&hd[k].ctl->n0, 0, sizeof(uint32_t), s);
+            }
+        }
         uint32_t r = 0;
         if (adaptive) {
             // every round runs the lowest pending op of each group: bounded
@@ -1255,6 +1299,14 @@ int batch_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
         if (e == cudaSuccess) e = L(g.shape, d, n, g.total, fm::GRP_END, r, 0, s);
         if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch wave", e);
     }
+    s = s0;
+    if (b->nlanes > 1) {  // join them back
+        for (uint32_t l = 0; e == cudaSuccess && l < b->nlanes; l++) {
+            e = cudaEventRecord(b->ev_join[l], b->lane_s[l]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b->ev_join[l], 0);
+        }
+        if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch join", e);
+    }
     e = cudaMemcpyAsync(b->h_len(), b->d_len, b->tables.size() * 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_res(), b->d_res, b->ops.size() * 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_status(), b->d_status, b->ops.size() * 4, cudaMemcpyDeviceToHost, s);
@@ -1275,6 +1327,7 @@ int fm_batch_create(const fm_op* ops, uint32_t nops, fm_batch** out) {
     b->device = ops[0].table ? ops[0].table->device : 0;
     std::vector<int> last_wave;
     std::vector<uint32_t> last_kind;
+    std::vector<uint32_t> op_wave;
     for (uint32_t i = 0; i < nops; i++) {
         const fm_op& o = ops[i];
         auto bad = [&](const char* why) {
@@ -1302,18 +1355,42 @@ int fm_batch_create(const fm_op* ops, uint32_t nops, fm_batch** out) {
         last_wave[ti] = w;
         last_kind[ti] = o.kind;
         if ((uint32_t)w + 1 > b->waves) b->waves = (uint32_t)w + 1;
+        op_wave.push_back((uint32_t)w);
+    }
+    // lanes: tables by decreasing work (sum of op sizes, mutations weighted
+    // up), each to the lane with the least work so far
+    const uint32_t ntab = (uint32_t)b->tables.size();
+    b->nlanes = ntab < fm_batch::BATCH_LANES ? ntab : fm_batch::BATCH_LANES;
+    std::vector<double> work(ntab, 0.0);
+    for (uint32_t i = 0; i < nops; i++)
+        work[b->table_of[i]] += (double)ops[i].n * (ops[i].kind == FM_OP_GET ? 1.0 : 4.0);
+    std::vector<uint32_t> order(ntab), lane_of(ntab, 0);
+    for (uint32_t i = 0; i < ntab; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return work[x] > work[y]; });
+    std::vector<double> lane_work(b->nlanes, 0.0);
+    for (uint32_t ti : order) {
+        uint32_t best = 0;
+        for (uint32_t l = 1; l < b->nlanes; l++)
+            if (lane_work[l] < lane_work[best]) best = l;
+        lane_of[ti] = best;
+        lane_work[best] += work[ti];
+    }
+    for (uint32_t i = 0; i < nops; i++) {
+        const fm_op& o = ops[i];
         if (o.n == 0) continue;  // nothing to launch; result 0, status OK
+        const uint32_t w = op_wave[i], lane = lane_of[b->table_of[i]];
         const fm::Shape sh = batch_aligned(o) ? o.table->shape : fm::SHAPE_GENERIC;
-        // the group of (wave, kind, shape), split at GROUP_MAX members
+        // the group of (lane, wave, kind, shape), split at GROUP_MAX members
         fm_batch::Group* g = nullptr;
         for (auto it = b->groups.rbegin(); it != b->groups.rend(); ++it) {
-            if (it->wave == (uint32_t)w && it->kind == o.kind && it->shape == sh && it->members.size() < fm::GROUP_MAX) {
+            if (it->wave == w && it->lane == lane && it->kind == o.kind && it->shape == sh &&
+                it->members.size() < fm::GROUP_MAX) {
                 g = &*it;
                 break;
             }
         }
         if (!g) {
-            b->groups.push_back(fm_batch::Group{(uint32_t)w, o.kind, sh, {}});
+            b->groups.push_back(fm_batch::Group{w, o.kind, sh, lane, {}});
             g = &b->groups.back();
         }
         g->members.push_back(i);
@@ -1358,6 +1435,17 @@ int fm_batch_create(const fm_op* ops, uint32_t nops, fm_batch** out) {
     b->h_pend = reinterpret_cast<uint32_t*>(b->arena.h + h_pend);
     memset(b->h_desc, 0, b->desc_bytes);
     memset(b->h_io, 0, b->io_bytes());
+    if (b->nlanes > 1) {
+        e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+        for (uint32_t l = 0; e == cudaSuccess && l < b->nlanes; l++) {
+            e = cudaStreamCreateWithFlags(&b->lane_s[l], cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join[l], cudaEventDisableTiming);
+        }
+        if (e != cudaSuccess) {
+            fm_batch_destroy(b);
+            return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch streams", e);
+        }
+    }
     *out = b;
     return FM_OK;
 }
@@ -1445,6 +1533,11 @@ void fm_batch_destroy(fm_batch* b) {
     if (b->pending && b->last_stream) cudaStreamSynchronize(b->last_stream);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
+    for (uint32_t l = 0; l < fm_batch::BATCH_LANES; l++) {
+        if (b->lane_s[l]) cudaStreamDestroy(b->lane_s[l]);
+        if (b->ev_join[l]) cudaEventDestroy(b->ev_join[l]);
+    }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     arena_give(b->arena);
     delete b;
 }
