@@ -981,9 +981,11 @@ constexpr int SERIAL_THREADS = 512;
 
 // One insert by a whole block of W threads (compile-time sizes,
 // capacity >= 128): warp 0 walks the chain into the large buffer, then every
-// thread moves records (204 account-shape records per round trip) and writes
-// flags.  A chain longer than the buffer takes the chunked warp path; a walk
-// that finds no free slot within a pass (overfull table) the scalar walk.
+// thread moves records (204 account-shape records per round trip with 512
+// threads) and writes flags.  A chain longer than the buffer moves its last
+// chunk first and each earlier chunk after warp 0 finds it again; a walk
+// that finds no free slot within a pass (overfull table) takes the scalar
+// walk.
 // Block-uniform call.
 template <int KB, int VB, int W = SERIAL_THREADS>
 __device__ void exec_serial_block(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t j,
@@ -1009,24 +1011,43 @@ __device__ void exec_serial_block(const TableView& t, const uint8_t* keys, const
     }
     __syncthreads();
     const int kind = so.kind;
-    if (kind == 5 || so.chunk_base != 0) {
-        if (threadIdx.x < 32) {
-            const Tile<32> tl;
-            int kk = 5;
-            if (kind != 5) kk = exec_tile<KB, VB, 32, SerialChain>(t, key, vals, j, tl, s, a);
-            if (kk == 5 && tl.lane == 0) a.claimed += exec_insert_key<KB, VB>(t, key, vin, a);
-        }
+    if (kind == 5) {
+        if (threadIdx.x == 0) a.claimed += exec_insert_key<KB, VB>(t, key, vin, a);
         __syncthreads();
         return;
     }
-    const uint32_t k = so.k;
+    const uint32_t k = so.k, cb = so.chunk_base;
     const int hi = kind == 3 ? (int)k - 1 : (int)k;
     const BlockCrew<W> crew;
-    tile_moves<KB, VB, 4>(t, key, vin, s, 0, hi, 0, k, kind, so.end_slot, so.src_base, crew);
+    // the last chunk of the chain (stages from cb) first
+    tile_moves<KB, VB, 4>(t, key, vin, s, cb, hi, (int)cb, k, kind, so.end_slot, so.src_base, crew);
     uint32_t md = 0;
-    for (uint32_t m = threadIdx.x; m < k; m += blockDim.x) {
-        t.flags[s.pos[m]] = mk_flag(ST_OCC, s.p[m]);
-        md = max(md, min(s.p[m], DIST_MASK));
+    for (uint32_t m = cb + threadIdx.x; m < k; m += blockDim.x) {
+        t.flags[s.pos[m - cb]] = mk_flag(ST_OCC, s.p[m - cb]);
+        md = max(md, min(s.p[m - cb], DIST_MASK));
+    }
+    __syncthreads();
+    // a chain longer than the buffer: earlier chunks from the top, each found
+    // again by warp 0 walking from home (slots before a chunk's end are
+    // untouched by the later chunks' moves), moved by the whole block
+    for (uint32_t top = cb; top > 0;) {
+        const uint32_t lo = top > (uint32_t)SMAXCH ? top - SMAXCH : 0u;
+        if (threadIdx.x < 32) {
+            const Tile<32> tl;
+            uint32_t k2, cb2, sb2;
+            uint64_t es2, ep2;
+            bool et2;
+            tile_walk<KB, 32, SerialChain>(t, key, s, tl, false, lo, top, k2, cb2, sb2, es2, ep2, et2);
+            if (tl.lane == 0) so.src_base = sb2;
+        }
+        __syncthreads();
+        tile_moves<KB, VB, 4>(t, key, vin, s, lo, (int)top - 1, (int)lo, k, kind, so.end_slot, so.src_base, crew);
+        for (uint32_t m = threadIdx.x; m < top - lo; m += blockDim.x) {
+            t.flags[s.pos[m]] = mk_flag(ST_OCC, s.p[m]);
+            md = max(md, min(s.p[m], DIST_MASK));
+        }
+        __syncthreads();
+        top = lo;
     }
     if (threadIdx.x == 0 && kind == 1) {
         t.flags[so.end_slot] = mk_flag(ST_OCC, so.end_p);

@@ -161,3 +161,24 @@ def test_large_table_many_components():
     ran = insert_both(g, o, k, v)
     assert_same(g, o, k[:20000])
     assert ran
+
+
+@pytest.mark.parametrize("shape", [(8, 8), (32, 128)])
+def test_chain_longer_than_the_block_buffer(shape):
+    """One cluster of 31,800 entries at their homes (identity hash), then an
+    insert homed inside it: the call takes the table past load 0.97, so it
+    runs as a component, and its chain of about 31,790 evictions is several
+    times the block's 8K-entry buffer (moved chunk by chunk from the top)."""
+    ks, vs = shape
+    cap = 1 << 15
+    g = gpu_map(cap, ks, vs)
+    o = OracleAdapter(cap, ks, vs)
+    homes = np.arange(31800, dtype=np.uint64)
+    pk = le(homes, ks)
+    pv = le(homes + np.uint64(7), vs)
+    assert g.bulk_insert(pk, pv) == o.bulk_insert(pk, pv)
+    k = le(np.array([5 + cap, 12 + 2 * cap], dtype=np.uint64), ks)  # homes 5 and 12
+    v = le(np.array([1, 2], dtype=np.uint64), vs)
+    ran = insert_both(g, o, k, v)
+    assert_same(g, o, np.concatenate([k, pk[::97]]))
+    assert ran
