@@ -1,29 +1,39 @@
 """Served form: continuous batching of bulk requests on a device-resident table.
 
 Requests (get / insert / remove of a key set, each with an arrival time)
-reach a :class:`FlashMapServer` in arrival order.  Two threads run them:
+reach a :class:`FlashMapServer` in arrival order.  Three threads serve them:
 
 * the stager admits arrived requests, oldest first, while their device
-  staging (keys, values, outputs) fits the memory budget, uploads their
-  inputs on its own copy stream and hands them on;
-* the executor takes every admitted request that is ready, runs them as one
+  staging (keys, values, outputs) fits the memory budget and uploads their
+  inputs on its own copy stream, in pieces of at most ``PIECE`` keys, so a
+  large request starts on the GPU after its first piece instead of its
+  whole upload;
+* the executor takes every staged piece that is ready and runs them as one
   :class:`~flash_map.FlashMapBatch` on the compute stream (arrival-order
   sequential semantics: each request's result is the one it would get alone
-  at its turn) or, when only one is ready, as the plain device-pointer call,
-  downloads the get results, stamps completion times and releases the
-  budget.
+  at its turn) or, when only one is ready, as the plain device-pointer call;
+  get results go down on a download stream behind the group's compute, while
+  the executor moves on to the next group.  An insert in several pieces
+  keeps the TableFull precheck of the whole request: its first piece starts
+  a group, where the host compares the table's exact count plus the whole
+  request with the capacity (a rejected request's pieces do not run; the
+  later pieces of an accepted one always fit);
+* the completer waits for each group's downloads, stamps completion times
+  (a request is done with its last piece) and releases the budget.
 
-So requests that arrive while a batch is on the GPU are admitted as memory
-frees up, their uploads overlap the running batch, and they join the next
-batch.  :class:`PlainServer` is the per-request baseline: one host-API bulk
-call per request in arrival order (the reference's ``AsyncFlashMap`` serves
-each request with one bulk call under a lock, src/async_map.rs:48-93).
+So requests that arrive while a group is on the GPU are staged meanwhile,
+their uploads and the previous group's downloads overlap the running group,
+and they join the next group.  :class:`PlainServer` is the per-request
+baseline: one host-API bulk call per request in arrival order (the
+reference's ``AsyncFlashMap`` serves each request with one bulk call under a
+lock, src/async_map.rs:48-93).
 
 No counterpart in the reference (bajpainaman/flash-map 0.5.0).
 """
 from __future__ import annotations
 
 import collections
+import queue
 import threading
 import time
 from dataclasses import dataclass, field
@@ -34,6 +44,8 @@ import numpy as np
 from .batch import GET, INSERT, REMOVE, BatchOp, FlashMapBatch
 from .errors import FM_ERR_PROBE_LIMIT, FM_ERR_TABLE_FULL, TableFull
 from .map import FlashMap
+
+PIECE = 1 << 18  # keys per staged piece of a request
 
 
 @dataclass
@@ -51,7 +63,7 @@ class Request:
     out_values: Optional[np.ndarray] = None
     out_found: Optional[np.ndarray] = None
     done: float = -1.0
-    _dev: list = field(default_factory=list, repr=False)
+    _left: int = field(default=0, repr=False)
 
     @property
     def n(self) -> int:
@@ -62,8 +74,8 @@ class Request:
         return self.done - self.arrival
 
 
-def staging_bytes(r: Request, key_size: int, value_size: int) -> int:
-    n = r.n
+def staging_bytes(r: Request, key_size: int, value_size: int, n: Optional[int] = None) -> int:
+    n = r.n if n is None else n
     if r.kind == INSERT:
         return n * (key_size + value_size)
     if r.kind == GET:
@@ -71,9 +83,18 @@ def staging_bytes(r: Request, key_size: int, value_size: int) -> int:
     return n * key_size
 
 
+class _Piece:
+    """Keys [off, off + n) of a request, staged on the device."""
+    __slots__ = ("req", "off", "n", "dk", "dv", "ov", "of", "ev", "need")
+
+    def __init__(self, req, off, n, need):
+        self.req, self.off, self.n, self.need = req, off, n, need
+        self.dk = self.dv = self.ov = self.of = self.ev = None
+
+
 class FlashMapServer:
     """Continuous batching over one FlashMap.  `budget` bounds the device
-    bytes staged for admitted, unfinished requests; a request larger than the
+    bytes staged for admitted, unfinished pieces; a piece larger than the
     whole budget is served alone once everything before it has finished."""
 
     def __init__(self, table: FlashMap, budget: int = 20 << 30, out_pool=None):
@@ -85,6 +106,7 @@ class FlashMapServer:
         self.dev = torch.device("cuda", table.device())
         self.copy_stream = torch.cuda.Stream(self.dev)
         self.stream = torch.cuda.Stream(self.dev)
+        self.down_stream = torch.cuda.Stream(self.dev)
         self.out_pool = out_pool  # optional callable(n, V) -> (pinned vals, pinned found) for get results
         self.batches = 0
         self.batch_sizes: List[int] = []
@@ -97,7 +119,8 @@ class FlashMapServer:
         K, V = self.t.key_size, self.t.value_size
         ready = collections.deque()
         cv = threading.Condition()
-        state = {"used": 0, "admitted": 0, "error": None}
+        state = {"used": 0, "error": None, "end": 0.0}
+        done_q: "queue.Queue" = queue.Queue()
         t0 = time.perf_counter()
 
         def stager():
@@ -107,23 +130,69 @@ class FlashMapServer:
                         wait = r.arrival - (time.perf_counter() - t0)
                         if wait > 0:
                             time.sleep(wait)
-                    need = staging_bytes(r, K, V)
+                    offs = list(range(0, r.n, PIECE)) if r.n else [0]
+                    r._left = len(offs)
+                    if r.kind == GET:
+                        if self.out_pool is not None:
+                            hv, hf = self.out_pool(r.n, V)
+                        else:
+                            hv = torch.empty((r.n, V), dtype=torch.uint8).pin_memory()
+                            hf = torch.empty((r.n,), dtype=torch.uint8).pin_memory()
+                        r._host = (hv, hf)
+                    for off in offs:
+                        n = min(PIECE, r.n - off)
+                        pc = _Piece(r, off, n, staging_bytes(r, K, V, n))
+                        with cv:
+                            while state["used"] > 0 and state["used"] + pc.need > self.budget:
+                                cv.wait()
+                            state["used"] += pc.need
+                        with torch.cuda.stream(self.copy_stream):
+                            pc.dk = torch.from_numpy(np.ascontiguousarray(r.keys[off:off + n])).to(
+                                self.dev, non_blocking=True)
+                            if r.kind == INSERT:
+                                pc.dv = torch.from_numpy(np.ascontiguousarray(r.values[off:off + n])).to(
+                                    self.dev, non_blocking=True)
+                            if r.kind == GET:
+                                pc.ov = torch.empty((n, V), dtype=torch.uint8, device=self.dev)
+                                pc.of = torch.empty((n,), dtype=torch.uint8, device=self.dev)
+                            pc.ev = torch.cuda.Event()
+                            pc.ev.record(self.copy_stream)
+                        with cv:
+                            ready.append(pc)
+                            cv.notify_all()
+            except Exception as e:  # pragma: no cover - surfaced by serve()
+                with cv:
+                    state["error"] = e
+                    cv.notify_all()
+
+        def completer():
+            try:
+                while True:
+                    item = done_q.get()
+                    if item is None:
+                        return
+                    ev, group, res = item
+                    if ev is not None:
+                        ev.synchronize()
+                    now = time.perf_counter() - t0
+                    freed = 0
+                    for pc, (cnt, st) in zip(group, res):
+                        r = pc.req
+                        r.result += cnt
+                        if st and not r.status:
+                            r.status = st
+                        r._left -= 1
+                        if r._left == 0:
+                            if r.kind == GET:
+                                hv, hf = r._host
+                                r.out_values, r.out_found = np.asarray(hv), np.asarray(hf)
+                                del r._host
+                            r.done = now
+                            state["end"] = max(state["end"], now)
+                        freed += pc.need
+                        pc.dk = pc.dv = pc.ov = pc.of = pc.ev = None
                     with cv:
-                        while state["used"] > 0 and state["used"] + need > self.budget:
-                            cv.wait()
-                        state["used"] += need
-                    with torch.cuda.stream(self.copy_stream):
-                        dk = torch.from_numpy(np.ascontiguousarray(r.keys)).to(self.dev, non_blocking=True)
-                        dv = (torch.from_numpy(np.ascontiguousarray(r.values)).to(self.dev, non_blocking=True)
-                              if r.kind == INSERT else None)
-                        ov = torch.empty((r.n, V), dtype=torch.uint8, device=self.dev) if r.kind == GET else None
-                        of = torch.empty((r.n,), dtype=torch.uint8, device=self.dev) if r.kind == GET else None
-                        ev = torch.cuda.Event()
-                        ev.record(self.copy_stream)
-                    r._dev = [dk, dv, ov, of, ev, need]
-                    with cv:
-                        ready.append(r)
-                        state["admitted"] += 1
+                        state["used"] -= freed
                         cv.notify_all()
             except Exception as e:  # pragma: no cover - surfaced by serve()
                 with cv:
@@ -131,78 +200,92 @@ class FlashMapServer:
                     cv.notify_all()
 
         th = threading.Thread(target=stager, daemon=True)
+        tc = threading.Thread(target=completer, daemon=True)
         th.start()
-        served = 0
-        end = t0
-        while served < len(requests):
-            with cv:
-                while not ready and state["error"] is None:
-                    cv.wait()
-                if state["error"] is not None:
-                    raise state["error"]
-                group = list(ready)
-                ready.clear()
-            for r in group:
-                self.stream.wait_event(r._dev[4])
-            if len(group) == 1:
-                # a lone request: the plain device call, without batch set-up
-                res = [self._run_one(group[0])]
-            else:
-                ops = [BatchOp(r.kind, self.t, r.n, r._dev[0], r._dev[1], r._dev[2], r._dev[3]) for r in group]
-                b = FlashMapBatch(ops)
-                b.run(self.stream)
-                res = b.wait()
-                b.close()
-            # results home: get outputs downloaded on the compute stream
-            outs = []
-            with torch.cuda.stream(self.stream):
-                for r in group:
-                    if r.kind == GET:
-                        if self.out_pool is not None:
-                            hv, hf = self.out_pool(r.n, V)
-                        else:
-                            hv = torch.empty((r.n, V), dtype=torch.uint8).pin_memory()
-                            hf = torch.empty((r.n,), dtype=torch.uint8).pin_memory()
-                        hv.copy_(r._dev[2], non_blocking=True)
-                        hf.copy_(r._dev[3], non_blocking=True)
-                        outs.append((r, hv, hf))
-            self.stream.synchronize()
-            now = time.perf_counter() - t0
-            freed = 0
-            for r, (cnt, st) in zip(group, res):
-                r.result, r.status, r.done = cnt, st, now
-                freed += r._dev[5]
-                r._dev = []
-            for r, hv, hf in outs:
-                r.out_values, r.out_found = hv.numpy(), hf.numpy()
-            with cv:
-                state["used"] -= freed
-                cv.notify_all()
-            served += len(group)
-            self.batches += 1
-            self.batch_sizes.append(len(group))
-            end = time.perf_counter()
+        tc.start()
+        total = sum(len(range(0, r.n, PIECE)) if r.n else 1 for r in requests)
+        ran = 0
+        cap = self.t.capacity()
+        try:
+            while ran < total:
+                with cv:
+                    while not ready and state["error"] is None:
+                        cv.wait()
+                    if state["error"] is not None:
+                        raise state["error"]
+                    group = list(ready)
+                    ready.clear()
+                    # the first piece of a multi-piece insert starts a group
+                    for idx in range(1, len(group)):
+                        if group[idx].off == 0 and group[idx].req.kind == INSERT and group[idx].req.n > PIECE:
+                            ready.extendleft(reversed(group[idx:]))
+                            del group[idx:]
+                            break
+                head = group[0]
+                if head.off == 0 and head.req.kind == INSERT and head.req.n > PIECE:
+                    # every earlier group has finished: len is exact here
+                    head.req._reject = self.t.len() + head.req.n > cap
+                skip = [pc for pc in group if getattr(pc.req, "_reject", False)]
+                if skip:
+                    done_q.put((None, skip, [(0, FM_ERR_TABLE_FULL)] * len(skip)))
+                    ran += len(skip)
+                    group = [pc for pc in group if not getattr(pc.req, "_reject", False)]
+                    if not group:
+                        continue
+                for pc in group:
+                    self.stream.wait_event(pc.ev)
+                if len(group) == 1:
+                    # a lone piece: the plain device call, without batch set-up
+                    res = [self._run_one(group[0])]
+                else:
+                    ops = [BatchOp(pc.req.kind, self.t, pc.n, pc.dk, pc.dv, pc.ov, pc.of) for pc in group]
+                    b = FlashMapBatch(ops)
+                    b.run(self.stream)
+                    res = b.wait()
+                    b.close()
+                # get results go down behind the group, on their own stream
+                ev = None
+                gets = [pc for pc in group if pc.req.kind == GET]
+                if gets:
+                    done_compute = torch.cuda.Event()
+                    done_compute.record(self.stream)
+                    self.down_stream.wait_event(done_compute)
+                    with torch.cuda.stream(self.down_stream):
+                        for pc in gets:
+                            hv, hf = pc.req._host
+                            hv[pc.off:pc.off + pc.n].copy_(pc.ov, non_blocking=True)
+                            hf[pc.off:pc.off + pc.n].copy_(pc.of, non_blocking=True)
+                    ev = torch.cuda.Event()
+                    ev.record(self.down_stream)
+                done_q.put((ev, group, res))
+                ran += len(group)
+                self.batches += 1
+                self.batch_sizes.append(len(group))
+        finally:
+            done_q.put(None)
+            tc.join()
         th.join()
-        return end - t0
+        if state["error"] is not None:
+            raise state["error"]
+        return state["end"]
 
-
-    def _run_one(self, r: Request):
-        """A lone request: the device-pointer call on the compute stream, with
+    def _run_one(self, pc: _Piece):
+        """A lone piece: the device-pointer call on the compute stream, with
         TableFull and the probe limit reported as the op's status, as a batch
         reports them; any other failure raises."""
         import ctypes as C
 
         from .map import _dev_ptr
 
-        dk, dv, ov, of = r._dev[:4]
         L, h, s = self.t._L, self.t._h, self.stream.cuda_stream
         out = C.c_uint64(0)
-        if r.kind == GET:
-            rc = L.fm_bulk_get_device(h, _dev_ptr(dk), r.n, _dev_ptr(ov), _dev_ptr(of), s)
-        elif r.kind == INSERT:
-            rc = L.fm_bulk_insert_device(h, _dev_ptr(dk), _dev_ptr(dv), r.n, C.byref(out), s)
+        kind = pc.req.kind
+        if kind == GET:
+            rc = L.fm_bulk_get_device(h, _dev_ptr(pc.dk), pc.n, _dev_ptr(pc.ov), _dev_ptr(pc.of), s)
+        elif kind == INSERT:
+            rc = L.fm_bulk_insert_device(h, _dev_ptr(pc.dk), _dev_ptr(pc.dv), pc.n, C.byref(out), s)
         else:
-            rc = L.fm_bulk_remove_device(h, _dev_ptr(dk), r.n, C.byref(out), s)
+            rc = L.fm_bulk_remove_device(h, _dev_ptr(pc.dk), pc.n, C.byref(out), s)
         if rc in (FM_ERR_TABLE_FULL, FM_ERR_PROBE_LIMIT):
             return 0, rc
         self.t._check(rc)

@@ -37,10 +37,18 @@ def make_requests(seed, ks, vs, present, n_req=240, rate=20000.0, sizes=(16, 200
     return reqs
 
 
+@pytest.mark.parametrize("piece", [None, 1000])
 @pytest.mark.parametrize("shape", [(32, 128), (8, 8)])
-def test_served_results_equal_arrival_order_replay(shape):
+def test_served_results_equal_arrival_order_replay(shape, piece, monkeypatch):
+    """piece=1000: requests go through the server in pieces of 1000 keys
+    (multi-piece gets, removes and inserts, the whole-request TableFull
+    precheck of a pieced insert)."""
     import flash_map as F
+    import flash_map.serve as S
     from flash_map.serve import FlashMapServer
+
+    if piece:
+        monkeypatch.setattr(S, "PIECE", piece)
 
     ks, vs = shape
     cap = 1 << 18
