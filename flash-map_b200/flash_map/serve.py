@@ -111,6 +111,34 @@ class FlashMapServer:
         self.batches = 0
         self.batch_sizes: List[int] = []
 
+    def warmup(self) -> None:
+        """Runs each kind of op, alone and as a batch, on a small scratch
+        table of the same record sizes, so that first-use costs (kernel
+        loading, the batch buffers) fall outside served requests.  The served
+        table is not touched."""
+        torch = self.torch
+        K, V = self.t.key_size, self.t.value_size
+        scratch = FlashMap(1 << 12, K, V, device_id=self.t.device())
+        try:
+            g = torch.Generator(device=self.dev)
+            g.manual_seed(0)
+            k = torch.randint(0, 256, (512, K), dtype=torch.uint8, device=self.dev, generator=g)
+            v = torch.randint(0, 256, (512, V), dtype=torch.uint8, device=self.dev, generator=g)
+            ov = torch.empty((512, V), dtype=torch.uint8, device=self.dev)
+            of = torch.empty((512,), dtype=torch.uint8, device=self.dev)
+            scratch.bulk_insert_device(k, v, 256, self.stream)
+            scratch.bulk_get_device(k, 512, ov, of, self.stream)
+            scratch.bulk_remove_device(k, 64, self.stream)
+            ops = [BatchOp(INSERT, scratch, 256, k[256:], v[256:]), BatchOp(GET, scratch, 512, k, None, ov, of),
+                   BatchOp(REMOVE, scratch, 64, k[64:])]
+            b = FlashMapBatch(ops)
+            b.run(self.stream)
+            b.wait()
+            b.close()
+            self.stream.synchronize()
+        finally:
+            scratch.close()
+
     def serve(self, requests: List[Request], realtime: bool = True) -> float:
         """Serves `requests` (sorted by arrival; arrival times in seconds from
         the start).  realtime: a request is admitted no earlier than its

@@ -60,6 +60,7 @@ def test_served_results_equal_arrival_order_replay(shape, piece, monkeypatch):
     assert g.bulk_insert(pk, pv) == o.bulk_insert(pk, pv)
     reqs = make_requests(6, ks, vs, pk)
     srv = FlashMapServer(g, budget=64 << 20)
+    srv.warmup()  # must leave the served table as it is
     srv.serve(reqs, realtime=True)
     assert srv.batches < len(reqs)  # requests were coalesced into batches
     for i, r in enumerate(reqs):
