@@ -218,10 +218,10 @@ struct TimerScope {
 int ensure_scratch(fm_table* t, uint64_t n) {
     if (t->sc.cap_ops >= n) return FM_OK;
     // pend[0], pend[1] (u32) | op_slot (u64) | op_word (u32) | op_flag (u8) | op_pt (PT_MAX u32) |
-    // long_list (u32) per op, then the component buffer (per table)
+    // long_list (u32) per op, then the component buffer and the remove chunk summaries (per table)
     const uint64_t per_op = 4 + 4 + 8 + 4 + 1 + 4 * fm::PT_MAX + 4;
     const uint64_t want = n + n / 4 + 1024;
-    const size_t bytes = (size_t)(want * per_op + 8 * 256 + fm::cmp_bytes(t->mask));
+    const size_t bytes = (size_t)(want * per_op + 9 * 256 + fm::cmp_bytes(t->mask) + 4 * fm::rsum_words(t->mask));
     if (t->sc_base) cudaFree(t->sc_base);
     t->sc_base = nullptr;
     t->sc = OpScratch{};
@@ -241,10 +241,13 @@ int ensure_scratch(fm_table* t, uint64_t n) {
     t->sc.op_flag = carve(want);
     t->sc.long_list = (uint32_t*)carve(want * 4);
     t->sc.comp = carve(fm::cmp_bytes(t->mask));
+    t->sc.rsum = (uint32_t*)carve(4 * fm::rsum_words(t->mask));
     t->sc.cap_ops = want;
     t->sc_bytes = bytes;
     // op_word doubles as the insert inflow bound: idle value 0xFFFFFFFF.
     e = cudaMemsetAsync(t->sc.op_word, 0xFF, want * 4, t->stream);
+    // the remove chunk marks: IDLE between calls
+    if (e == cudaSuccess) e = cudaMemsetAsync(t->sc.rsum, 0xFF, 4 * fm::rsum_words(t->mask), t->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_GPU_ALLOC, "scratch init", e);
     return FM_OK;
@@ -276,6 +279,7 @@ int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t
         const uint8_t* kk = d_k + base * t->ksz;
         const uint8_t* vv = d_v ? d_v + base * t->vsz : nullptr;
         cudaError_t e = cudaMemsetAsync(t->d_ctl, 0, fm::CTL_CALL_BYTES, s);
+        if (e == cudaSuccess && !insert) e = fm::launch_rem_summary(v, t->sc, t->d_ctl, s);
         if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "round setup", e);
         uint32_t r = 0;
         uint32_t left = m;
@@ -1248,6 +1252,10 @@ int batch_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
                                         hd[k].ctl, s);
                 if (e == cudaSuccess) e = cudaMemsetAsync(&hd[k].ctl->n0, 0, sizeof(uint32_t), s);
             }
+        } else {
+            // removes: each member's chunk summaries (built when its windows are long)
+            const auto* hd = reinterpret_cast<const fm::GroupOp*>(b->h_desc + g.desc_off);
+            for (uint32_t k = 0; e == cudaSuccess && k < n; k++) e = fm::launch_rem_summary(hd[k].t, hd[k].sc, hd[k].ctl, s);
         }
         uint32_t r = 0;
         if (adaptive) {

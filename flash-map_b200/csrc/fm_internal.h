@@ -29,6 +29,8 @@ struct Ctl {
     uint32_t nlong[2];       // inserts deferred to the warp-per-op pass, per round parity
     uint32_t n0;             // grouped (batch) calls: the call's op count after the precheck
     uint32_t tail_handoff;   // insert tail: 1 + the round it left pending for the host (0: none)
+    uint32_t rsum_on;        // remove: the chunk summaries (OpScratch::rsum) are built for this call
+    uint32_t pad_[3];
     unsigned long long count;  // new keys (insert) / removed keys (remove), single-block kernels
     unsigned long long count_part[COUNT_PARTS][4];  // the same from grid kernels, [i][0] used
     // Persistent table facts (survive across calls, reset by clear):
@@ -41,7 +43,7 @@ struct Ctl {
         return s;
     }
 };
-constexpr size_t CTL_CALL_BYTES = 48 + 32 * COUNT_PARTS;  // npend .. count_part
+constexpr size_t CTL_CALL_BYTES = 64 + 32 * COUNT_PARTS;  // npend .. count_part
 static_assert(offsetof(Ctl, dmax) == CTL_CALL_BYTES, "Ctl layout");
 
 // Op status codes written by device code (the FM_* values of the C ABI).
@@ -64,8 +66,15 @@ struct OpScratch {
     uint32_t* op_pt;     // remove: up to PT_MAX potential-target distances per op
     uint32_t* long_list; // insert: ops of this round deferred to the warp-per-op pass
     uint8_t* comp;       // insert: component buffer (cmp_bytes of the table; null: none)
+    uint32_t* rsum;      // remove: per 32-slot chunk, a metadata summary then the least mark
+                         //   (rsum_words of the table; marks IDLE between calls; null: none)
     uint64_t cap_ops;
 };
+
+// Remove chunk summaries: for each chunk of 32 slots, (has an EMPTY slot) << 31
+// | largest stored distance, then the least op index marking a slot of it.
+__host__ __device__ inline uint64_t rsum_chunks(uint64_t mask) { return (mask + 32) >> 5; }
+__host__ __device__ inline uint64_t rsum_words(uint64_t mask) { return 2 * rsum_chunks(mask); }
 
 // Component buffer of the one-at-a-time insert path: a 256-byte header, then
 // 32 bytes per chunk of CMP_CHUNK slots.  CMP_N0_CTL as a call's op count:
@@ -114,6 +123,10 @@ cudaError_t launch_rem_rounds(const TableView& t, Shape sh, const uint8_t* keys,
                               uint32_t nrounds, uint32_t grid_ops, const OpScratch& sc, Ctl* ctl, cudaStream_t s);
 cudaError_t launch_rem_tail(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, uint32_t r,
                             const OpScratch& sc, Ctl* ctl, cudaStream_t s);
+// Builds the chunk summaries of a remove call (after its control block is
+// reset) when the table's largest stored distance makes the windows long;
+// the call's kernels then skip chunks that cannot matter.
+cudaError_t launch_rem_summary(const TableView& t, const OpScratch& sc, Ctl* ctl, cudaStream_t s);
 cudaError_t launch_count(const TableView& t, Ctl* ctl, cudaStream_t s);
 int num_sms();
 unsigned long long launch_count();

@@ -28,13 +28,48 @@ __device__ __forceinline__ uint64_t home_of(const TableView& t, const uint8_t* k
     return key.hash(ksz, t.hash_mode) & t.mask;
 }
 
+// The call's chunk summaries, or null when the call did not build them.
+__device__ __forceinline__ uint32_t* rsum_of(const OpScratch& sc, const Ctl* ctl) {
+    return *(volatile const uint32_t*)&ctl->rsum_on ? sc.rsum : nullptr;
+}
+
+// Below this largest stored distance the windows are short: no summaries.
+constexpr uint32_t RSUM_MIN_DMAX = 64;
+
+// Chunk summaries of a remove call, once per call (capacity >= 32): per 32
+// slots whether one is EMPTY and the largest stored distance.  Removes make
+// no EMPTY slot and only lower distances, so they stay valid bounds for the
+// whole call.
+__global__ void __launch_bounds__(256) k_rem_sum(TableView t, OpScratch sc, Ctl* ctl) {
+    if (*(volatile const uint32_t*)&ctl->dmax < RSUM_MIN_DMAX) return;  // grid-uniform
+    const uint64_t nch = rsum_chunks(t.mask);
+    const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c == 0) ctl->rsum_on = 1u;
+    if (c >= nch) return;
+    const uint4* p = reinterpret_cast<const uint4*>(t.flags + c * 32);
+    uint32_t md = 0;
+    bool empty = false;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        const uint4 w = p[q];
+        const uint32_t f4[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int l = 0; l < 4; l++) {
+            const uint32_t st = st_of(f4[l]);
+            if (st == ST_EMPTY) empty = true;
+            else if (st == ST_OCC) md = max(md, (uint32_t)dist_of(f4[l]));
+        }
+    }
+    sc.rsum[c] = (empty ? 0x80000000u : 0u) | md;
+}
+
 // Phase 1 for op j: probe, then mark every possible target.  With capacity
 // >= 8 the metadata is read in aligned 8-slot windows (two 16-byte loads, one
 // 32-byte sector) and scanned in registers; key compares happen only where
 // the stored distance equals the probe depth.
 template <int KB>
 __device__ __forceinline__ void scan_op(const TableView& t, const uint8_t* keys, uint32_t j, uint64_t dmax,
-                                        const OpScratch& sc) {
+                                        const OpScratch& sc, const uint32_t* rs) {
     const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
     const uint64_t mask = t.mask;
     RegKey<KB> key;
@@ -46,6 +81,7 @@ __device__ __forceinline__ void scan_op(const TableView& t, const uint8_t* keys,
     uint64_t wend = NONE64;
     auto mark = [&](uint64_t q) {
         atomicMin(&t.seg_min[(h + q) & mask], j);
+        if (rs) atomicMin(const_cast<uint32_t*>(rs) + rsum_chunks(mask) + (((h + q) & mask) >> 5), j);
         if (npt < PT_MAX) sc.op_pt[(uint64_t)j * PT_MAX + npt] = (uint32_t)q;
         ++npt;
     };
@@ -93,6 +129,32 @@ __device__ __forceinline__ void scan_op(const TableView& t, const uint8_t* keys,
             // 2. later copies of the key up to the bound (windows again)
             const uint64_t q0 = (tp != NONE64 ? tp : p) + 1;
             bool done = q0 > lim;
+            if (rs) {
+                // chunk by chunk: a chunk without an EMPTY slot whose largest
+                // stored distance is below the depth reached holds no copy
+                for (uint64_t q = q0; !done && q <= lim;) {
+                    const uint64_t s0 = (h + q) & mask;
+                    const uint64_t qe = min(q + (31 - (s0 & 31)), lim);  // this chunk's last depth in the window
+                    const uint32_t sm = rs[s0 >> 5];
+                    if (!(sm >> 31) && (uint64_t)(sm & 0x7FFFFFFFu) < q) {
+                        wend = qe;
+                        q = qe + 1;
+                        continue;
+                    }
+                    for (; q <= qe; ++q) {
+                        const uint64_t s = (h + q) & mask;
+                        const uint32_t f = t.flags[s];
+                        const uint32_t st = st_of(f);
+                        if (st == ST_EMPTY) {
+                            done = true;
+                            break;
+                        }
+                        wend = q;
+                        if (st == ST_OCC && dist_matches(f, q) && key.eq(t.keys + s * ksz, ksz)) mark(q);
+                    }
+                }
+                done = true;
+            }
             for (uint64_t wb = (h + q0) & ~7ull; !done; wb += 8) {
                 const uint4* fp = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
                 const uint4 a = fp[0], b = fp[1];
@@ -159,13 +221,27 @@ __device__ __forceinline__ void scan_op(const TableView& t, const uint8_t* keys,
 // aligned 4-slot groups of marks with capacity >= 4).
 template <int KB>
 __device__ __forceinline__ bool check_op(const TableView& t, const uint8_t* keys, uint32_t j, const OpScratch& sc,
-                                         uint32_t& removed) {
+                                         uint32_t& removed, const uint32_t* rs) {
     const uint64_t mask = t.mask;
     const uint32_t wend = sc.op_word[j];
     if (wend != IDLE) {
         RegKey<KB> key;
         const uint64_t h = home_of<KB>(t, keys, j, key);
-        if (mask >= 3) {
+        if (rs) {
+            // a chunk's least mark first: slots only where it is below j and
+            // the chunk is cut by the window's ends
+            const uint32_t* cm = rs + rsum_chunks(mask);
+            for (uint64_t q = 0; q <= wend;) {
+                const uint64_t s0 = (h + q) & mask;
+                const uint64_t qe = min(q + (31 - (s0 & 31)), (uint64_t)wend);
+                if (cm[s0 >> 5] < j) {
+                    if ((s0 & 31) == 0 && qe == q + 31) return false;
+                    for (uint64_t x = q; x <= qe; ++x)
+                        if (t.seg_min[(h + x) & mask] < j) return false;
+                }
+                q = qe + 1;
+            }
+        } else if (mask >= 3) {
             const uint64_t last = h + wend;
             for (uint64_t wb = h & ~3ull; wb <= last; wb += 4) {
                 const uint4 m = *reinterpret_cast<const uint4*>(t.seg_min + (wb & mask));
@@ -189,7 +265,8 @@ __device__ __forceinline__ bool check_op(const TableView& t, const uint8_t* keys
 
 // Phase 3 for op j: clear its marks and its window word.
 template <int KB>
-__device__ __forceinline__ void reset_op(const TableView& t, const uint8_t* keys, uint32_t j, const OpScratch& sc) {
+__device__ __forceinline__ void reset_op(const TableView& t, const uint8_t* keys, uint32_t j, const OpScratch& sc,
+                                         uint32_t* rs) {
     const uint64_t mask = t.mask;
     const uint32_t npt = sc.op_flag[j];
     const uint32_t wend = sc.op_word[j];
@@ -197,12 +274,20 @@ __device__ __forceinline__ void reset_op(const TableView& t, const uint8_t* keys
     if (npt == 0) return;
     RegKey<KB> key;
     const uint64_t h = home_of<KB>(t, keys, j, key);
+    uint32_t* cm = rs ? rs + rsum_chunks(mask) : nullptr;
     if (npt <= PT_MAX) {
-        for (uint32_t k = 0; k < npt; k++) t.seg_min[(h + sc.op_pt[(uint64_t)j * PT_MAX + k]) & mask] = IDLE;
+        for (uint32_t k = 0; k < npt; k++) {
+            const uint64_t s = (h + sc.op_pt[(uint64_t)j * PT_MAX + k]) & mask;
+            t.seg_min[s] = IDLE;
+            if (cm) cm[s >> 5] = IDLE;
+        }
     } else {
         for (uint64_t q = 0; q <= wend; ++q) {
             const uint64_t s = (h + q) & mask;
-            if (t.seg_min[s] != IDLE) t.seg_min[s] = IDLE;
+            if (t.seg_min[s] != IDLE) {
+                t.seg_min[s] = IDLE;
+                if (cm) cm[s >> 5] = IDLE;
+            }
         }
     }
 }
@@ -213,8 +298,9 @@ __global__ void __launch_bounds__(RBLOCK) k_rem_p1(TableView t, const uint8_t* _
     const RoundOps ops = round_ops(sc, ctl, r, n0);
     if (blockIdx.x == 0 && threadIdx.x == 0) reset_next_round(ctl, r);
     const uint64_t dmax = *(volatile uint32_t*)&ctl->dmax;
+    const uint32_t* rs = rsum_of(sc, ctl);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ops.n; i += gridDim.x * blockDim.x)
-        scan_op<KB>(t, keys, ops.op(i), dmax, sc);
+        scan_op<KB>(t, keys, ops.op(i), dmax, sc, rs);
 }
 
 template <int KB>
@@ -229,6 +315,7 @@ __global__ void __launch_bounds__(RBLOCK) k_rem_p2(TableView t, const uint8_t* _
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t iters = grid_iters(ops.n);
+    const uint32_t* rs = rsum_of(sc, ctl);
     uint32_t removed = 0;
     for (uint32_t it = 0; it < iters; it++) {
         const uint32_t i = i0 + it * stride;
@@ -237,7 +324,7 @@ __global__ void __launch_bounds__(RBLOCK) k_rem_p2(TableView t, const uint8_t* _
         bool ran = false;
         if (valid) {
             j = ops.op(i);
-            ran = check_op<KB>(t, keys, j, sc, removed);
+            ran = check_op<KB>(t, keys, j, sc, removed, rs);
         }
         block_append(out, out_n, j, valid && !ran, s_app);
     }
@@ -249,8 +336,9 @@ template <int KB>
 __global__ void __launch_bounds__(RBLOCK) k_rem_p3(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
                                                    uint32_t r, OpScratch sc, Ctl* ctl) {
     const RoundOps ops = round_ops(sc, ctl, r, n0);
+    uint32_t* rs = rsum_of(sc, ctl);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ops.n; i += gridDim.x * blockDim.x)
-        reset_op<KB>(t, keys, ops.op(i), sc);
+        reset_op<KB>(t, keys, ops.op(i), sc, rs);
 }
 
 template <int KB>
@@ -262,6 +350,7 @@ __device__ __forceinline__ void rem_tail_body(const TableView& t, const uint8_t*
     uint32_t n = s_n;
     if (n == 0 || n > limit) return;
     const uint64_t dmax = *(volatile uint32_t*)&ctl->dmax;
+    uint32_t* rs = rsum_of(sc, ctl);
     uint32_t removed = 0, rounds = 0;
     uint32_t r = r0;
     bool stuck = false;
@@ -270,14 +359,14 @@ __device__ __forceinline__ void rem_tail_body(const TableView& t, const uint8_t*
         uint32_t* out = pend_of(sc, r + 1);
         if (threadIdx.x == 0) s_next = 0;
         __syncthreads();
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) scan_op<KB>(t, keys, in ? in[i] : i, dmax, sc);
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) scan_op<KB>(t, keys, in ? in[i] : i, dmax, sc, rs);
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
             const uint32_t j = in ? in[i] : i;
-            if (!check_op<KB>(t, keys, j, sc, removed)) out[atomicAdd(&s_next, 1u)] = j;
+            if (!check_op<KB>(t, keys, j, sc, removed, rs)) out[atomicAdd(&s_next, 1u)] = j;
         }
         __syncthreads();
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) reset_op<KB>(t, keys, in ? in[i] : i, sc);
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) reset_op<KB>(t, keys, in ? in[i] : i, sc, rs);
         __syncthreads();
         const uint32_t nn = s_next;
         ++r;
@@ -328,7 +417,7 @@ __global__ void __launch_bounds__(RBLOCK) k_grp_rem_p1(const GroupOp* __restrict
         const GroupOp& g = ops[o];
         const uint32_t i = f - s_pre[o];
         const uint32_t j = r == 0 ? i : pend_of(g.sc, r)[i];
-        scan_op<KB>(g.t, g.keys, j, *(volatile uint32_t*)&g.ctl->dmax, g.sc);
+        scan_op<KB>(g.t, g.keys, j, *(volatile uint32_t*)&g.ctl->dmax, g.sc, rsum_of(g.sc, g.ctl));
     }
 }
 
@@ -345,7 +434,7 @@ __global__ void __launch_bounds__(RBLOCK) k_grp_rem_p2(const GroupOp* __restrict
         const uint32_t i = f - s_pre[o];
         const uint32_t j = r == 0 ? i : pend_of(g.sc, r)[i];
         uint32_t removed = 0;
-        const bool ran = check_op<KB>(g.t, g.keys, j, g.sc, removed);
+        const bool ran = check_op<KB>(g.t, g.keys, j, g.sc, removed, rsum_of(g.sc, g.ctl));
         append_peer(pend_of(g.sc, r + 1), &g.ctl->npend[(r + 1) & 1], j, !ran, o);
         add_peer(g.ctl, removed, o);
     }
@@ -360,7 +449,7 @@ __global__ void __launch_bounds__(RBLOCK) k_grp_rem_p3(const GroupOp* __restrict
         const GroupOp& g = ops[o];
         const uint32_t i = f - s_pre[o];
         const uint32_t j = r == 0 ? i : pend_of(g.sc, r)[i];
-        reset_op<KB>(g.t, g.keys, j, g.sc);
+        reset_op<KB>(g.t, g.keys, j, g.sc, rsum_of(g.sc, g.ctl));
     }
 }
 
@@ -453,6 +542,16 @@ cudaError_t launch_grp_rem(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t
         case SHAPE_32_32: grp_rem_shape<32>(ops, nops, sum_n, phase, r0, nrounds, s); break;
         default: grp_rem_shape<0>(ops, nops, sum_n, phase, r0, nrounds, s); break;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rem_summary(const TableView& t, const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+    // chunks are whole (capacity >= 32) and depths stay below the 28-bit
+    // stored distance, so a depth compares exactly with the largest one
+    if (!sc.rsum || t.mask < 31 || t.mask >= (1ull << 28)) return cudaSuccess;
+    const uint64_t nch = rsum_chunks(t.mask);
+    k_rem_sum<<<(unsigned)((nch + 255) / 256), 256, 0, s>>>(t, sc, ctl);
+    count_launches(1);
     return cudaGetLastError();
 }
 

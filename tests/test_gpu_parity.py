@@ -465,3 +465,33 @@ def test_host_api_pieces_pinned_buffers():
     rm = torch.from_numpy(keys[rng.choice(n, 100_000, replace=False)]).pin_memory().numpy()
     assert g.bulk_remove(rm) == o.bulk_remove(np.array(rm))
     assert_same_layout(g, o)
+
+
+@pytest.mark.parametrize("shape", [(8, 8), (32, 128)])
+def test_remove_long_windows_chunk_summaries(shape):
+    """Removes where the largest stored distance is in the hundreds (load
+    0.97 after churn that reuses tombstones, so keys can have copies past a
+    probe's exit): the remove windows run long and the kernels skip chunks by
+    their summaries.  Big batches with in-batch duplicates and absent keys;
+    counts, gets and the full layout after every call."""
+    ks, vs = shape
+    cap = 1 << 16
+    rng = np.random.default_rng(97 + ks)
+    g = gpu_map(cap, ks, vs)
+    o = OracleAdapter(cap, ks, vs)
+    keys = rng.integers(0, 256, (int(cap * 0.97), ks), dtype=np.uint8)
+    vals = rng.integers(0, 256, (len(keys), vs), dtype=np.uint8)
+    assert g.bulk_insert(keys, vals) == o.bulk_insert(keys, vals)
+    for r in range(3):
+        rm = keys[rng.choice(len(keys), len(keys) // 10, replace=False)]
+        assert g.bulk_remove(rm) == o.bulk_remove(rm)
+        back = np.concatenate([rm[: len(rm) // 2], rng.integers(0, 256, (len(rm) // 3, ks), dtype=np.uint8)])
+        bv = rng.integers(0, 256, (len(back), vs), dtype=np.uint8)
+        assert g.bulk_insert(back, bv) == o.bulk_insert(back, bv)
+        assert_same_layout(g, o)
+    big = keys[rng.integers(0, len(keys), len(keys) // 2)]  # repeats: in-batch duplicates
+    big = np.concatenate([big, rng.integers(0, 256, (5000, ks), dtype=np.uint8)])
+    big = big[rng.permutation(len(big))]
+    assert g.bulk_remove(big) == o.bulk_remove(big)
+    assert_same_layout(g, o)
+    assert_same_gets(g, o, keys[:20000])
