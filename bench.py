@@ -627,6 +627,11 @@ def served_leg(torch, F, dev, scale=1):
     pinned host pools (inserts: fresh keys; gets/removes: the skewed mix)."""
     from flash_map.serve import FlashMapServer, PlainServer, Request, latency_summary
 
+    # earlier legs' buffers and the allocator's cached blocks go first: under
+    # memory pressure one staging allocation can stall the host for 100 ms
+    gc.collect()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
     rng = np.random.default_rng(6)
     g = torch.Generator(device=dev)
     g.manual_seed(6)

@@ -111,13 +111,21 @@ class FlashMapServer:
         self.batches = 0
         self.batch_sizes: List[int] = []
 
-    def warmup(self) -> None:
+    def warmup(self, staging_bytes: int = 2 << 30) -> None:
         """Runs each kind of op, alone and as a batch, on a small scratch
         table of the same record sizes, so that first-use costs (kernel
-        loading, the batch buffers) fall outside served requests.  The served
-        table is not touched."""
+        loading, the batch buffers) fall outside served requests, and leaves
+        `staging_bytes` of device blocks cached for the copy stream's staging
+        allocations (a fresh allocation while the device is busy and nearly
+        full can stall the stager for tens of milliseconds).  The served table
+        is not touched."""
         torch = self.torch
         K, V = self.t.key_size, self.t.value_size
+        with torch.cuda.stream(self.copy_stream):
+            block = 64 << 20
+            held = [torch.empty(block, dtype=torch.uint8, device=self.dev)
+                    for _ in range(max(1, min(staging_bytes, self.budget) // block))]
+            del held  # cached by the allocator for this stream
         scratch = FlashMap(1 << 12, K, V, device_id=self.t.device())
         try:
             g = torch.Generator(device=self.dev)
