@@ -85,19 +85,63 @@ def staging_bytes(r: Request, key_size: int, value_size: int, n: Optional[int] =
 
 class _Piece:
     """Keys [off, off + n) of a request, staged on the device."""
-    __slots__ = ("req", "off", "n", "dk", "dv", "ov", "of", "ev", "need")
+    __slots__ = ("req", "off", "n", "dk", "dv", "ov", "of", "ev", "need", "in_ring")
 
     def __init__(self, req, off, n, need):
         self.req, self.off, self.n, self.need = req, off, n, need
         self.dk = self.dv = self.ov = self.of = self.ev = None
+        self.in_ring = False
+
+
+def _al(nbytes: int) -> int:
+    return (nbytes + 255) & ~255
+
+
+class _Ring:
+    """First-in first-out space in one device buffer.  Pieces are released
+    in the order they were staged (groups complete in order), so the free
+    space is the ring between the newest and the oldest live piece."""
+
+    def __init__(self, buf):
+        self.buf = buf
+        self.size = buf.numel()
+        self.live = collections.deque()  # offsets, oldest first
+        self.head = 0
+
+    def take(self, need: int) -> Optional[int]:
+        if not self.live:
+            off = 0
+        else:
+            tail = self.live[0]
+            if self.head > tail:  # live [tail, head): free at the end, then before tail
+                if self.head + need <= self.size:
+                    off = self.head
+                elif need <= tail:
+                    off = 0
+                else:
+                    return None
+            elif self.head + need <= tail:  # wrapped: free [head, tail)
+                off = self.head
+            else:
+                return None
+        self.live.append(off)
+        self.head = off + need
+        return off
+
+    def give(self) -> None:
+        self.live.popleft()
+        if not self.live:
+            self.head = 0
 
 
 class FlashMapServer:
     """Continuous batching over one FlashMap.  `budget` bounds the device
-    bytes staged for admitted, unfinished pieces; a piece larger than the
-    whole budget is served alone once everything before it has finished."""
+    bytes staged for admitted, unfinished pieces: they are carved from a
+    staging buffer of min(budget, ring_bytes) bytes that the server owns; a
+    piece larger than it is served alone once everything before it has
+    finished."""
 
-    def __init__(self, table: FlashMap, budget: int = 20 << 30, out_pool=None):
+    def __init__(self, table: FlashMap, budget: int = 20 << 30, out_pool=None, ring_bytes: int = 4 << 30):
         import torch
 
         self.t = table
@@ -105,27 +149,25 @@ class FlashMapServer:
         self.torch = torch
         self.dev = torch.device("cuda", table.device())
         self.copy_stream = torch.cuda.Stream(self.dev)
+        # staging space owned by the server (min(budget, ring_bytes)): pieces
+        # are carved from it, so staging never waits on the framework's
+        # allocator; a piece larger than it is staged on its own
+        with torch.cuda.stream(self.copy_stream):
+            self._ring = _Ring(torch.empty(max(256, min(budget, ring_bytes)) & ~255, dtype=torch.uint8,
+                                           device=self.dev))
         self.stream = torch.cuda.Stream(self.dev)
         self.down_stream = torch.cuda.Stream(self.dev)
         self.out_pool = out_pool  # optional callable(n, V) -> (pinned vals, pinned found) for get results
         self.batches = 0
         self.batch_sizes: List[int] = []
 
-    def warmup(self, staging_bytes: int = 2 << 30) -> None:
+    def warmup(self) -> None:
         """Runs each kind of op, alone and as a batch, on a small scratch
         table of the same record sizes, so that first-use costs (kernel
-        loading, the batch buffers) fall outside served requests, and leaves
-        `staging_bytes` of device blocks cached for the copy stream's staging
-        allocations (a fresh allocation while the device is busy and nearly
-        full can stall the stager for tens of milliseconds).  The served table
-        is not touched."""
+        loading, the batch buffers) fall outside served requests.  The served
+        table is not touched."""
         torch = self.torch
         K, V = self.t.key_size, self.t.value_size
-        with torch.cuda.stream(self.copy_stream):
-            block = 64 << 20
-            held = [torch.empty(block, dtype=torch.uint8, device=self.dev)
-                    for _ in range(max(1, min(staging_bytes, self.budget) // block))]
-            del held  # cached by the allocator for this stream
         scratch = FlashMap(1 << 12, K, V, device_id=self.t.device())
         try:
             g = torch.Generator(device=self.dev)
@@ -157,6 +199,7 @@ class FlashMapServer:
         cv = threading.Condition()
         state = {"used": 0, "error": None, "end": 0.0}
         done_q: "queue.Queue" = queue.Queue()
+        ring = self._ring
         t0 = time.perf_counter()
 
         def stager():
@@ -178,19 +221,36 @@ class FlashMapServer:
                     for off in offs:
                         n = min(PIECE, r.n - off)
                         pc = _Piece(r, off, n, staging_bytes(r, K, V, n))
+                        parts = [n * K] + ([n * V] if r.kind == INSERT else []) + (
+                            [n * V, n] if r.kind == GET else [])
+                        rneed = sum(_al(x) for x in parts)
+                        at = None
                         with cv:
-                            while state["used"] > 0 and state["used"] + pc.need > self.budget:
-                                cv.wait()
-                            state["used"] += pc.need
+                            if rneed <= ring.size:
+                                # (after a piece staged alone, nothing until it is done)
+                                while state["used"] > 0 or (at := ring.take(rneed)) is None:
+                                    cv.wait()
+                                pc.in_ring = True
+                            else:  # alone: once everything staged before it is done
+                                while ring.live or state["used"] > 0:
+                                    cv.wait()
+                                state["used"] += pc.need
                         with torch.cuda.stream(self.copy_stream):
-                            pc.dk = torch.from_numpy(np.ascontiguousarray(r.keys[off:off + n])).to(
-                                self.dev, non_blocking=True)
+                            if at is not None:
+                                views = []
+                                for x in parts:
+                                    views.append(ring.buf[at:at + x])
+                                    at += _al(x)
+                            else:
+                                views = [torch.empty(x, dtype=torch.uint8, device=self.dev) for x in parts]
+                            pc.dk = views[0].view(n, K)
+                            pc.dk.copy_(torch.from_numpy(np.ascontiguousarray(r.keys[off:off + n])), non_blocking=True)
                             if r.kind == INSERT:
-                                pc.dv = torch.from_numpy(np.ascontiguousarray(r.values[off:off + n])).to(
-                                    self.dev, non_blocking=True)
+                                pc.dv = views[1].view(n, V)
+                                pc.dv.copy_(torch.from_numpy(np.ascontiguousarray(r.values[off:off + n])),
+                                            non_blocking=True)
                             if r.kind == GET:
-                                pc.ov = torch.empty((n, V), dtype=torch.uint8, device=self.dev)
-                                pc.of = torch.empty((n,), dtype=torch.uint8, device=self.dev)
+                                pc.ov, pc.of = views[1].view(n, V), views[2]
                             pc.ev = torch.cuda.Event()
                             pc.ev.record(self.copy_stream)
                         with cv:
@@ -212,6 +272,7 @@ class FlashMapServer:
                         ev.synchronize()
                     now = time.perf_counter() - t0
                     freed = 0
+                    given = 0
                     for pc, (cnt, st) in zip(group, res):
                         r = pc.req
                         r.result += cnt
@@ -225,9 +286,14 @@ class FlashMapServer:
                                 del r._host
                             r.done = now
                             state["end"] = max(state["end"], now)
-                        freed += pc.need
+                        if pc.in_ring:
+                            given += 1
+                        else:
+                            freed += pc.need
                         pc.dk = pc.dv = pc.ov = pc.of = pc.ev = None
                     with cv:
+                        for _ in range(given):
+                            ring.give()
                         state["used"] -= freed
                         cv.notify_all()
             except Exception as e:  # pragma: no cover - surfaced by serve()
