@@ -69,3 +69,29 @@ def test_components_commute(case, seed):
     assert whole == parts
     for x, y in zip(a.snapshot(), b.snapshot()):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_components_commute_round_the_ring(seed):
+    """The same claim when the crowded region runs past the end of the table
+    into slot 0 (keys homed in the last 400 slots of a 0.85-load table)."""
+    cap = 1 << 12
+    rng = np.random.default_rng(100 + seed)
+    a, b = OracleAdapter(cap, 8, 8), OracleAdapter(cap, 8, 8)
+    pk = rng.integers(0, 256, (int(cap * 0.85), 8), dtype=np.uint8)
+    for m in (a, b):
+        m.bulk_insert(pk, pk)
+    n = 500
+    homes = (cap - 400 + rng.integers(0, 400, n)).astype(np.uint64)
+    k = ((np.arange(n, dtype=np.uint64) + 1) * np.uint64(cap) + homes).view(np.uint8).reshape(n, 8).copy()
+    v = rng.integers(0, 256, (n, 8), dtype=np.uint8)
+    comp = component_of(a.snapshot()[0].astype(np.int64), homes.astype(np.int64), cap)
+    starts = np.unique(comp)
+    whole = a.bulk_insert(k, v)
+    parts = 0
+    for c in starts[::-1]:
+        idx = np.nonzero(comp == c)[0]
+        parts += b.bulk_insert(k[idx], v[idx])
+    assert whole == parts
+    for x, y in zip(a.snapshot(), b.snapshot()):
+        assert np.array_equal(x, y)
