@@ -158,7 +158,10 @@ const char* fm_kernel_class_name(uint32_t cls);
  * table's count after the ops before it).  The ops are planned into waves of
  * independent ops (distinct tables; consecutive gets of one table share a
  * wave); each wave runs grouped kernels that serve all its ops of one kind
- * and record shape per launch.  Without a graph, fm_batch_run drives each
+ * and record shape per launch.  Tables are spread over up to 8 stream lanes
+ * forked from the caller's stream and joined back before the results are
+ * copied out, so the waves of different tables overlap; a table's ops stay in
+ * order on its lane.  Without a graph, fm_batch_run drives each
  * wave's insert/remove rounds from the host (a 4-byte readback per two
  * rounds, as the plain calls do) and records how many rounds each wave
  * needed.  fm_batch_capture records the whole batch into a CUDA graph with
@@ -166,8 +169,9 @@ const char* fm_kernel_class_name(uint32_t cls);
  * synchronisation; later fm_batch_run calls replay it.  A replay whose data
  * needs more rounds than recorded still gives the same results, more slowly
  * (the remaining ops finish in a single block per op) -- run the batch
- * eagerly once on representative data before capturing.  Between fm_batch_run and fm_batch_wait the
- * batch's tables must not be used by other calls.  Per-op results (new /
+ * eagerly once on representative data before capturing.  Between
+ * fm_batch_run and fm_batch_wait the batch's tables must not be used by other
+ * calls.  Per-op results (new /
  * removed key counts) and status codes (FM_OK, FM_ERR_TABLE_FULL,
  * FM_ERR_PROBE_LIMIT, ...) are written back into the op array by
  * fm_batch_wait, which also updates each table's len. */
