@@ -701,8 +701,11 @@ def served_leg(torch, F, dev, scale=1):
     wall = quiet(srv.serve, reqs_s)
     out["served"] = dict(latency_summary(reqs_s), mops=round(total_keys / wall / 1e6, 3), wall_s=round(wall, 3),
                          batches=srv.batches, mean_requests_per_batch=round(n_req / max(srv.batches, 1), 2))
+    del srv  # its staging buffer goes before the plain server runs
     m.copy_from(backup)
     torch.cuda.synchronize()
+    gc.collect()
+    torch.cuda.empty_cache()
     reqs_p = requests()
     wall_p = quiet(PlainServer(m, out_pool=lambda n, v: (out_v[:n].numpy(), out_f[:n].numpy())).serve, reqs_p)
     out["plain"] = dict(latency_summary(reqs_p), mops=round(total_keys / wall_p / 1e6, 3), wall_s=round(wall_p, 3))
