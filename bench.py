@@ -20,9 +20,12 @@ bytes.  with_capacity(10,000,000) as written rounds up to 2^24 slots, where
            time, read from the library's per-kernel CUDA events in an extra
            step, against MEASURED_PEAKS.json hbm_gbs.
   cpu_baseline: the sequential CPU oracle on the 1/16-scale sample.
+  oracle_check: the same leg replays the whole step the GPU ran on the
+           sequential oracle and compares every result and the final table.
 
 `--impl reference` times the reference's CPU algorithm (multithreaded CAS
-restatement of src/rayon_cpu.rs, all host threads) on the 1/16-scale sample.
+restatement of src/rayon_cpu.rs, all host threads) on the same full-size
+workload.
 Multi-GPU (torchrun): every rank runs an independent table (replicas, weak
 scaling); no collective on the data path.
 """
@@ -135,6 +138,40 @@ def cpu_step(O, w, inp, threads=None, traffic=False):
     return dt, tr
 
 
+def oracle_replay_check(run):
+    """Part of the CPU-baseline leg: the sequential oracle replays the step
+    the GPU just ran (same inputs, same call sizes) and every result is
+    compared: each insert call's new-key count summed, every get's found flag
+    and value bytes, the remove count, len, and the whole final table
+    (metadata word of every slot, key and value bytes of every occupied slot)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    w, m = run.w, run.m
+    t0 = time.perf_counter()
+    keys, vals = run.keys.cpu().numpy(), run.vals.cpu().numpy()
+    q, rem = run.q.cpu().numpy(), run.rem.cpu().numpy()
+    # the GPU's results of its last step: outputs, then the final table
+    gv, gf = run.out_v.cpu().numpy(), run.out_f.cpu().numpy().astype(bool)
+    gsnap = m.snapshot()
+    o = O.OracleMap(w.cap, KB, VB)
+    added = sum(o.bulk_insert(keys[b:b + CALL], vals[b:b + CALL]) for b in range(0, w.pairs, CALL))
+    ov, of = o.bulk_get(q)
+    removed = o.bulk_remove(rem)
+    osnap = o.snapshot()
+    ok = {
+        "inserts_new_keys": added == w.pairs,
+        "gets_found": bool(np.array_equal(gf, of)),
+        "gets_values": bool(np.array_equal(gv, ov)),
+        "removes": removed == w.removes,
+        "len": m.len() == len(o),
+        "table": all(bool(np.array_equal(a, b)) for a, b in zip(gsnap, osnap)),
+    }
+    return {"replayed": f"the whole step on the sequential CPU oracle ({w.pairs} inserts in calls of {CALL}, "
+                        f"{w.gets} gets, {w.removes} removes)",
+            "identical": all(ok.values()), "checks": ok, "seconds": round(time.perf_counter() - t0, 1)}
+
+
 def bytes_per_op(tr):
     out = {}
     for k, v in tr.items():
@@ -169,6 +206,9 @@ def cpu_baseline_leg(w):
 
 
 def reference_arm(args, w):
+    """The reference's CPU algorithm on the host cores, on the same workload
+    as the GPU arm (full size: every step is one clear + the step's inserts,
+    gets and removes)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -176,22 +216,22 @@ def reference_arm(args, w):
     import oracle as O
 
     threads = os.cpu_count() or 1
-    ws = w.scaled(SAMPLE_DIV)
-    inp = cpu_sample_inputs(ws)
+    inp = cpu_sample_inputs(w)
     for _ in range(args.warmup):
-        cpu_step(O, ws, inp, threads=threads)
-    times = [cpu_step(O, ws, inp, threads=threads)[0] for _ in range(args.steps)]
+        cpu_step(O, w, inp, threads=threads)
+    times = [cpu_step(O, w, inp, threads=threads)[0] for _ in range(args.steps)]
     total = sum(times)
-    v = ws.ops * len(times) / total / 1e6
+    v = w.ops * len(times) / total / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "Mops/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / len(times) * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": dict(w.desc(), parallelism="host threads"),
         "cpu_baseline": {"value": round(v, 3), "unit": "Mops/s", "cores": threads, "kind": "port",
-                         "sample": f"the step at 1/{SAMPLE_DIV} scale ({ws.cap} slots, {ws.pairs} pairs); "
-                                   "multithreaded CAS restatement of src/rayon_cpu.rs (the reference's Rust "
-                                   "crate cannot be built here)"},
+                         "sample": f"the whole step ({w.cap} slots, {w.pairs} pairs in calls of {CALL}, "
+                                   f"{w.gets} gets, {w.removes} removes), {threads} threads; multithreaded CAS "
+                                   "restatement of src/rayon_cpu.rs (the reference's Rust crate cannot be "
+                                   "built here)"},
         "e2e": {"value": round(v, 3), "unit": "Mops/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -727,6 +767,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form workload")
     ap.add_argument("--no-served", action="store_true", help="skip the served-form workload")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default lookup kernel configuration")
+    ap.add_argument("--no-oracle-check", action="store_true",
+                    help="skip the oracle replay of the step (part of the CPU-baseline leg)")
     ap.add_argument("--nvtx", action="store_true",
                     help="mark one insert call and the bulk_get of the kernel-timing step with NVTX ranges")
     ap.add_argument("--scale", type=int, default=1,
@@ -777,6 +819,9 @@ def main():
     ms_step = total_ms / args.steps
     value = main_w.ops * world / (ms_step / 1e3) / 1e6
     kt = run.kernel_pass(args.nvtx)
+    check = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.no_oracle_check:
+        check = oracle_replay_check(run)
     e2e = None if args.no_e2e else run.e2e(args.steps, barrier, dist, world)
 
     line = {
@@ -790,6 +835,8 @@ def main():
                           "autotuned": not args.no_autotune},
         "kernels": kernel_summary(kt, main_w),
     }
+    if check:
+        line["oracle_check"] = check
     if e2e:
         line["e2e"] = e2e
     clk_sum = clk.summary()

@@ -29,6 +29,31 @@ int cuda_fail(int code, const char* what, cudaError_t e) {
     return fail(code, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Host-side failure injection (fm_inject_fault): one armed site and the
+// number of passes through it still to let by.  The failing CUDA call is not
+// made; the site returns the error that call would have returned.
+std::atomic<uint32_t> g_fault_site{FM_FAULT_NONE};
+std::atomic<int64_t> g_fault_after{-1};
+
+bool fault_at(uint32_t site) {
+    if (g_fault_site.load(std::memory_order_relaxed) != site) return false;
+    if (g_fault_after.fetch_sub(1) != 0) return false;
+    g_fault_site.store(FM_FAULT_NONE);
+    return true;
+}
+
+// cudaMalloc behind the allocation fault site.
+cudaError_t dev_alloc(void** p, size_t bytes) {
+    if (fault_at(FM_FAULT_ALLOC)) return cudaErrorMemoryAllocation;
+    return cudaMalloc(p, bytes);
+}
+
+// cudaMemcpyAsync behind the transfer fault site.
+cudaError_t copy_async(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
+    if (fault_at(FM_FAULT_TRANSFER)) return cudaErrorInvalidValue;
+    return cudaMemcpyAsync(dst, src, bytes, kind, s);
+}
+
 // Device chunk of one mutating call: op indices are u32 and 0xFFFFFFFF marks
 // an idle segment slot, so a call is split into sequential chunks (which is
 // exactly the sequential semantics) of at most this many operations.
@@ -74,7 +99,7 @@ cudaError_t grow(T*& p, size_t& cap, size_t need) {
     p = nullptr;
     cap = 0;
     size_t want = need + need / 4;
-    cudaError_t e = cudaMalloc((void**)&p, want);
+    cudaError_t e = dev_alloc((void**)&p, want);
     if (e == cudaSuccess) cap = want;
     return e;
 }
@@ -225,7 +250,7 @@ int ensure_scratch(fm_table* t, uint64_t n) {
     if (t->sc_base) cudaFree(t->sc_base);
     t->sc_base = nullptr;
     t->sc = OpScratch{};
-    cudaError_t e = cudaMalloc((void**)&t->sc_base, bytes);
+    cudaError_t e = dev_alloc((void**)&t->sc_base, bytes);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_GPU_ALLOC, "scratch allocation", e);
     uint8_t* p = t->sc_base;
     auto carve = [&](size_t b) {
@@ -253,12 +278,23 @@ int ensure_scratch(fm_table* t, uint64_t n) {
     return FM_OK;
 }
 
+// The least op index marking each 32-slot chunk (the second half of the
+// remove summaries) back to idle: a remove that fails part way can leave
+// marks set, and a stale mark below an op's index would block that op in
+// every later remove.
+cudaError_t reset_rsum_marks(fm_table* t, cudaStream_t s) {
+    if (!t->sc.rsum) return cudaSuccess;
+    const uint64_t nch = fm::rsum_chunks(t->mask);
+    return cudaMemsetAsync(t->sc.rsum + nch, 0xFF, nch * 4, s);
+}
+
 // After a failed call the segment registrations and the per-op scratch may be
 // left set; put every one of them back to idle.
 void recover(fm_table* t, cudaStream_t s) {
     cudaMemsetAsync(t->d_seg_min, 0xFF, t->cap * 4, s);
     cudaMemsetAsync(t->d_seg_cnt, 0, t->cap * 4, s);
     if (t->sc.op_word) cudaMemsetAsync(t->sc.op_word, 0xFF, t->sc.cap_ops * 4, s);
+    reset_rsum_marks(t, s);
     cudaStreamSynchronize(s);
 }
 
@@ -309,6 +345,7 @@ int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t
             if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, insert ? "insert rounds" : "remove rounds", e);
             e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
             if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e == cudaSuccess && fault_at(FM_FAULT_ROUND)) e = cudaErrorLaunchFailure;
             if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "round readback", e);
             if (t->h_ctl->err & fm::ERR_SCRATCH) return fail(FM_ERR_KERNEL_LAUNCH, "stale segment registration");
             if (t->h_ctl->err & fm::ERR_NO_PROGRESS) return fail(FM_ERR_PROBE_LIMIT, "round made no progress");
@@ -416,6 +453,14 @@ const char* fm_last_error(void) { return tl_err.c_str(); }
 
 uint64_t fm_launch_count(void) { return fm::launch_count(); }
 
+int fm_inject_fault(uint32_t site, uint32_t after) {
+    if (site > FM_FAULT_ROUND) return fail(FM_ERR_INVALID_ARG, "unknown fault site");
+    g_fault_site.store(FM_FAULT_NONE);
+    g_fault_after.store((int64_t)after);
+    g_fault_site.store(site);
+    return FM_OK;
+}
+
 int fm_create(uint64_t capacity, uint32_t key_size, uint32_t value_size, uint32_t hash_mode, int device_id,
               fm_table** out) {
     if (!out) return fail(FM_ERR_INVALID_ARG, "out is NULL");
@@ -456,12 +501,12 @@ int fm_create(uint64_t capacity, uint32_t key_size, uint32_t value_size, uint32_
             return bail(FM_ERR_CUDA_INIT, "event", e);
     const size_t kb = (size_t)cap * (key_size ? key_size : 1);
     const size_t vb = (size_t)cap * (value_size ? value_size : 1);
-    if ((e = cudaMalloc((void**)&t->d_flags, cap * 4)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "flags", e);
-    if ((e = cudaMalloc((void**)&t->d_keys, kb)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "keys", e);
-    if ((e = cudaMalloc((void**)&t->d_vals, vb)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "values", e);
-    if ((e = cudaMalloc((void**)&t->d_seg_min, cap * 4)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "seg_min", e);
-    if ((e = cudaMalloc((void**)&t->d_seg_cnt, cap * 4)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "seg_cnt", e);
-    if ((e = cudaMalloc((void**)&t->d_ctl, sizeof(Ctl))) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "ctl", e);
+    if ((e = dev_alloc((void**)&t->d_flags, cap * 4)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "flags", e);
+    if ((e = dev_alloc((void**)&t->d_keys, kb)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "keys", e);
+    if ((e = dev_alloc((void**)&t->d_vals, vb)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "values", e);
+    if ((e = dev_alloc((void**)&t->d_seg_min, cap * 4)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "seg_min", e);
+    if ((e = dev_alloc((void**)&t->d_seg_cnt, cap * 4)) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "seg_cnt", e);
+    if ((e = dev_alloc((void**)&t->d_ctl, sizeof(Ctl))) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "ctl", e);
     if ((e = cudaMallocHost((void**)&t->h_ctl, sizeof(Ctl))) != cudaSuccess) return bail(FM_ERR_GPU_ALLOC, "ctl", e);
     memset(t->h_ctl, 0, sizeof(Ctl));
     // Zeroed SoA table: all flags EMPTY (gpu.rs:81-92).
@@ -539,15 +584,15 @@ int fm_bulk_get(fm_table* t, const void* keys, uint64_t n, void* out_values, uin
         uint8_t* dq = c->d_buf[sl];
         uint8_t* dv = c->d_buf[sl] + off_v;
         uint8_t* df = c->d_buf[sl] + off_f;
-        if ((e = cudaMemcpyAsync(dq, hk + base * t->ksz, m * t->ksz, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        if ((e = copy_async(dq, hk + base * t->ksz, m * t->ksz, cudaMemcpyHostToDevice, st)) != cudaSuccess)
             rc = cuda_fail(FM_ERR_TRANSFER, "htod keys", e);
         if (!rc && (e = fm::launch_get_cfg(t->view(), t->shape, dq, m, dv, df,
                                            fm::tuned_get_cfg(t->shape, fm_load_factor(t)), st)) != cudaSuccess)
             rc = cuda_fail(FM_ERR_KERNEL_LAUNCH, "bulk_get", e);
         if (!rc && t->vsz &&
-            (e = cudaMemcpyAsync(hv + base * t->vsz, dv, m * t->vsz, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            (e = copy_async(hv + base * t->vsz, dv, m * t->vsz, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
             rc = cuda_fail(FM_ERR_TRANSFER, "dtoh values", e);
-        if (!rc && (e = cudaMemcpyAsync(out_found + base, df, m, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        if (!rc && (e = copy_async(out_found + base, df, m, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
             rc = cuda_fail(FM_ERR_TRANSFER, "dtoh found", e);
     }
     for (int i = 0; i < 2; i++)
@@ -572,9 +617,13 @@ namespace {
 
 // A host-buffer insert (values != nullptr or vsz == 0) or remove, in pieces:
 // the copy stream uploads piece i+1 into the other staging half while the
-// rounds of piece i run on the table's stream.
+// rounds of piece i run on the table's stream.  *out is the count of the
+// pieces that completed, also when a later piece fails (those pieces are in
+// the table; the failing piece may be in part).
 int host_pieces(fm_table* t, bool insert, const void* keys, const void* values, uint64_t n, uint64_t* out,
                 bool* limit) {
+    *out = 0;
+    *limit = false;
     const uint64_t piece = n < HOST_MUT_PIECE ? n : HOST_MUT_PIECE;
     const size_t kb = (size_t)piece * t->ksz, vb = insert ? (size_t)piece * t->vsz : 0;
     const size_t off_v = (kb + 255) & ~(size_t)255;
@@ -586,9 +635,9 @@ int host_pieces(fm_table* t, bool insert, const void* keys, const void* values, 
     auto upload = [&](uint64_t base, int sl) -> cudaError_t {
         const uint64_t m = (n - base) < piece ? (n - base) : piece;
         uint8_t* d = t->d_in + sl * half;
-        cudaError_t err = cudaMemcpyAsync(d, hk + base * t->ksz, m * t->ksz, cudaMemcpyHostToDevice, t->copy_stream);
+        cudaError_t err = copy_async(d, hk + base * t->ksz, m * t->ksz, cudaMemcpyHostToDevice, t->copy_stream);
         if (err == cudaSuccess && vb)
-            err = cudaMemcpyAsync(d + off_v, hv + base * t->vsz, m * t->vsz, cudaMemcpyHostToDevice, t->copy_stream);
+            err = copy_async(d + off_v, hv + base * t->vsz, m * t->vsz, cudaMemcpyHostToDevice, t->copy_stream);
         if (err == cudaSuccess) err = cudaEventRecord(t->piece_ready[sl], t->copy_stream);
         return err;
     };
@@ -600,21 +649,29 @@ int host_pieces(fm_table* t, bool insert, const void* keys, const void* values, 
     for (uint64_t base = 0, i = 0; base < n; base += piece, ++i) {
         const int sl = (int)(i & 1);
         const uint64_t m = (n - base) < piece ? (n - base) : piece;
+        int rc = FM_OK;
         if ((e = cudaStreamWaitEvent(t->stream, t->piece_ready[sl], 0)) != cudaSuccess)
-            return cuda_fail(FM_ERR_TRANSFER, "piece wait", e);
+            rc = cuda_fail(FM_ERR_TRANSFER, "piece wait", e);
         // the other half was last read by piece i-1, whose rounds have returned
-        if (base + piece < n && (e = upload(base + piece, sl ^ 1)) != cudaSuccess)
-            return cuda_fail(FM_ERR_TRANSFER, "htod", e);
+        if (!rc && base + piece < n && (e = upload(base + piece, sl ^ 1)) != cudaSuccess)
+            rc = cuda_fail(FM_ERR_TRANSFER, "htod", e);
         uint8_t* d = t->d_in + sl * half;
         uint64_t c = 0;
         bool l = false;
-        int rc = run_rounds(t, insert, d, insert && t->vsz ? d + off_v : (insert ? d : nullptr), m, t->stream, &c, &l);
+        if (!rc)
+            rc = run_rounds(t, insert, d, insert && t->vsz ? d + off_v : (insert ? d : nullptr), m, t->stream, &c,
+                            &l);
         if (rc) {
+            const std::string msg = tl_err;
             cudaStreamSynchronize(t->copy_stream);
+            cudaStreamSynchronize(t->stream);
+            *out = total;
+            tl_err = msg;
             return rc;
         }
         total += c;
         lim = lim || l;
+        *out = total;
     }
     *out = total;
     *limit = lim;
@@ -636,8 +693,8 @@ int fm_bulk_insert(fm_table* t, const void* keys, const void* values, uint64_t n
     uint64_t added = 0;
     bool limit = false;
     rc = host_pieces(t, true, keys, values, n, &added, &limit);
+    t->len += added;  // on failure: the pieces that completed
     if (rc) return rc;
-    t->len += added;
     *num_new = added;
     return limit ? limit_error() : FM_OK;
 }
@@ -653,8 +710,8 @@ int fm_bulk_remove(fm_table* t, const void* keys, uint64_t n, uint64_t* num_remo
     uint64_t removed = 0;
     bool limit = false;
     int rc = host_pieces(t, false, keys, nullptr, n, &removed, &limit);
+    t->len -= removed;  // on failure: the pieces that completed
     if (rc) return rc;
-    t->len -= removed;
     *num_removed = removed;
     return FM_OK;
 }
@@ -665,6 +722,7 @@ int fm_clear(fm_table* t) {
     DeviceGuard dg(t->device);
     cudaError_t e = cudaMemsetAsync(t->d_flags, 0, t->cap * 4, t->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(&t->d_ctl->dmax, 0, 8, t->stream);  // dmax, tomb_claimed
+    if (e == cudaSuccess) e = reset_rsum_marks(t, t->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "clear", e);
     t->len.store(0);
@@ -856,22 +914,29 @@ const char* fm_kernel_class_name(uint32_t cls) {
 // ---------------------------------------------------------------------------
 // Allocation-free insert (no counterpart in the reference).
 //
-// Some callers cannot allocate GPU memory at the point where they insert: a
-// pipeline stage inside a captured or long-lived stream, a process that runs
-// with its device memory pre-reserved under a fixed budget, or code running
-// from a CUDA host callback, where cudaMalloc is not allowed.  For them,
-// fm_bulk_insert_device_noalloc runs the same insert kernels as
-// fm_bulk_insert_device, but every per-call buffer (round control block,
-// pending lists, per-op words) comes from the file-scope device array below,
-// sized for FM_NOALLOC_MAX_OPS operations (about 2.5 MB, held by every GPU
-// that loads the library until the process exits).
+// Some callers must not allocate device memory once they are running: a
+// serving process that reserves all its device memory up front under a fixed
+// budget, or one whose caching allocator (PyTorch's, say) holds the free
+// memory, where a cudaMalloc made here at insert time could fail and a
+// cudaFree would synchronize the whole device and stall the caller's other
+// streams.  For them, fm_bulk_insert_device_noalloc runs the round-based
+// insert kernels with every per-call buffer (round control block, pending
+// lists, per-op words) taken from the file-scope device array below, sized for
+// FM_NOALLOC_MAX_OPS operations (about 2.5 MB, held by every GPU that loads
+// the library until the process exits).  It never calls cudaMalloc, cudaFree
+// or another allocating routine.
 //
-// The first call on a device sets the array up (looks up its device address
-// and marks the per-op words idle) and synchronizes; make that first call
-// before any stream capture.  Later calls only launch kernels and copy small
-// control words.  All calls share the one array: calls whose GPU work
-// overlaps -- on any table of the same device -- race on it, so serialize them
-// (one stream, or an event between calls).
+// It is called from an ordinary host thread: like fm_bulk_insert_device it
+// launches kernels, copies control words back and waits on the caller's
+// stream, so it cannot run inside a CUDA host function.  The first call on a
+// device sets the array up (looks up its device address with that device
+// current, marks the per-op words idle) and synchronizes the device; make that
+// first call before any stream capture on the device.  All calls share the
+// one array: calls whose GPU work overlaps -- on any table of the same device
+// -- race on it, so serialize them (one stream, or an event between calls).
+// Near a full table, where rounds stop making progress, the remaining ops run
+// one at a time on one block (the tail or k_ins_serial): the component path of
+// the allocating insert needs a per-table buffer this array does not hold.
 // ---------------------------------------------------------------------------
 namespace {
 

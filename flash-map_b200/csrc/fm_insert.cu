@@ -1280,18 +1280,15 @@ __global__ void __launch_bounds__(RBLOCK, FM_P4_MIN_BLOCKS) k_ins_p4(TableView t
     publish_rare(ctl, a.maxd, a.tomb, a.limit);
 }
 
-// Lanes per insert of the long-walk pass: 32, 16 or 8 (environment variable
-// FLASHMAP_P4_LANES, read once; default 32, the fastest measured on B200 at
-// load 0.8: 8 and 16 lanes share warp instructions between inserts but walk
-// more windows and move fewer records per round trip).
-int p4_lanes() {
-    static int lanes = [] {
-        const char* e = getenv("FLASHMAP_P4_LANES");
-        const int v = e ? atoi(e) : 32;
-        return (v == 8 || v == 16 || v == 32) ? v : 32;
-    }();
-    return lanes;
-}
+// Lanes per insert of the long-walk pass: 32, 16 or 8 (compile-time setting
+// FM_P4_LANES; default 32, the fastest measured on B200 at load 0.8: 8 and 16
+// lanes share warp instructions between inserts but walk more windows and
+// move fewer records per round trip).
+#ifndef FM_P4_LANES
+#define FM_P4_LANES 32
+#endif
+static_assert(FM_P4_LANES == 8 || FM_P4_LANES == 16 || FM_P4_LANES == 32, "FM_P4_LANES: 8, 16 or 32");
+constexpr int p4_lanes() { return FM_P4_LANES; }
 
 // ---- single-block tails ----------------------------------------------------
 //
@@ -2149,10 +2146,7 @@ void rounds_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, 
         }
         if constexpr (KB != 0 && VB != 0) {
             KtScope kt(KC_INS_LONG, s);
-            const int l = p4_lanes();
-            if (l == 8) k_ins_p4<KB, VB, 8><<<g4, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
-            else if (l == 16) k_ins_p4<KB, VB, 16><<<g4, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
-            else k_ins_p4<KB, VB, 32><<<g4, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
+            k_ins_p4<KB, VB, p4_lanes()><<<g4, RBLOCK, 0, s>>>(t, keys, vals, r, sc, ctl);
         }
     }
     count_launches((KB != 0 && VB != 0 ? 4 : 3) * nrounds);

@@ -25,6 +25,7 @@ EXPORTS = (
     "fm_bulk_insert_device_noalloc", "fm_kernel_timing", "fm_kernel_times", "fm_kernel_times_reset",
     "fm_kernel_class_name", "fm_batch_create", "fm_batch_capture", "fm_batch_run", "fm_batch_wait",
     "fm_batch_waves", "fm_batch_destroy", "fm_autotune", "fm_tuned_get_config", "fm_copy",
+    "fm_inject_fault",
 )
 
 
@@ -117,6 +118,8 @@ def _declare(L) -> None:
     L.fm_autotune.argtypes = [i32, C.c_char_p]
     L.fm_tuned_get_config.restype = i32
     L.fm_tuned_get_config.argtypes = [u32, u32, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.fm_inject_fault.restype = i32
+    L.fm_inject_fault.argtypes = [u32, u32]
 
 
 def load_library(path: str = LIB_PATH):
@@ -154,6 +157,17 @@ def tuned_get_config(key_size: int, value_size: int, load: float):
     lanes, bps = C.c_int(0), C.c_int(0)
     load_library().fm_tuned_get_config(key_size, value_size, load, C.byref(lanes), C.byref(bps))
     return lanes.value, bps.value
+
+
+FAULT_NONE, FAULT_ALLOC, FAULT_TRANSFER, FAULT_ROUND = 0, 1, 2, 3
+
+
+def inject_fault(site: int, after: int = 0) -> None:
+    """Arm one host-side failure (fm_inject_fault): the after-th next pass
+    through `site` fails as if its CUDA call had failed.  Tests only."""
+    from .errors import raise_for_status
+
+    raise_for_status(load_library().fm_inject_fault(site, after), last_error())
 
 
 def last_error() -> str:

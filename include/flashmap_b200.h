@@ -114,16 +114,29 @@ int fm_bulk_remove_device(fm_table* t, const void* d_keys, uint64_t n, uint64_t*
                           void* stream);
 
 /* Allocation-free insert.  No counterpart in the reference: an addition for
- * callers that cannot allocate GPU memory when they insert (work issued from
- * a CUDA host callback, where cudaMalloc is not allowed; a pipeline stage on
- * a long-lived stream; a process whose device memory is reserved up front).
- * Same semantics and arguments as fm_bulk_insert_device, but it calls no
- * cudaMalloc/cudaFree: its per-call scratch is a fixed device array inside
- * the library, so a call takes at most FM_NOALLOC_MAX_OPS keys (larger
- * batches fail with FM_ERR_INVALID_ARG; split them).  The first call on a
- * device sets that array up and synchronizes -- make it before any stream
- * capture.  All calls share the array: calls whose GPU work overlaps (on any
- * table of the same device) race, so keep them ordered on one stream. */
+ * callers that must not allocate device memory once they are running -- a
+ * serving process that sizes all its device memory up front under a fixed
+ * budget, or one whose caching allocator (PyTorch's, for instance) holds the
+ * free memory, so that a cudaMalloc made by this library at insert time could
+ * fail, and a cudaFree would synchronize the whole device and stall the
+ * caller's other streams.  Same semantics and arguments as
+ * fm_bulk_insert_device, but it calls no cudaMalloc, cudaFree or other
+ * allocating routine: its per-call scratch is a fixed device array inside the
+ * library (about 2.5 MB, held by every device that loads the library until
+ * the process exits), so a call takes at most FM_NOALLOC_MAX_OPS keys (larger
+ * batches fail with FM_ERR_INVALID_ARG; split them).
+ * Call it from an ordinary host thread: it launches kernels, copies control
+ * words and waits on `stream` like fm_bulk_insert_device does, so it cannot
+ * run inside a CUDA host function (cudaLaunchHostFunc), where CUDA calls are
+ * not allowed.  The first call on a device also sets the array up (looks up
+ * its device address, marks its per-op words idle, synchronizes the device);
+ * make that first call before any stream capture on that device.  All calls
+ * share the one array: calls whose GPU work overlaps (on any table of the same
+ * device) race on it, so keep them ordered on one stream.  Near a full table,
+ * where the parallel rounds of an insert stop making progress, this entry
+ * point finishes the remaining keys one at a time on a single thread block
+ * (fm_bulk_insert_device spreads that work over the GPU), so it is much slower
+ * there. */
 #define FM_NOALLOC_MAX_OPS 65536u
 int fm_bulk_insert_device_noalloc(fm_table* t, const void* d_keys, const void* d_values, uint64_t n,
                                   uint64_t* num_new, void* stream);
@@ -137,6 +150,21 @@ const char* fm_last_error(void);
 /* Instrumentation (no counterpart in gpu.rs): number of kernels this library
  * has launched in the process so far, across all tables. */
 uint64_t fm_launch_count(void);
+
+/* Host-side failure injection for tests of the error paths (no counterpart in
+ * gpu.rs; the reference's error variants are src/error.rs:5-27).  Arms one
+ * fault for the whole process: the `after`-th next pass (0 = the next one)
+ * through `site` fails as if the CUDA call made there had returned an error,
+ * the call reports the matching status, and the fault disarms.  The failing
+ * CUDA call is not made, so nothing fails on the GPU.  FM_FAULT_NONE disarms.
+ * After a failed mutating call the table holds the host pieces that completed
+ * (len counts them) and possibly part of the failing piece; fm_recount gives
+ * the exact count. */
+#define FM_FAULT_NONE 0u
+#define FM_FAULT_ALLOC 1u     /* a device allocation (table, scratch, staging) -> FM_ERR_GPU_ALLOC */
+#define FM_FAULT_TRANSFER 2u  /* a host<->device copy of the host-pointer calls -> FM_ERR_TRANSFER */
+#define FM_FAULT_ROUND 3u     /* the readback after a pass of insert/remove rounds -> FM_ERR_KERNEL_LAUNCH */
+int fm_inject_fault(uint32_t site, uint32_t after);
 
 /* Per-kernel device timing (no counterpart in gpu.rs).  While on, every call
  * on the table records a CUDA event pair around each kernel it launches;

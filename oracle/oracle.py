@@ -22,7 +22,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libfm_oracle.so")
 REF_HOST_PATH = os.path.join(HERE, "_ref", "libref_host.so")
-REF_TREE = "/root/reference"
+# The reference source tree (bajpainaman/flash-map 0.5.0), needed only to
+# build the checker under _ref/; FLASHMAP_REFERENCE_TREE names it.
+REF_TREE = os.environ.get("FLASHMAP_REFERENCE_TREE", "")
 
 EMPTY, OCCUPIED, TOMBSTONE, INSERTING = 0, 1, 2, 3
 ERR_TABLE_FULL = 5
@@ -45,8 +47,8 @@ def build(quiet: bool = True) -> None:
     checker).  Only the checker is built here; nothing is run."""
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True, stdout=out)
-    if os.path.isdir(os.path.join(REF_TREE, "src")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True, stdout=out)
+    if REF_TREE and os.path.isdir(os.path.join(REF_TREE, "src")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_TREE}"], check=True, stdout=out)
 
 
 _lib = None
@@ -268,14 +270,14 @@ _ref = None
 
 
 def ref_host_available() -> bool:
-    return os.path.exists(REF_HOST_PATH) or os.path.isdir(os.path.join(REF_TREE, "src"))
+    return os.path.exists(REF_HOST_PATH) or bool(REF_TREE and os.path.isdir(os.path.join(REF_TREE, "src")))
 
 
 def ref_host():
     global _ref
     if _ref is None:
         if not os.path.exists(REF_HOST_PATH):
-            subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+            subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_TREE}"], check=True)
         L = C.CDLL(REF_HOST_PATH)
         vp = C.c_void_p
         L.ref_identity_hash.restype = C.c_uint64
