@@ -316,7 +316,7 @@ def max_over_ranks(value, dist, device):
     return float(t.item())
 
 
-INSERT_KERNELS = ("k_ins_p1", "k_ins_p2", "k_ins_p3", "k_ins_p4", "k_ins_tail", "k_ins_serial")
+INSERT_KERNELS = ("ins_find", "ins_flow", "ins_exec", "ins_warp", "k_ins_tail", "k_ins_serial")
 REMOVE_KERNELS = ("k_rem_p1", "k_rem_p2", "k_rem_p3", "k_rem_tail")
 
 # DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum) per op of
@@ -873,7 +873,7 @@ def main():
         peak, kind = read_peak()
         line["roofline"] = roofline_for(
             kt, INSERT_KERNELS, main_w.pairs, bpo["insert"], peak, kind,
-            "bulk_insert kernel set (k_ins_p1..p4 per round + k_ins_tail, every call of the step; the step's "
+            "bulk_insert kernel set (k_dx_find, k_dx_flow, k_dx_exec, k_dx_warp, every call of the step; the step's "
             "largest device-time share)", NCU_TRAFFIC_PER_OP["insert"])
         line["roofline_get"] = roofline_for(
             kt, ("k_get",), main_w.gets, bpo["get"], peak, kind, get_kernel_label(),

@@ -158,6 +158,8 @@ thread_local cudaEvent_t tl_open[fm::KC_N] = {};
 
 }  // namespace
 
+bool fm::kt_active() { return tl_timer != nullptr; }
+
 void fm::kt_mark(int cls, bool begin, cudaStream_t s) {
     KTimer* k = tl_timer;
     if (!k || cls < 0 || cls >= KC_N) return;
@@ -328,6 +330,31 @@ int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t
         // below FM_HANDOFF_LOAD the tail's own one-at-a-time order is cheaper
         // than a hand-back (a readback and a scan of the table)
         const bool handoff = reach >= FM_HANDOFF_LOAD;
+        if (insert && !direct && sh != fm::SHAPE_GENERIC && t->sc.comp) {
+            // no rounds: lone ops run at once, ops sharing free slots run in
+            // index order per component; what the kernels leave (a table with
+            // no free slot for some op, components too large for a warp) runs
+            // on the component path
+            e = fm::launch_ins_direct(v, sh, kk, vv, m, t->sc, t->d_ctl, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e == cudaSuccess && fault_at(FM_FAULT_ROUND)) e = cudaErrorLaunchFailure;
+            if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "insert", e);
+            if (t->h_ctl->err & fm::ERR_SCRATCH) return fail(FM_ERR_KERNEL_LAUNCH, "stale segment registration");
+            const uint32_t rest_r = t->h_ctl->serial[0] ? 0u : 1u;
+            const uint32_t rest_n = t->h_ctl->serial[0] ? m : t->h_ctl->npend[1];
+            if (rest_n) {
+                e = fm::launch_ins_comp(v, sh, kk, vv, m, rest_r, rest_n, t->sc, t->d_ctl, s);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "component insert", e);
+            }
+            total += t->h_ctl->total_count();
+            *err_bits |= t->h_ctl->err;
+            t->last_rounds = t->h_ctl->rounds;
+            continue;
+        }
         for (;;) {
             if (direct) {
                 e = fm::launch_ins_comp(v, sh, kk, vv, m, 0, m, t->sc, t->d_ctl, s);
@@ -903,9 +930,10 @@ int fm_kernel_times_reset(fm_table* t) {
 }
 
 const char* fm_kernel_class_name(uint32_t cls) {
-    static const char* names[fm::KC_N] = {"k_get",       "k_ins_p1",    "k_ins_p2",    "k_ins_p3",
-                                          "k_ins_p4",    "k_ins_tail",  "k_ins_serial", "k_rem_p1",
-                                          "k_rem_p2",    "k_rem_p3",    "k_rem_tail",  "k_count"};
+    // insert classes: the direct kernels (k_dx_*) or the round kernels (k_ins_p1..p4)
+    static const char* names[fm::KC_N] = {"k_get",      "ins_find",   "ins_flow",     "ins_exec",
+                                          "ins_warp",   "k_ins_tail", "k_ins_serial", "k_rem_p1",
+                                          "k_rem_p2",   "k_rem_p3",   "k_rem_tail",   "k_count"};
     return cls < (uint32_t)fm::KC_N ? names[cls] : nullptr;
 }
 

@@ -31,6 +31,7 @@
 #include <limits>
 #include <cstdlib>
 #include <type_traits>
+#include <utility>
 
 #include "fm_rounds.cuh"
 
@@ -1913,6 +1914,439 @@ __global__ void __launch_bounds__(RBLOCK) k_cmp_clean(TableView t, OpScratch sc)
     }
 }
 
+// ---- direct insert: components found from each op's free slot -------------
+//
+// The plain insert call below the component load, without rounds.  An insert
+// reads and writes only [home, F'] (F' its first free slot when it runs) and
+// fills F' when its key is new (the argument of the component path above).
+// With F each op's first free slot before the call, the ops that can touch
+// common slots are those joined by a chain of free slots over which their
+// demand carries; here the chains are found from the ops' own free slots
+// instead of by a scan of the table:
+//   find  (a thread per op)  F, then the op joins F's list: seg_cnt[F] counts
+//         the ops at F, seg_min[F] heads a list linked through op_word, and
+//         the first op to arrive leads F (op_flag 1).
+//   flow  (a thread per leader of an F holding c >= 2 ops)  walks the free
+//         slots after F carrying c - 1 ops, each slot taking one and adding
+//         its own ops, and marks every later F it reaches (DX_ABS in seg_cnt)
+//         as part of this component, until the carry is 0.
+//   exec  (a thread per op)  an op alone at an unmarked F runs at once: its
+//         walk [home, F] from the metadata, the possible updates compared,
+//         the records moved two per round trip; a walk too long for one
+//         thread, and the leader of an unmarked F with c >= 2, go to the warp
+//         pass's list; the other ops wait for their component.
+//   warp  (a warp per list entry)  a long lone op runs as a tile walk; a
+//         component gathers its ops from the lists of its free slots (the
+//         flow walk again), sorts them by index and runs them one after
+//         another as tile walks.
+// Components touch disjoint slots, so all of this runs at once.  A call that
+// finds an op with no free slot or a flow round the whole table leaves every
+// op to the component path (Ctl::serial[0]); a component with more ops than a
+// warp gathers leaves its ops to it (pend[1], Ctl::npend[1]).  Every
+// registration and list word is idle again when the four kernels end.
+constexpr uint32_t DX_ABS = 0x80000000u;   // seg_cnt: the free slot is in an earlier slot's component
+constexpr uint32_t DX_CNT = 0x7FFFFFFFu;
+constexpr uint32_t DX_ROOT = 0x80000000u;  // warp-pass list entry: a component's leader
+constexpr int DX_LCH = 16;                 // evictions of a walk on the thread path
+constexpr int DX_LCMP = 2;                 // possible updates of a walk on the thread path
+constexpr int DX_LTRIPS = 4;               // 16-slot metadata reads of a walk on the thread path
+constexpr int DX_GATHER = 64;              // ops of a component the warp pass runs itself
+constexpr int DX_THREADS = 256;            // threads of an exec block
+
+// Programmatic dependent launch between the direct kernels (compile-time
+// setting FM_DX_PDL, default on): each kernel lets the next one launch as
+// soon as all its blocks have started, and the next one waits for it to
+// finish (and its writes to be visible) before reading anything it wrote, so
+// launch latency overlaps execution instead of adding to it.
+#ifndef FM_DX_PDL
+#define FM_DX_PDL 1
+#endif
+__device__ __forceinline__ void dx_wait_prev() {
+#if FM_DX_PDL
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+__device__ __forceinline__ void dx_let_next() {
+#if FM_DX_PDL
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+
+// First free slot at or after unwrapped position a, looking at no more than
+// `budget` slots (less the slots looked at); NONE64 when none lies within it.
+__device__ __forceinline__ uint64_t dx_next_free(const TableView& t, uint64_t a, uint64_t& budget) {
+    const uint64_t mask = t.mask;
+    if (mask >= 7) {
+        for (uint64_t wb = a & ~7ull; budget > 0; wb += 8) {
+            const uint4* fp = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
+            const uint4 x = fp[0], y = fp[1];
+            const uint32_t f8[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+            uint64_t hit = NONE64;
+#pragma unroll
+            for (int l = 0; l < 8; l++) {
+                if (hit != NONE64 || wb + l < a || budget == 0) continue;
+                --budget;
+                if (is_free(f8[l])) hit = wb + l;
+            }
+            if (hit != NONE64) return hit;
+        }
+        return NONE64;
+    }
+    for (; budget > 0; ++a) {
+        --budget;
+        if (is_free(t.flags[a & mask])) return a;
+    }
+    return NONE64;
+}
+
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_dx_find(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
+                                                    OpScratch sc, Ctl* ctl) {
+    dx_let_next();
+    bool no_free = false;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n0; j += gridDim.x * blockDim.x) {
+        const uint64_t F = find_free<KB>(t, keys, j);
+        sc.op_slot[j] = F;
+        uint8_t lead = 0;
+        uint32_t next = IDLE;
+        if (F == NONE64) {
+            no_free = true;
+        } else {
+            lead = atomicAdd(&t.seg_cnt[F], 1u) == 0u ? 1 : 0;
+            next = atomicExch(&t.seg_min[F], j);
+        }
+        sc.op_word[j] = next;
+        sc.op_flag[j] = lead;
+    }
+    if (no_free) ctl->serial[0] = 1u;
+}
+
+__global__ void __launch_bounds__(RBLOCK) k_dx_flow(TableView t, uint32_t n0, OpScratch sc, Ctl* ctl) {
+    dx_wait_prev();
+    dx_let_next();
+    if (*(volatile uint32_t*)&ctl->serial[0]) return;  // every op goes to the component path
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n0; j += gridDim.x * blockDim.x) {
+        if (!sc.op_flag[j]) continue;
+        const uint64_t F = sc.op_slot[j];
+        const uint32_t c = t.seg_cnt[F] & DX_CNT;
+        if (c < 2) continue;
+        uint64_t flow = c - 1, a = F + 1, budget = t.mask;  // back at F: the flow wraps the table
+        for (;;) {
+            const uint64_t at = dx_next_free(t, a, budget);
+            if (at == NONE64) {
+                ctl->serial[0] = 1u;
+                break;
+            }
+            const uint64_t F2 = at & t.mask;
+            const uint32_t w2 = t.seg_cnt[F2];
+            const uint32_t c2 = w2 & DX_CNT;
+            if (c2) {
+                if (t.seg_min[F2] >= n0) {  // registrations come only from this call's ops
+                    atomicOr(&ctl->err, ERR_SCRATCH);
+                    break;
+                }
+                if (!(w2 & DX_ABS)) atomicOr(&t.seg_cnt[F2], DX_ABS);
+            }
+            flow = flow + c2 - 1;
+            if (flow == 0) break;
+            a = at + 1;
+        }
+    }
+}
+
+// A record (key and value) held in registers for a move.
+template <int KB, int VB>
+struct DxRec {
+    RegKey<KB> k;
+    RegVal<VB> v;
+    __device__ __forceinline__ void load_in(const uint8_t* kp, const uint8_t* vp) {
+        k.load(kp, KB);
+        v.load_ro(vp);
+    }
+    __device__ __forceinline__ void load_slot(const TableView& t, uint64_t s, bool value_only) {
+        if (!value_only) k.load_table(t.keys + s * KB, KB);
+        v.load(t.vals + s * VB, VB);
+    }
+    __device__ __forceinline__ void store_slot(const TableView& t, uint64_t s, bool value_only) const {
+        if (!value_only) k.store(t.keys + s * KB, KB);
+        v.store(t.vals + s * VB, VB);
+    }
+};
+
+// One op alone at its free slot F (nothing of another op lies in [home, F]),
+// on one thread.  Every slot in [home, F) is occupied (F is the first free
+// slot at or after home), so the walk is in closed form: with H the home of
+// the carried entry (the op's home first), a resident whose home r exceeds H
+// is evicted (the carried entry takes its slot at depth position - H, and the
+// resident is carried on: H = r), one with r == H is a possible update, and F
+// takes the last carried entry.  The possible updates are compared in one
+// round trip (the first equal key in walk order ends the walk in place), then
+// the records move highest first, two per round trip: move m writes P_m (the
+// m-th eviction slot; the end slot for the last) from P_(m-1) (the new entry
+// for m = 0), and a pair loads both sources before storing either, which
+// keeps each slot's read before its write.  Returns 1 (claimed F), 0 (updated
+// in place) or -1 with nothing written when the walk needs more than
+// DX_LTRIPS metadata reads, DX_LCH evictions or DX_LCMP possible updates, or
+// when the metadata does not show F as the first free slot.  Needs capacity
+// >= 8 and below 2^28 slots.
+template <int KB, int VB>
+__device__ __noinline__ int dx_lane(const TableView& t, const RegKey<KB>& key, uint64_t F, const uint8_t* kin,
+                                    const uint8_t* vin, uint32_t (*s_pos)[DX_THREADS],
+                                    uint32_t (*s_dep)[DX_THREADS], ExecAcc& acc) {
+    const uint64_t mask = t.mask;
+    const uint32_t me = threadIdx.x;
+    const uint64_t h = key.hash(KB, t.hash_mode) & mask;
+    const uint64_t e = h + ((F - h) & mask);  // F, unwrapped
+    const uint64_t wb = h & ~7ull;
+    if (e - wb >= 16ull * DX_LTRIPS) return -1;
+    uint32_t k = 0, nc = 0;
+    uint64_t cpos0 = 0, cpos1 = 0;
+    uint32_t cst0 = 0, cst1 = 0;
+    long long H = (long long)h;
+    bool end_tomb = false;
+    for (uint64_t w = wb; w <= e; w += 16) {
+        const uint4* p0 = reinterpret_cast<const uint4*>(t.flags + (w & mask));
+        const uint4* p1 = reinterpret_cast<const uint4*>(t.flags + ((w + 8) & mask));
+        const uint4 fa = p0[0], fb = p0[1], fc = p1[0], fd = p1[1];
+        const uint32_t f16[16] = {fa.x, fa.y, fa.z, fa.w, fb.x, fb.y, fb.z, fb.w,
+                                  fc.x, fc.y, fc.z, fc.w, fd.x, fd.y, fd.z, fd.w};
+#pragma unroll
+        for (int l = 0; l < 16; l++) {
+            const uint64_t pos = w + l;
+            if (pos < h || pos > e) continue;
+            if (pos == e) {
+                if (!is_free(f16[l])) return -1;  // not the free slot the find pass saw
+                end_tomb = st_of(f16[l]) == ST_TOMB;
+                continue;
+            }
+            if (st_of(f16[l]) != ST_OCC) return -1;  // a free slot before F: likewise
+            const long long r = (long long)pos - (long long)dist_of(f16[l]);
+            if (r > H) {
+                if (k == (uint32_t)DX_LCH) return -1;
+                s_pos[k][me] = (uint32_t)(pos & mask);
+                s_dep[k][me] = (uint32_t)((long long)pos - H);
+                ++k;
+                H = r;
+            } else if (r == H) {
+                if (nc == (uint32_t)DX_LCMP) return -1;
+                if (nc == 0) cpos0 = pos, cst0 = k;
+                else cpos1 = pos, cst1 = k;
+                ++nc;
+            }
+        }
+    }
+    // possible updates: the resident keys and the carried keys, one round trip
+    int kind = 1;
+    uint64_t end_slot = e & mask;
+    uint32_t kk = k;
+    if (nc) {
+        RegKey<KB> r0, r1, c0, c1;
+        r0.load_table(t.keys + (cpos0 & mask) * KB, KB);
+        if (cst0) c0.load_table(t.keys + (uint64_t)s_pos[cst0 - 1][me] * KB, KB);
+        else c0 = key;
+        if (nc > 1) {
+            r1.load_table(t.keys + (cpos1 & mask) * KB, KB);
+            if (cst1) c1.load_table(t.keys + (uint64_t)s_pos[cst1 - 1][me] * KB, KB);
+            else c1 = key;
+        }
+        if (c0.same(r0)) {
+            kind = 2, end_slot = cpos0 & mask, kk = cst0;
+        } else if (nc > 1 && c1.same(r1)) {
+            kind = 2, end_slot = cpos1 & mask, kk = cst1;
+        }
+    }
+    // moves, highest first, two per round trip
+    for (int m = (int)kk; m >= 0; m -= 2) {
+        DxRec<KB, VB> ra, rb;
+        const bool vo = kind == 2 && m == (int)kk;  // the update writes the value only
+        const uint64_t da = m < (int)kk ? (uint64_t)s_pos[m][me] : end_slot;
+        if (m == 0) ra.load_in(kin, vin);
+        else ra.load_slot(t, s_pos[m - 1][me], vo);
+        const bool two = m >= 1;
+        uint64_t db = 0;
+        if (two) {
+            db = s_pos[m - 1][me];
+            if (m == 1) rb.load_in(kin, vin);
+            else rb.load_slot(t, s_pos[m - 2][me], false);
+        }
+        ra.store_slot(t, da, vo);
+        if (two) rb.store_slot(t, db, false);
+    }
+    uint32_t md = 0;
+    for (uint32_t i = 0; i < kk; i++) {
+        const uint32_t d = s_dep[i][me];
+        t.flags[s_pos[i][me]] = mk_flag(ST_OCC, d);
+        md = max(md, d);
+    }
+    if (kind == 1) {
+        const uint64_t d = (uint64_t)((long long)e - H);
+        t.flags[end_slot] = mk_flag(ST_OCC, d);
+        md = max(md, (uint32_t)d);
+        acc.tomb = acc.tomb || end_tomb;
+    }
+    acc.maxd = max(acc.maxd, md);
+    return kind == 1 ? 1 : 0;
+}
+
+// The exec pass: one thread per op (uniform trip count per warp, for the
+// warp-aggregated appends).
+template <int KB, int VB>
+__global__ void __launch_bounds__(DX_THREADS, 2) k_dx_exec(TableView t, const uint8_t* __restrict__ keys,
+                                                           const uint8_t* __restrict__ vals, uint32_t n0,
+                                                           OpScratch sc, Ctl* ctl) {
+    __shared__ uint32_t s_pos[DX_LCH][DX_THREADS];
+    __shared__ uint32_t s_dep[DX_LCH][DX_THREADS];
+    __shared__ uint32_t s_tmp[DX_THREADS / 32];
+    dx_wait_prev();
+    dx_let_next();
+    const bool serial = *(volatile uint32_t*)&ctl->serial[0] != 0;
+    const bool lanes_ok = t.mask >= 7 && t.mask < (uint64_t)DIST_MASK;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t iters = (n0 + stride - 1) / stride;
+    ExecAcc a;
+    for (uint32_t it = 0; it < iters; it++) {
+        const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x + it * stride;
+        uint32_t item = 0;
+        bool defer = false;
+        if (j < n0) {
+            const uint64_t F = sc.op_slot[j];
+            if (F != NONE64) {
+                const uint32_t w = t.seg_cnt[F];
+                if (serial) {  // registrations back to idle; the component path runs every op
+                    t.seg_min[F] = IDLE;
+                    t.seg_cnt[F] = 0;
+                    sc.op_word[j] = IDLE;
+                } else if (w == 1u) {  // alone at F, and F in no other op's component
+                    RegKey<KB> key;
+                    key.load(keys + (uint64_t)j * KB, KB);
+                    int c = -1;
+                    if (lanes_ok)
+                        c = dx_lane<KB, VB>(t, key, F, keys + (uint64_t)j * KB, vals + (uint64_t)j * VB, s_pos,
+                                            s_dep, a);
+                    if (c < 0) defer = true, item = j;
+                    else a.claimed += (uint32_t)c;
+                    t.seg_min[F] = IDLE;
+                    t.seg_cnt[F] = 0;
+                    sc.op_word[j] = IDLE;
+                } else if (sc.op_flag[j] && !(w & DX_ABS)) {
+                    defer = true, item = j | DX_ROOT;
+                }
+            }
+        }
+        append(sc.long_list, &ctl->nlong[0], item, defer);
+    }
+    block_add_count(ctl, a.claimed, s_tmp);
+    publish_rare(ctl, a.maxd, a.tomb, a.limit);
+}
+
+// One op on a warp: the tile walk (the scalar walk on small tables).
+template <int KB, int VB>
+__device__ __forceinline__ void dx_run_tile(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t j,
+                                            const Tile<32>& tl, P4Chain<32>& s, ExecAcc& a) {
+    RegKey<KB> key;
+    key.load(keys + (uint64_t)j * KB, KB);
+    if (t.mask >= 4 * 32 - 1) {
+        if (exec_tile<KB, VB, 32, P4Chain<32>>(t, key, vals, j, tl, s, a) == 5) a.limit = true;
+    } else if (tl.lane == 0) {
+        a.claimed += exec_insert_key<KB, VB>(t, key, vals + (uint64_t)j * VB, a);
+    }
+    tl.sync();  // the next op on this warp reads these writes
+}
+
+// The ops of the component led by op j, gathered by lane 0 from the lists of
+// j's free slot F and of every free slot the flow from F reaches (the flow
+// pass's walk again: nothing in the component has run), their registrations
+// and list words set idle on the way; then sorted into index order by the
+// warp.  Returns their count, or 0 when there are more than DX_GATHER (their
+// ops then go to pend[1] for the component path).
+__device__ __noinline__ uint32_t dx_gather(const TableView& t, uint32_t j, uint32_t n0, const OpScratch& sc,
+                                           Ctl* ctl, uint32_t* s_ops, const Tile<32>& tl) {
+    uint32_t g = 0;
+    if (tl.lane == 0) {
+        const uint64_t mask = t.mask;
+        uint64_t F = sc.op_slot[j];
+        uint64_t a = F, budget = mask;
+        uint64_t flow = 0;
+        for (;;) {
+            const uint32_t c = t.seg_cnt[F] & DX_CNT;
+            uint32_t x = t.seg_min[F];
+            if (c) {
+                t.seg_min[F] = IDLE;
+                t.seg_cnt[F] = 0;
+            }
+            for (uint32_t q = 0; q < c && x != IDLE; q++) {
+                if (x >= n0) {
+                    atomicOr(&ctl->err, ERR_SCRATCH);
+                    break;
+                }
+                const uint32_t nx = sc.op_word[x];
+                sc.op_word[x] = IDLE;
+                if (g == (uint32_t)DX_GATHER) {  // too many for this warp: all of them to the component path
+                    const uint32_t at = atomicAdd(&ctl->npend[1], (uint32_t)DX_GATHER);
+                    for (int i = 0; i < DX_GATHER; i++) sc.pend[1][at + i] = s_ops[i];
+                }
+                if (g < (uint32_t)DX_GATHER) s_ops[g] = x;
+                else sc.pend[1][atomicAdd(&ctl->npend[1], 1u)] = x;
+                ++g;
+                x = nx;
+            }
+            flow = flow + c - 1;
+            if (flow == 0) break;
+            const uint64_t at = dx_next_free(t, a + 1, budget);
+            if (at == NONE64) break;  // the flow pass found no wrap: not reached
+            a = at;
+            F = at & mask;
+        }
+    }
+    g = tl.shfl(g, 0);
+    tl.sync();
+    if (g > (uint32_t)DX_GATHER) return 0;
+    const uint32_t lane = tl.lane;
+    const uint32_t v0 = lane < g ? s_ops[lane] : 0u;
+    const uint32_t v1 = lane + 32 < g ? s_ops[lane + 32] : 0u;
+    uint32_t r0 = 0, r1 = 0;
+    for (uint32_t q = 0; q < g; q++) {
+        const uint32_t x = s_ops[q];
+        r0 += x < v0 ? 1u : 0u;
+        r1 += x < v1 ? 1u : 0u;
+    }
+    tl.sync();
+    if (lane < g) s_ops[r0] = v0;
+    if (lane + 32 < g) s_ops[r1] = v1;
+    tl.sync();
+    return g;
+}
+
+// The warp pass: a warp per entry of the list the exec pass built.
+template <int KB, int VB>
+__global__ void __launch_bounds__(RBLOCK, FM_P4_MIN_BLOCKS) k_dx_warp(TableView t, const uint8_t* __restrict__ keys,
+                                                                      const uint8_t* __restrict__ vals, uint32_t n0,
+                                                                      OpScratch sc, Ctl* ctl) {
+    constexpr int NW = RBLOCK / 32;
+    __shared__ P4Chain<32> s_chain[NW];
+    __shared__ uint32_t s_ops[NW][DX_GATHER];
+    __shared__ uint32_t s_tmp[NW];
+    dx_wait_prev();
+    const uint32_t n = *(volatile const uint32_t*)&ctl->nlong[0];
+    if (n == 0) return;  // block-uniform
+    const Tile<32> tl;
+    const uint32_t wi = threadIdx.x >> 5;
+    ExecAcc a;
+    for (uint32_t i = blockIdx.x * NW + wi; i < n; i += gridDim.x * NW) {
+        const uint32_t item = sc.long_list[i];
+        uint32_t g = 1;  // a lone op, or a component's ops in index order
+        if (item & DX_ROOT) {
+            g = dx_gather(t, item & ~DX_ROOT, n0, sc, ctl, s_ops[wi], tl);
+        } else {
+            if (tl.lane == 0) s_ops[wi][0] = item;
+            tl.sync();
+        }
+        for (uint32_t q = 0; q < g; q++) dx_run_tile<KB, VB>(t, keys, vals, s_ops[wi][q], tl, s_chain[wi], a);
+    }
+    block_add_count(ctl, a.claimed, s_tmp);
+    publish_rare(ctl, a.maxd, a.tomb, a.limit);
+}
+
 constexpr int INS_T = 32;  // lanes per insert in the single-block tail
 
 // ---- grouped rounds (batch waves) ------------------------------------------
@@ -2213,6 +2647,61 @@ void comp_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, ui
     count_launches(launches + 6);
 }
 
+// A launch that may start while the stream's previous kernel still runs
+// (programmatic dependent launch; the kernel waits for it in dx_wait_prev),
+// or a plain launch.
+template <class... P, class... A>
+void launch_dependent(void (*k)(P...), unsigned grid, unsigned block, cudaStream_t s, bool pdl, A&&... args) {
+    if (!pdl) {
+        k<<<grid, block, 0, s>>>(std::forward<A>(args)...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
+
+// The direct insert of a call (compile-time shapes): find, flow, exec, warp.
+template <int KB, int VB>
+void direct_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, const OpScratch& sc,
+                  Ctl* ctl, cudaStream_t s) {
+    if constexpr (KB == 0 || VB == 0) {
+        return;
+    } else {
+        const unsigned g = grid_for(n0, 8);
+        // a warp per entry the exec pass may list, up to the blocks resident at once
+        const unsigned gw = grid_for((uint64_t)n0 * 32, FM_P4_MIN_BLOCKS);
+        // with per-kernel timing on, events sit between the kernels, so they
+        // run as plain launches
+        const bool pdl = FM_DX_PDL && !kt_active();
+        {
+            KtScope kt(KC_INS_FIND, s);
+            k_dx_find<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
+        }
+        {
+            KtScope kt(KC_INS_WALK, s);
+            launch_dependent(k_dx_flow, g, RBLOCK, s, pdl, t, n0, sc, ctl);
+        }
+        {
+            KtScope kt(KC_INS_EXEC, s);
+            launch_dependent(k_dx_exec<KB, VB>, g, DX_THREADS, s, pdl, t, keys, vals, n0, sc, ctl);
+        }
+        {
+            KtScope kt(KC_INS_LONG, s);
+            launch_dependent(k_dx_warp<KB, VB>, gw, RBLOCK, s, pdl, t, keys, vals, n0, sc, ctl);
+        }
+        count_launches(4);
+    }
+}
+
 }  // namespace
 
 #define FM_SHAPE_SWITCH(sh, CALL)                 \
@@ -2229,6 +2718,15 @@ cudaError_t launch_ins_rounds(const TableView& t, Shape sh, const uint8_t* keys,
                               uint32_t r0, uint32_t nrounds, uint32_t grid_ops, const OpScratch& sc, Ctl* ctl,
                               cudaStream_t s) {
 #define FM_CALL(K, V) rounds_shape<K, V>(t, keys, vals, n0, r0, nrounds, grid_ops, n0, sc, ctl, s)
+    FM_SHAPE_SWITCH(sh, FM_CALL)
+#undef FM_CALL
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ins_direct(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
+                              const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+    if (sh == SHAPE_GENERIC || !sc.comp) return cudaErrorInvalidValue;
+#define FM_CALL(K, V) direct_shape<K, V>(t, keys, vals, n0, sc, ctl, s)
     FM_SHAPE_SWITCH(sh, FM_CALL)
 #undef FM_CALL
     return cudaGetLastError();

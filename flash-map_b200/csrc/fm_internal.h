@@ -102,6 +102,15 @@ cudaError_t launch_get(const TableView& t, Shape sh, const uint8_t* qkeys, uint6
 cudaError_t launch_ins_rounds(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
                               uint32_t r0, uint32_t nrounds, uint32_t grid_ops, const OpScratch& sc, Ctl* ctl,
                               cudaStream_t s);
+// A whole insert call of n0 ops without rounds (compile-time record shapes,
+// a table with a component buffer): ops alone at their first free slot run
+// at once, the ops that share free slots (components) run in index order on
+// a warp each.  On return (stream-ordered) Ctl::serial[0] set means nothing
+// ran and every op is left to launch_ins_comp at round 0; otherwise
+// Ctl::npend[1] ops (components too large for a warp) are left in pend[1]
+// for launch_ins_comp at round 1.
+cudaError_t launch_ins_direct(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
+                              const OpScratch& sc, Ctl* ctl, cudaStream_t s);
 // Runs every remaining round starting at r in one block if the pending count
 // is at most TAIL_MAX; otherwise returns without touching anything.  With
 // handoff, rounds that stop progressing are left pending for the host
@@ -204,10 +213,10 @@ cudaError_t launch_grp_pending_each(const GroupOp* ops, uint32_t nops, uint32_t 
 // calling thread (no events otherwise).
 enum KernelClass : int {
     KC_GET = 0,     // k_get_thread / k_get
-    KC_INS_FIND,    // k_ins_p1: first free slot, segment registration
-    KC_INS_WALK,    // k_ins_p2: leaders and flow bounds
-    KC_INS_EXEC,    // k_ins_p3: thread-per-op execution
-    KC_INS_LONG,    // k_ins_p4: warp-per-op execution of long walks
+    KC_INS_FIND,    // k_dx_find / k_ins_p1: first free slot, registration
+    KC_INS_WALK,    // k_dx_flow / k_ins_p2: flows over the free slots
+    KC_INS_EXEC,    // k_dx_exec / k_ins_p3: thread-per-op execution
+    KC_INS_LONG,    // k_dx_warp / k_ins_p4: warp-per-op execution (long walks, components)
     KC_INS_TAIL,    // k_ins_tail: remaining rounds in one block
     KC_INS_SERIAL,  // k_ins_serial
     KC_REM_MARK,    // k_rem_p1
@@ -218,6 +227,7 @@ enum KernelClass : int {
     KC_N
 };
 void kt_mark(int cls, bool begin, cudaStream_t s);
+bool kt_active();  // per-kernel timing is on for the calling thread's current call
 struct KtScope {
     int c;
     cudaStream_t s;

@@ -95,3 +95,99 @@ def test_components_commute_round_the_ring(seed):
     assert whole == parts
     for x, y in zip(a.snapshot(), b.snapshot()):
         assert np.array_equal(x, y)
+
+
+def direct_groups(flags, homes, cap):
+    """The grouping of the direct insert (k_dx_find / k_dx_flow / k_dx_exec /
+    k_dx_warp in flash-map_b200/csrc/fm_insert.cu), restated: every op's
+    first free slot F; the ops at each F; from every F holding c >= 2 ops a
+    flow walk over the following free slots carrying c - 1, each slot taking
+    one op and adding its own, which marks every later F it reaches; then an
+    op alone at an unmarked F is its own group, and an unmarked F with c >= 2
+    leads a group of the ops of every F its flow reaches.  Returns the groups
+    (op indices in index order), or None where the device hands the whole call
+    to the component path (an op with no free slot, a flow round the ring)."""
+    st = flags & 0xF
+    fidx = np.nonzero((st == 0) | (st == 2))[0]
+    if len(fidx) == 0:
+        return None
+    pos = np.searchsorted(fidx, homes)
+    F = fidx[np.where(pos < len(fidx), pos, 0)]
+    ops_at = {}
+    for j, f in enumerate(F):
+        ops_at.setdefault(int(f), []).append(j)
+    nxt = {int(fidx[i]): int(fidx[(i + 1) % len(fidx)]) for i in range(len(fidx))}
+
+    def chain(f0):
+        out, f, flow = [f0], f0, len(ops_at[f0]) - 1
+        while flow > 0:
+            f = nxt[f]
+            if f == f0:
+                return None  # the carry comes back round the ring
+            out.append(f)
+            flow += len(ops_at.get(f, [])) - 1
+        return out
+
+    marked = set()
+    for f, ops in ops_at.items():
+        if len(ops) >= 2:
+            ch = chain(f)
+            if ch is None:
+                return None
+            marked.update(x for x in ch[1:] if x in ops_at)
+    groups = []
+    for f, ops in ops_at.items():
+        if f in marked:
+            continue
+        if len(ops) == 1:
+            groups.append(np.array(ops))
+        else:
+            groups.append(np.array(sorted(j for x in chain(f) for j in ops_at.get(x, []))))
+    return groups
+
+
+@pytest.mark.parametrize("case", [(1 << 12, 0.5, 0.1, 0.0), (1 << 12, 0.8, 0.05, 0.0), (1 << 13, 0.85, 0.1, 0.0),
+                                  (1 << 13, 0.8, 0.08, 0.3), (1 << 12, 0.9, 0.05, 0.2)])
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_direct_groups_commute(case, seed):
+    """Every op lands in exactly one group of the direct insert, and running
+    the groups one after another in a shuffled order gives the same counts
+    and the same table, slot for slot, as the batch in index order."""
+    cap, load0, frac, rm = case
+    rng = np.random.default_rng(50 + seed)
+    a, b = OracleAdapter(cap, 8, 8), OracleAdapter(cap, 8, 8)
+    pk = rng.integers(0, 256, (int(cap * load0), 8), dtype=np.uint8)
+    for m in (a, b):
+        m.bulk_insert(pk, pk)
+    if rm:
+        r = pk[rng.choice(len(pk), int(len(pk) * rm), replace=False)]
+        assert a.bulk_remove(r) == b.bulk_remove(r)
+    n = int(cap * frac)
+    k = rng.integers(0, 256, (n, 8), dtype=np.uint8)
+    k[rng.choice(n, n // 10)] = k[rng.integers(0, n, n // 10)]  # in-batch duplicates
+    k[rng.choice(n, n // 10)] = pk[rng.integers(0, len(pk), n // 10)]  # updates
+    v = rng.integers(0, 256, (n, 8), dtype=np.uint8)
+    homes = (k.view("<u8").reshape(-1) & np.uint64(cap - 1)).astype(np.int64)
+    groups = direct_groups(a.snapshot()[0].astype(np.int64), homes, cap)
+    assert groups is not None
+    allops = np.sort(np.concatenate(groups))
+    assert np.array_equal(allops, np.arange(n))
+    assert sum(len(g) == 1 for g in groups) > len(groups) // 2  # mostly lone ops
+    whole = a.bulk_insert(k, v)
+    parts = 0
+    for gi in rng.permutation(len(groups)):
+        parts += b.bulk_insert(k[groups[gi]], v[groups[gi]])
+    assert whole == parts
+    for x, y in zip(a.snapshot(), b.snapshot()):
+        assert np.array_equal(x, y)
+
+
+def test_direct_groups_hand_a_ring_flow_to_the_component_path():
+    """A batch whose flow would come back round the whole ring: the direct
+    insert leaves it to the component path (Ctl::serial[0])."""
+    cap = 64
+    flags = np.zeros(cap, np.int64)
+    flags[:] = 1  # occupied, distance 0
+    flags[[5, 40]] = 0  # two free slots
+    homes = np.array([3, 4, 3], np.int64)  # three ops at slot 5: a carry of 2, one slot after it
+    assert direct_groups(flags, homes, cap) is None
