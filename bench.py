@@ -652,7 +652,8 @@ def batched_leg(torch, F, native, dev, steps, warmup, scale=1):
 # ---------------------------------------------------------------------------
 # Served form: Poisson request stream against a device-resident table
 # ---------------------------------------------------------------------------
-SERVE_RATE, SERVE_REQS = 2000.0, 500
+SERVE_RATE, SERVE_REQS, SERVE_SAT_REQS = 2000.0, 2000, 500
+SERVE_INSERT_POOL = 16_000_000  # fresh insert keys, taken in turn (later passes update)
 
 
 def served_leg(torch, F, dev, scale=1):
@@ -661,11 +662,16 @@ def served_leg(torch, F, dev, scale=1):
     Poisson stream at 2,000/s, each insert / get / remove with probability
     0.3 / 0.6 / 0.1 and a size log-uniform in 64..1M keys, get and remove keys
     80% present (Zipf s=0.9 over a 4M-key sample of the present keys); 20 GB
-    staging budget.  500 requests (a quarter second of arrivals), served with
-    continuous batching and, from the same start state (a device copy), by
-    the plain one-call-per-request server.  Request inputs are slices of
-    pinned host pools (inserts: fresh keys; gets/removes: the skewed mix)."""
-    from flash_map.serve import FlashMapServer, PlainServer, Request, latency_summary
+    staging budget (admitted against free HBM).  2,000 requests (one second
+    of arrivals) are served in real time with continuous batching and, from
+    the same start state (a device copy), by the plain one-call-per-request
+    server through AsyncFlashMap; then the first 500 requests arrive all at
+    once (saturation) for both, which gives each form's throughput.  Request
+    inputs are slices of pinned host pools (inserts: a pool of 16M fresh keys
+    taken in turn, so later passes update; gets/removes: the skewed mix); get
+    results land in one shared pinned buffer (timing only; the results
+    compared between the forms are the per-request counts and statuses)."""
+    from flash_map.serve import AsyncPlainServer, FlashMapServer, Request, latency_summary
 
     # earlier legs' buffers and the allocator's cached blocks go first: under
     # memory pressure one staging allocation can stall the host for 100 ms
@@ -690,12 +696,11 @@ def served_leg(torch, F, dev, scale=1):
     kinds = rng.choice([1, 0, 2], size=n_req, p=[0.3, 0.6, 0.1])
     sizes = np.exp(rng.uniform(np.log(64), np.log(1_000_000 // scale), n_req)).astype(np.int64)
     arrivals = np.cumsum(rng.exponential(1.0 / SERVE_RATE, n_req))
-    n_ins = int(sizes[kinds == 1].sum())
-    n_look = int(sizes[kinds != 1].sum())
-    ins_k = torch.randint(0, 256, (n_ins, KB), dtype=torch.uint8).pin_memory().numpy()
-    ins_v = torch.randint(0, 256, (n_ins, VB), dtype=torch.uint8).pin_memory().numpy()
+    pool_i = SERVE_INSERT_POOL // scale
+    ins_k = torch.randint(0, 256, (pool_i, KB), dtype=torch.uint8).pin_memory().numpy()
+    ins_v = torch.randint(0, 256, (pool_i, VB), dtype=torch.uint8).pin_memory().numpy()
     # lookup pool: 80% present with Zipf(0.9) ranks (inverse CDF of r^-0.9), 20% fresh
-    pool_n = min(n_look, 24_000_000 // scale)
+    pool_n = 24_000_000 // scale
     ranks = np.minimum((rng.random(pool_n) ** 10 * len(sample)).astype(np.int64), len(sample) - 1)
     look = sample[ranks]
     fresh = rng.random(pool_n) < 0.2
@@ -704,52 +709,74 @@ def served_leg(torch, F, dev, scale=1):
     out_v = torch.empty((1_000_000 // scale + 1, VB), dtype=torch.uint8).pin_memory()
     out_f = torch.empty((1_000_000 // scale + 1,), dtype=torch.uint8).pin_memory()
 
-    def requests():
+    def requests(count, at_once):
         reqs, io, lo = [], 0, 0
-        for i in range(n_req):
+        for i in range(count):
             n = int(sizes[i])
+            t = 0.0 if at_once else float(arrivals[i])
             if kinds[i] == 1:
-                reqs.append(Request(1, ins_k[io:io + n], ins_v[io:io + n], float(arrivals[i])))
+                if io + n > pool_i:
+                    io = 0
+                reqs.append(Request(1, ins_k[io:io + n], ins_v[io:io + n], t))
                 io += n
             else:
                 if lo + n > pool_n:
                     lo = 0
-                reqs.append(Request(int(kinds[i]), look[lo:lo + n], None, float(arrivals[i])))
+                reqs.append(Request(int(kinds[i]), look[lo:lo + n], None, t))
                 lo += n
         return reqs
 
-    torch.cuda.synchronize()
-    total_keys = int(sizes.sum())
-    out = {"workload": f"{n_req} requests, Poisson {SERVE_RATE:.0f}/s, insert/get/remove 0.3/0.6/0.1, sizes "
-                       f"log-uniform 64..{1_000_000 // scale}, 80% present Zipf(0.9) on get/remove, table "
-                       f"with_capacity({cap_req}) prefilled with {prefill}, 20 GB staging budget",
-           "keys": total_keys}
-    def quiet(serve, reqs):
+    def quiet(serve, reqs, realtime):
         # no garbage collection while requests are timed: freeing another
         # leg's pinned buffers can stall the host for a long time
         gc.collect()
         torch.cuda.synchronize()
         gc.disable()
         try:
-            return serve(reqs, realtime=True)
+            return serve(reqs, realtime=realtime)
         finally:
             gc.enable()
 
-    reqs_s = requests()
-    srv = FlashMapServer(m, budget=20 << 30, out_pool=lambda n, v: (out_v[:n], out_f[:n]))
-    srv.warmup()  # first-use costs outside the timing (the plain path's kernels ran in earlier legs)
-    wall = quiet(srv.serve, reqs_s)
-    out["served"] = dict(latency_summary(reqs_s), mops=round(total_keys / wall / 1e6, 3), wall_s=round(wall, 3),
-                         batches=srv.batches, mean_requests_per_batch=round(n_req / max(srv.batches, 1), 2))
-    del srv  # its staging buffer goes before the plain server runs
-    m.copy_from(backup)
+    def restore():
+        m.copy_from(backup)
+        torch.cuda.synchronize()
+        gc.collect()
+
     torch.cuda.synchronize()
+    out = {"workload": f"{n_req} requests, Poisson {SERVE_RATE:.0f}/s, insert/get/remove 0.3/0.6/0.1, sizes "
+                       f"log-uniform 64..{1_000_000 // scale}, 80% present Zipf(0.9) on get/remove, table "
+                       f"with_capacity({cap_req}) prefilled with {prefill}, 20 GB staging budget against free "
+                       f"HBM; saturation: the first {SERVE_SAT_REQS} requests all at t=0",
+           "keys": int(sizes.sum()), "keys_saturated": int(sizes[:SERVE_SAT_REQS].sum())}
+    srv = FlashMapServer(m, budget=20 << 30, out_pool=lambda n, v: (out_v[:n], out_f[:n]))
+    out["staging_bytes"] = srv.staging_bytes
+    srv.warmup()  # first-use costs outside the timing (the plain path's kernels ran in earlier legs)
+    runs = {}
+    for name, count, at_once in (("realtime", n_req, False), ("saturated", SERVE_SAT_REQS, True)):
+        restore()
+        srv.batches = 0
+        rs = requests(count, at_once)
+        wall = quiet(srv.serve, rs, not at_once)
+        keys = int(sizes[:count].sum())
+        served = dict(latency_summary(rs), mops=round(keys / wall / 1e6, 3), wall_s=round(wall, 3),
+                      batches=srv.batches, mean_requests_per_batch=round(count / max(srv.batches, 1), 2))
+        runs[name] = (rs, served)
+    del srv  # its staging buffer goes before the plain server runs
     gc.collect()
     torch.cuda.empty_cache()
-    reqs_p = requests()
-    wall_p = quiet(PlainServer(m, out_pool=lambda n, v: (out_v[:n].numpy(), out_f[:n].numpy())).serve, reqs_p)
-    out["plain"] = dict(latency_summary(reqs_p), mops=round(total_keys / wall_p / 1e6, 3), wall_s=round(wall_p, 3))
-    out["identical_results"] = all((a.result, a.status) == (b.result, b.status) for a, b in zip(reqs_s, reqs_p))
+    plain = AsyncPlainServer(m, out_pool=lambda n, v: (out_v[:n].numpy(), out_f[:n].numpy()))
+    for name, count, at_once in (("realtime", n_req, False), ("saturated", SERVE_SAT_REQS, True)):
+        restore()
+        rp = requests(count, at_once)
+        wall_p = quiet(plain.serve, rp, not at_once)
+        keys = int(sizes[:count].sum())
+        rs, served = runs[name]
+        out[name] = {
+            "served": served,
+            "plain_async": dict(latency_summary(rp), mops=round(keys / wall_p / 1e6, 3), wall_s=round(wall_p, 3)),
+            "served_vs_plain_mops": round(served["mops"] / (keys / wall_p / 1e6), 3),
+            "identical_results": all((a.result, a.status) == (b.result, b.status) for a, b in zip(rs, rp)),
+        }
     m.close()
     backup.close()
     return out

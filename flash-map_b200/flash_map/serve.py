@@ -134,14 +134,21 @@ class _Ring:
             self.head = 0
 
 
-class FlashMapServer:
-    """Continuous batching over one FlashMap.  `budget` bounds the device
-    bytes staged for admitted, unfinished pieces: they are carved from a
-    staging buffer of min(budget, ring_bytes) bytes that the server owns; a
-    piece larger than it is served alone once everything before it has
-    finished."""
+# Device memory the server leaves free beside its staging buffer (kernel
+# scratch, the framework's other buffers): a tenth of what is free, at most
+# 2 GiB.
+HEADROOM_MAX = 2 << 30
 
-    def __init__(self, table: FlashMap, budget: int = 20 << 30, out_pool=None, ring_bytes: int = 4 << 30):
+
+class FlashMapServer:
+    """Continuous batching over one FlashMap.  Requests are admitted against
+    device memory: the staging buffer the server owns is the budget, or the
+    free HBM (cudaMemGetInfo) less a headroom when less is free, and at most
+    `ring_bytes` when given.  The device bytes staged for admitted, unfinished
+    pieces are carved from it; a piece larger than it is served alone once
+    everything before it has finished."""
+
+    def __init__(self, table: FlashMap, budget: int = 20 << 30, out_pool=None, ring_bytes: Optional[int] = None):
         import torch
 
         self.t = table
@@ -149,11 +156,13 @@ class FlashMapServer:
         self.torch = torch
         self.dev = torch.device("cuda", table.device())
         self.copy_stream = torch.cuda.Stream(self.dev)
-        # staging space owned by the server (min(budget, ring_bytes)): pieces
-        # are carved from it, so staging never waits on the framework's
-        # allocator; a piece larger than it is staged on its own
+        free = torch.cuda.mem_get_info(self.dev)[0]
+        room = max(256, free - min(HEADROOM_MAX, free // 10))
+        self.staging_bytes = min(budget, room, ring_bytes if ring_bytes is not None else budget)
+        # pieces are carved from staging space the server owns, so staging
+        # never waits on the framework's allocator
         with torch.cuda.stream(self.copy_stream):
-            self._ring = _Ring(torch.empty(max(256, min(budget, ring_bytes)) & ~255, dtype=torch.uint8,
+            self._ring = _Ring(torch.empty(max(256, self.staging_bytes) & ~255, dtype=torch.uint8,
                                            device=self.dev))
         self.stream = torch.cuda.Stream(self.dev)
         self.down_stream = torch.cuda.Stream(self.dev)
@@ -427,6 +436,78 @@ class PlainServer:
                 r.result = self.t.bulk_remove(r.keys)
             r.done = time.perf_counter() - t0
         return time.perf_counter() - t0
+
+
+class AsyncPlainServer:
+    """Per-request plain calls through :class:`~flash_map.AsyncFlashMap`, as
+    the reference's async wrapper serves them (src/async_map.rs:48-93): each
+    request is one host-API bulk call run off the event loop under the
+    wrapper's reader/writer lock, issued when it arrives, so gets overlap one
+    another while inserts and removes run alone.  Every request also waits
+    for the earlier requests it conflicts with -- a write for all of them, a
+    get for the earlier writes -- so each result is its arrival-order result,
+    the same as :class:`FlashMapServer` gives."""
+
+    def __init__(self, table: FlashMap, out_pool=None, workers: int = 8):
+        self.t = table
+        self.out_pool = out_pool  # optional callable(n, V) -> (host vals, host found) buffers for get results
+        self.workers = workers
+
+    def serve(self, requests: List[Request], realtime: bool = True) -> float:
+        import asyncio
+        from concurrent.futures import ThreadPoolExecutor
+
+        from .async_map import AsyncFlashMap
+
+        am = AsyncFlashMap(self.t)
+        V = self.t.value_size
+
+        async def one(r: Request, deps, t0):
+            if deps:
+                await asyncio.gather(*deps)
+            if r.kind == GET:
+                if self.out_pool is not None:
+                    hv, hf = self.out_pool(r.n, V)
+                    hv, hf = np.asarray(hv), np.asarray(hf)
+                    await am._run(False, lambda: self.t.bulk_get(r.keys, out_values=hv, out_found=hf))
+                    r.out_values, r.out_found = hv, hf
+                else:
+                    vals, found = await am.bulk_get(r.keys)
+                    r.out_values, r.out_found = vals, found.astype(np.uint8)
+            elif r.kind == INSERT:
+                try:
+                    r.result = await am.bulk_insert(r.keys, r.values)
+                except TableFull:
+                    r.result, r.status = 0, FM_ERR_TABLE_FULL
+            else:
+                r.result = await am.bulk_remove(r.keys)
+            r.done = time.perf_counter() - t0
+
+        async def main():
+            loop = asyncio.get_running_loop()
+            loop.set_default_executor(ThreadPoolExecutor(max_workers=self.workers))
+            t0 = time.perf_counter()
+            last_write = None
+            reads = []
+            tasks = []
+            for r in requests:
+                if realtime:
+                    wait = r.arrival - (time.perf_counter() - t0)
+                    if wait > 0:
+                        await asyncio.sleep(wait)
+                if r.kind == GET:
+                    deps = [last_write] if last_write is not None else []
+                    task = asyncio.ensure_future(one(r, deps, t0))
+                    reads.append(task)
+                else:
+                    deps = ([last_write] if last_write is not None else []) + reads
+                    task = asyncio.ensure_future(one(r, deps, t0))
+                    last_write, reads = task, []
+                tasks.append(task)
+            await asyncio.gather(*tasks)
+            return time.perf_counter() - t0
+
+        return asyncio.run(main())
 
 
 def latency_summary(requests: List[Request]) -> dict:
