@@ -98,10 +98,20 @@ def test_transfer_failure_in_get_leaves_table_unchanged():
     assert found.all() and np.array_equal(vals, k)
 
 
+def _clustered(cap, n, first_home, span, ks):
+    """n keys whose identity-hash homes lie in [first_home, first_home + span):
+    a run of n entries, so stored distances reach about n."""
+    homes = first_home + (np.arange(n, dtype=np.uint64) % np.uint64(span))
+    x = (np.arange(n, dtype=np.uint64) + np.uint64(1)) * np.uint64(cap) + homes
+    out = np.zeros((n, ks), np.uint8)
+    out[:, :8] = x.view(np.uint8).reshape(n, 8)
+    return out
+
+
 @pytest.mark.parametrize("shape", [(8, 8), (32, 128)])
 def test_failed_remove_with_chunk_summaries_then_remove(shape):
-    """A remove on a near-full table (largest stored distance far above 256,
-    so the call builds per-chunk summaries and marks) fails after its first
+    """A remove on a table whose largest stored distance is far above 256
+    (so the call builds per-chunk summaries and marks) fails after its first
     pass of rounds; the next removes on the table must still make progress
     and match the oracle from the state the failure left."""
     import flash_map as F
@@ -110,8 +120,9 @@ def test_failed_remove_with_chunk_summaries_then_remove(shape):
     ks, vs = shape
     cap = 1 << 14
     rng = np.random.default_rng(4 + ks)
-    k = rng.integers(0, 256, (cap - 8, ks), dtype=np.uint8)
-    v = rng.integers(0, 256, (cap - 8, vs), dtype=np.uint8)
+    k = np.concatenate([_clustered(cap, 1500, 300, 40, ks),
+                        rng.integers(0, 256, (cap // 2, ks), dtype=np.uint8)])
+    v = rng.integers(0, 256, (len(k), vs), dtype=np.uint8)
     g = F.FlashMap(cap, ks, vs)
     o = OracleAdapter(cap, ks, vs)
     assert g.bulk_insert(k, v) == o.bulk_insert(k, v)
