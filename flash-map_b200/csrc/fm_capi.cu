@@ -317,10 +317,30 @@ int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t
         const uint8_t* kk = d_k + base * t->ksz;
         const uint8_t* vv = d_v ? d_v + base * t->vsz : nullptr;
         cudaError_t e = cudaMemsetAsync(t->d_ctl, 0, fm::CTL_CALL_BYTES, s);
-        if (e == cudaSuccess && !insert) e = fm::launch_rem_summary(v, t->sc, t->d_ctl, s);
         if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "round setup", e);
         uint32_t r = 0;
         uint32_t left = m;
+        if (!insert) {
+            // no rounds: ops grouped by the first EMPTY slot after their home
+            // (lone ops at once, each group in index order); ops the kernels
+            // leave (no EMPTY slot anywhere, groups too large) run in rounds
+            e = fm::launch_rem_direct(v, sh, kk, m, t->sc, t->d_ctl, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e == cudaSuccess && fault_at(FM_FAULT_ROUND)) e = cudaErrorLaunchFailure;
+            if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "remove", e);
+            if (t->h_ctl->err & fm::ERR_SCRATCH) return fail(FM_ERR_KERNEL_LAUNCH, "stale segment registration");
+            r = t->h_ctl->serial[0] ? 0u : 1u;
+            left = t->h_ctl->serial[0] ? m : t->h_ctl->npend[1];
+            if (left == 0) {
+                total += t->h_ctl->total_count();
+                *err_bits |= t->h_ctl->err;
+                t->last_rounds = 0;
+                continue;
+            }
+            e = fm::launch_rem_summary(v, t->sc, t->d_ctl, s);
+            if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "round setup", e);
+        }
         // a chunk that can take the table to FM_DIRECT_LOAD or beyond runs as
         // components from the start: rounds stall there, and their tiles'
         // short chain buffers walk chains of thousands of entries again and

@@ -128,6 +128,14 @@ cudaError_t launch_ins_serial(const TableView& t, Shape sh, const uint8_t* keys,
 // launch_ins_serial.
 cudaError_t launch_ins_comp(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
                             uint32_t r, uint32_t npend, const OpScratch& sc, Ctl* ctl, cudaStream_t s);
+// A whole remove call of n0 ops without rounds: ops grouped by the first
+// EMPTY slot at or after their home, lone ops run at once, each group in
+// index order on one thread.  On return (stream-ordered) Ctl::serial[0] set
+// means nothing ran (an op found no EMPTY slot) and every op is left to the
+// rounds from round 0; otherwise Ctl::npend[1] ops (groups too large for one
+// thread) are left in pend[1] for the rounds from round 1.
+cudaError_t launch_rem_direct(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, const OpScratch& sc,
+                              Ctl* ctl, cudaStream_t s);
 cudaError_t launch_rem_rounds(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, uint32_t r0,
                               uint32_t nrounds, uint32_t grid_ops, const OpScratch& sc, Ctl* ctl, cudaStream_t s);
 cudaError_t launch_rem_tail(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, uint32_t r,

@@ -517,6 +517,191 @@ void rounds_shape(const TableView& t, const uint8_t* keys, uint32_t n0, uint32_t
     count_launches(3 * nrounds);
 }
 
+// ---- direct remove: groups between EMPTY slots ------------------------------
+//
+// A remove's probe (rayon_cpu.rs:273-328) reads only [home, E], E the first
+// EMPTY slot at or after its home, and writes at most one slot of it (the
+// whole word TOMBSTONE).  Removes make no EMPTY slot, so E stays the same for
+// the whole call, and ops with different E read and write disjoint slots.
+// So the ops are grouped by E, without rounds:
+//   find (a thread per op)  E, then the op joins E's list: seg_cnt[E] counts
+//        the ops at E, seg_min[E] heads a list linked through op_word, and
+//        the first op to arrive leads E (op_flag 1).
+//   exec (a thread per op)  an op alone at its E runs its probe at once; the
+//        leader of an E with c >= 2 ops gathers them from the list, orders
+//        them by index and runs their probes one after another.
+// A call where some op finds no EMPTY slot (its probe could go round the
+// table) leaves every op to the rounds (Ctl::serial[0]); a group of more than
+// RX_GATHER ops leaves its ops to them (pend[1], Ctl::npend[1]).  Every
+// registration and list word is idle again when the two kernels end.
+constexpr uint32_t RX_GATHER = 32;
+
+// First EMPTY slot at or after home h, NONE64 when the table has none (two
+// aligned 8-slot windows per round trip with capacity >= 8).
+__device__ __forceinline__ uint64_t rx_first_empty(const TableView& t, uint64_t h) {
+    const uint64_t mask = t.mask;
+    if (mask >= 7) {
+        uint64_t wb = h & ~7ull;
+        for (uint64_t w = 0; w <= (mask >> 4) + 1; ++w, wb += 16) {
+            const uint4* p0 = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
+            const uint4* p1 = reinterpret_cast<const uint4*>(t.flags + ((wb + 8) & mask));
+            const uint4 a = p0[0], b = p0[1], c = p1[0], d = p1[1];
+            const uint32_t f16[16] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w};
+#pragma unroll
+            for (int l = 0; l < 16; l++) {
+                const uint64_t pos = wb + l;
+                if (pos < h) continue;
+                if (pos - h > mask) return NONE64;
+                if (st_of(f16[l]) == ST_EMPTY) return pos & mask;
+            }
+        }
+        return NONE64;
+    }
+    for (uint64_t p = 0; p <= mask; ++p)
+        if (st_of(t.flags[(h + p) & mask]) == ST_EMPTY) return (h + p) & mask;
+    return NONE64;
+}
+
+// The sequential remove of one key (rayon_cpu.rs:273-328): skip TOMBSTONEs,
+// stop at EMPTY or at the Robin Hood exit (OCCUPIED with depth > stored
+// distance), and turn the first OCCUPIED slot holding the key (its stored
+// distance equal to the depth) into the whole word TOMBSTONE.  Returns 1 when
+// it did.
+template <int KB>
+__device__ __forceinline__ uint32_t rx_probe(const TableView& t, const RegKey<KB>& key, uint64_t h) {
+    const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
+    const uint64_t mask = t.mask;
+    if (mask >= 7) {
+        for (uint64_t wb = h & ~7ull;; wb += 8) {
+            const uint4* fp = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
+            const uint4 a = fp[0], b = fp[1];
+            const uint32_t f8[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int l = 0; l < 8; l++) {
+                const uint64_t pos = wb + l;
+                if (pos < h) continue;
+                const uint64_t p = pos - h;
+                if (p > mask) return 0;
+                const uint32_t f = f8[l];
+                const uint32_t st = st_of(f);
+                if (st == ST_EMPTY) return 0;
+                if (st == ST_OCC) {
+                    if (p > dist_of(f)) return 0;
+                    const uint64_t slot = pos & mask;
+                    if (dist_matches(f, p) && key.eq(t.keys + slot * ksz, ksz)) {
+                        t.flags[slot] = ST_TOMB;
+                        return 1;
+                    }
+                }
+            }
+        }
+    }
+    for (uint64_t p = 0; p <= mask; ++p) {
+        const uint64_t slot = (h + p) & mask;
+        const uint32_t f = t.flags[slot];
+        const uint32_t st = st_of(f);
+        if (st == ST_EMPTY) return 0;
+        if (st == ST_OCC) {
+            if (p > dist_of(f)) return 0;
+            if (dist_matches(f, p) && key.eq(t.keys + slot * ksz, ksz)) {
+                t.flags[slot] = ST_TOMB;
+                return 1;
+            }
+        }
+    }
+    return 0;
+}
+
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_rx_find(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
+                                                    OpScratch sc, Ctl* ctl) {
+    bool no_empty = false;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n0; j += gridDim.x * blockDim.x) {
+        RegKey<KB> key;
+        const uint64_t E = rx_first_empty(t, home_of<KB>(t, keys, j, key));
+        sc.op_slot[j] = E;
+        uint8_t lead = 0;
+        uint32_t next = IDLE;
+        if (E == NONE64) {
+            no_empty = true;
+        } else {
+            lead = atomicAdd(&t.seg_cnt[E], 1u) == 0u ? 1 : 0;
+            next = atomicExch(&t.seg_min[E], j);
+        }
+        sc.op_word[j] = next;
+        sc.op_flag[j] = lead;
+    }
+    if (no_empty) ctl->serial[0] = 1u;
+}
+
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_rx_exec(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
+                                                    OpScratch sc, Ctl* ctl) {
+    __shared__ uint32_t s_tmp[RBLOCK / 32];
+    const bool serial = *(volatile uint32_t*)&ctl->serial[0] != 0;
+    uint32_t removed = 0;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t iters = (n0 + stride - 1) / stride;
+    for (uint32_t it = 0; it < iters; it++) {
+        const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x + it * stride;
+        if (j >= n0) continue;
+        const uint64_t E = sc.op_slot[j];
+        if (E == NONE64) continue;
+        if (serial) {  // registrations back to idle; the rounds run every op
+            t.seg_min[E] = IDLE;
+            t.seg_cnt[E] = 0;
+            sc.op_word[j] = IDLE;
+            continue;
+        }
+        if (!sc.op_flag[j]) continue;  // the leader of E runs this op
+        const uint32_t c = t.seg_cnt[E];
+        uint32_t ops[RX_GATHER];
+        uint32_t x = t.seg_min[E];
+        uint32_t g = 0;
+        for (uint32_t q = 0; q < c && x != IDLE; q++) {
+            if (x >= n0) {  // registrations come only from this call's ops
+                atomicOr(&ctl->err, ERR_SCRATCH);
+                break;
+            }
+            const uint32_t nx = sc.op_word[x];
+            sc.op_word[x] = IDLE;
+            if (c <= RX_GATHER) ops[g++] = x;
+            else sc.pend[1][atomicAdd(&ctl->npend[1], 1u)] = x;
+            x = nx;
+        }
+        t.seg_min[E] = IDLE;
+        t.seg_cnt[E] = 0;
+        // index order (insertion sort of at most RX_GATHER ops), then the probes
+        for (uint32_t a = 1; a < g; a++) {
+            const uint32_t v = ops[a];
+            uint32_t b = a;
+            for (; b > 0 && ops[b - 1] > v; --b) ops[b] = ops[b - 1];
+            ops[b] = v;
+        }
+        for (uint32_t q = 0; q < g; q++) {
+            RegKey<KB> key;
+            const uint64_t h = home_of<KB>(t, keys, ops[q], key);
+            removed += rx_probe<KB>(t, key, h);
+        }
+    }
+    block_add_count(ctl, removed, s_tmp);
+}
+
+template <int KB>
+void direct_shape(const TableView& t, const uint8_t* keys, uint32_t n0, const OpScratch& sc, Ctl* ctl,
+                  cudaStream_t s) {
+    const unsigned g = grid_for(n0, 8);
+    {
+        KtScope kt(KC_REM_MARK, s);
+        k_rx_find<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
+    }
+    {
+        KtScope kt(KC_REM_EXEC, s);
+        k_rx_exec<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
+    }
+    count_launches(2);
+}
+
 }  // namespace
 
 cudaError_t launch_rem_rounds(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, uint32_t r0,
@@ -542,6 +727,19 @@ cudaError_t launch_grp_rem(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t
         case SHAPE_32_64:
         case SHAPE_32_32: grp_rem_shape<32>(ops, nops, sum_n, phase, r0, nrounds, s); break;
         default: grp_rem_shape<0>(ops, nops, sum_n, phase, r0, nrounds, s); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rem_direct(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, const OpScratch& sc,
+                              Ctl* ctl, cudaStream_t s) {
+    switch (sh) {
+        case SHAPE_8_8:
+        case SHAPE_8_32: direct_shape<8>(t, keys, n0, sc, ctl, s); break;
+        case SHAPE_32_128:
+        case SHAPE_32_64:
+        case SHAPE_32_32: direct_shape<32>(t, keys, n0, sc, ctl, s); break;
+        default: direct_shape<0>(t, keys, n0, sc, ctl, s); break;
     }
     return cudaGetLastError();
 }
