@@ -1233,6 +1233,26 @@ struct fm_batch {
     uint8_t* h_io = nullptr;               // pinned: len[tables], res[ops], status[ops]
     uint32_t* d_pend = nullptr;            // pending counts (eager runs): GROUP_MAX + 1 words
     uint32_t* h_pend = nullptr;
+    // Queue mode (every op of a compile-time record shape): the ops run as
+    // chains of phases drained by one persistent launch per record shape and
+    // segment; an insert that can take its table to FM_DIRECT_LOAD closes the
+    // segment and runs on the component path between launches.
+    bool qmode = false;
+    struct QStep {
+        bool external = false;  // a near-full insert on the component path
+        uint32_t op = 0;        // external: the op
+        fm::Shape shape = fm::SHAPE_GENERIC;
+        uint32_t ph0 = 0, nph = 0;  // persistent launch: its phases (and done counters)
+        uint64_t units = 0;
+        uint32_t ext = 0;       // external: index of its GroupOp descriptor
+    };
+    std::vector<QStep> qsteps;
+    std::vector<fm::QPhase> qphases;
+    std::vector<uint32_t> qext_ops;  // op index of each external descriptor
+    size_t q_ops_off = 0, q_ph_off = 0, q_ext_off = 0;  // in the descriptor buffer
+    uint32_t* d_done = nullptr;      // one counter per phase
+    fm::QState* d_qstate = nullptr;  // one per step
+    fm::QState* h_qstate = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     unsigned long long launches_per_run = 0;
@@ -1313,6 +1333,182 @@ int batch_fill(fm_batch* b) {
         }
     }
     return FM_OK;
+}
+
+// Queue mode: the op descriptors from the current table state (scratch sized
+// for each table's largest mutating op first: growing it reallocates).
+int queue_fill(fm_batch* b) {
+    for (size_t i = 0; i < b->tables.size(); i++) b->h_len()[i] = b->tables[i]->len.load();
+    std::vector<uint64_t> need(b->tables.size(), 0);
+    for (size_t i = 0; i < b->ops.size(); i++)
+        if (b->ops[i].kind != FM_OP_GET) need[b->table_of[i]] = std::max(need[b->table_of[i]], b->ops[i].n);
+    for (size_t i = 0; i < b->tables.size(); i++) {
+        if (!need[i]) continue;
+        int rc = ensure_scratch(b->tables[i], need[i]);
+        if (rc) return rc;
+    }
+    auto* q = reinterpret_cast<fm::QOp*>(b->h_desc + b->q_ops_off);
+    for (size_t i = 0; i < b->ops.size(); i++) {
+        const fm_op& o = b->ops[i];
+        fm_table* t = o.table;
+        fm::QOp& d = q[i];
+        d.t = t->view();
+        d.keys = (const uint8_t*)o.d_keys;
+        d.vals = (const uint8_t*)o.d_values;
+        d.out_vals = (uint8_t*)o.d_out_values;
+        d.out_found = o.d_out_found;
+        d.sc = t->sc;
+        d.ctl = t->d_ctl;
+        d.len = b->d_len + b->table_of[i];
+        d.result = b->d_res + i;
+        d.status = b->d_status + i;
+        d.n = (uint32_t)o.n;
+        d.kind = o.kind;
+        d.counted = 1;
+    }
+    auto* g = reinterpret_cast<fm::GroupOp*>(b->h_desc + b->q_ext_off);
+    for (size_t k = 0; k < b->qext_ops.size(); k++) {
+        const uint32_t i = b->qext_ops[k];
+        const fm::QOp& d = q[i];
+        g[k].t = d.t;
+        g[k].keys = d.keys;
+        g[k].vals = d.vals;
+        g[k].sc = d.sc;
+        g[k].ctl = d.ctl;
+        g[k].len = d.len;
+        g[k].result = d.result;
+        g[k].status = d.status;
+        g[k].n = d.n;
+        g[k].counted = 1;
+    }
+    memcpy(b->h_desc + b->q_ph_off, b->qphases.data(), b->qphases.size() * sizeof(fm::QPhase));
+    return FM_OK;
+}
+
+// Queue mode: uploads, the steps in order on stream s, downloads.
+int queue_enqueue(fm_batch* b, cudaStream_t s) {
+    cudaError_t e = cudaMemcpyAsync(b->d_desc, b->h_desc, b->desc_bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_len, b->h_len(), b->tables.size() * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_res, 0, b->ops.size() * 8, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_status, 0, b->ops.size() * 4, s);
+    if (e == cudaSuccess && !b->qphases.empty()) e = cudaMemsetAsync(b->d_done, 0, b->qphases.size() * 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_qstate, 0, b->qsteps.size() * sizeof(fm::QState), s);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "batch upload", e);
+    const auto* dq = reinterpret_cast<const fm::QOp*>(b->d_desc + b->q_ops_off);
+    const auto* dph = reinterpret_cast<const fm::QPhase*>(b->d_desc + b->q_ph_off);
+    const auto* dg = reinterpret_cast<const fm::GroupOp*>(b->d_desc + b->q_ext_off);
+    const auto* hg = reinterpret_cast<const fm::GroupOp*>(b->h_desc + b->q_ext_off);
+    for (size_t si = 0; si < b->qsteps.size(); si++) {
+        const fm_batch::QStep& st = b->qsteps[si];
+        if (!st.external) {
+            e = fm::launch_queue(st.shape, dph + st.ph0, st.nph, st.units, dq, b->d_done + st.ph0, b->d_qstate + si, s);
+        } else {
+            // precheck, the component path, then the write-back (its rounds
+            // see no op left)
+            const fm::GroupOp& h = hg[st.ext];
+            e = fm::launch_grp_ins(st.shape, dg + st.ext, 1, h.n, fm::GRP_BEGIN, 0, 0, s);
+            if (e == cudaSuccess)
+                e = fm::launch_ins_comp(h.t, st.shape, h.keys, h.vals, fm::CMP_N0_CTL, 0, h.n, h.sc, h.ctl, s);
+            if (e == cudaSuccess) e = cudaMemsetAsync(&h.ctl->n0, 0, sizeof(uint32_t), s);
+            if (e == cudaSuccess) e = fm::launch_grp_ins(st.shape, dg + st.ext, 1, h.n, fm::GRP_END, 0, 0, s);
+        }
+        if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch queue", e);
+    }
+    e = cudaMemcpyAsync(b->h_len(), b->d_len, b->tables.size() * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_res(), b->d_res, b->ops.size() * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_status(), b->d_status, b->ops.size() * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->h_qstate, b->d_qstate, b->qsteps.size() * sizeof(fm::QState), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "batch download", e);
+    return FM_OK;
+}
+
+// Queue mode plan: segments of ops closed by near-full inserts; per segment
+// and record shape, the phases of every table's chain of ops listed level by
+// level (the first phase of every chain, then the second, ...), each waiting
+// for the one before it in its chain.
+void queue_plan(fm_batch* b) {
+    const uint32_t nops = (uint32_t)b->ops.size();
+    std::vector<double> est(b->tables.size());
+    for (size_t i = 0; i < b->tables.size(); i++) est[i] = (double)b->tables[i]->len.load();
+    std::vector<uint32_t> seg;
+    auto flush = [&]() {
+        for (int shi = 0; shi < (int)fm::SHAPE_GENERIC; shi++) {
+            const fm::Shape sh = (fm::Shape)shi;
+            // per table, its chain of (op, phase kind, units)
+            std::vector<std::vector<fm::QPhase>> chain(b->tables.size());
+            bool any = false;
+            for (uint32_t i : seg) {
+                const fm_op& o = b->ops[i];
+                if (o.table->shape != sh) continue;
+                any = true;
+                auto& c = chain[b->table_of[i]];
+                const uint32_t n = (uint32_t)o.n;
+                auto add = [&](uint32_t kind) {
+                    fm::QPhase p{};
+                    p.op = i;
+                    p.kind = kind;
+                    p.units = fm::queue_units(kind, n);
+                    c.push_back(p);
+                };
+                if (o.kind == FM_OP_GET) {
+                    add(fm::QP_GET);
+                } else if (o.kind == FM_OP_INSERT) {
+                    for (uint32_t k : {fm::QP_BEGIN, fm::QP_IFIND, fm::QP_IFLOW, fm::QP_IEXEC, fm::QP_IWARP, fm::QP_END})
+                        add(k);
+                } else {
+                    for (uint32_t k : {fm::QP_BEGIN, fm::QP_RFIND, fm::QP_REXEC, fm::QP_END}) add(k);
+                }
+            }
+            if (!any) continue;
+            fm_batch::QStep st;
+            st.shape = sh;
+            st.ph0 = (uint32_t)b->qphases.size();
+            std::vector<int32_t> last(b->tables.size(), -1);  // index (within the step) of the chain's last phase
+            size_t maxlen = 0;
+            for (auto& c : chain) maxlen = std::max(maxlen, c.size());
+            uint64_t base = 0;
+            for (size_t lvl = 0; lvl < maxlen; lvl++) {
+                for (size_t ti = 0; ti < chain.size(); ti++) {
+                    if (lvl >= chain[ti].size()) continue;
+                    fm::QPhase p = chain[ti][lvl];
+                    p.dep = last[ti];
+                    p.base = base;
+                    base += p.units;
+                    last[ti] = (int32_t)(b->qphases.size() - st.ph0);
+                    b->qphases.push_back(p);
+                }
+            }
+            st.nph = (uint32_t)(b->qphases.size() - st.ph0);
+            st.units = base;
+            b->qsteps.push_back(st);
+        }
+        seg.clear();
+    };
+    for (uint32_t i = 0; i < nops; i++) {
+        const fm_op& o = b->ops[i];
+        if (o.n == 0) continue;  // nothing to run; result 0, status OK
+        const uint32_t ti = b->table_of[i];
+        if (o.kind == FM_OP_INSERT) {
+            const double cap = (double)b->tables[ti]->cap;
+            est[ti] += (double)o.n;
+            if (est[ti] >= FM_DIRECT_LOAD * cap) {
+                est[ti] = std::min(est[ti], cap);
+                flush();
+                fm_batch::QStep st;
+                st.external = true;
+                st.op = i;
+                st.shape = o.table->shape;
+                st.ext = (uint32_t)b->qext_ops.size();
+                b->qext_ops.push_back(i);
+                b->qsteps.push_back(st);
+                continue;
+            }
+        }
+        seg.push_back(i);
+    }
+    flush();
 }
 
 // Enqueues the batch on stream s: descriptor and count upload, the waves,
@@ -1478,6 +1674,54 @@ int fm_batch_create(const fm_op* ops, uint32_t nops, fm_batch** out) {
         if ((uint32_t)w + 1 > b->waves) b->waves = (uint32_t)w + 1;
         op_wave.push_back((uint32_t)w);
     }
+    // queue mode: every op with keys of a compile-time record shape, 16-byte
+    // aligned buffers and fewer than 2^31 keys
+    b->qmode = true;
+    for (uint32_t i = 0; i < nops && b->qmode; i++) {
+        const fm_op& o = ops[i];
+        if (o.n == 0) continue;
+        if (o.table->shape == fm::SHAPE_GENERIC || !batch_aligned(o) || o.n >= (1ull << 31)) b->qmode = false;
+    }
+    if (b->qmode) {
+        queue_plan(b);
+        size_t off = 0;
+        auto take = [&](size_t bytes) {
+            const size_t o = off;
+            off = (off + bytes + 255) & ~(size_t)255;
+            return o;
+        };
+        b->q_ops_off = take(nops * sizeof(fm::QOp));
+        b->q_ph_off = take(std::max<size_t>(1, b->qphases.size()) * sizeof(fm::QPhase));
+        b->q_ext_off = take(std::max<size_t>(1, b->qext_ops.size()) * sizeof(fm::GroupOp));
+        b->desc_bytes = off;
+        DeviceGuard dg(b->device);
+        auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+        const size_t nst = std::max<size_t>(1, b->qsteps.size());
+        const size_t o_len = al(b->desc_bytes), o_res = o_len + al(b->tables.size() * 8),
+                     o_st = o_res + al(nops * 8), o_done = o_st + al(nops * 4),
+                     o_qs = o_done + al(std::max<size_t>(1, b->qphases.size()) * 4),
+                     dneed = o_qs + al(nst * sizeof(fm::QState));
+        const size_t h_io = al(b->desc_bytes), h_qs = h_io + al(b->io_bytes()), hneed = h_qs + al(nst * sizeof(fm::QState));
+        cudaError_t e = cudaSuccess;
+        b->arena = arena_take(b->device, dneed, hneed, &e);
+        if (e != cudaSuccess) {
+            fm_batch_destroy(b);
+            return cuda_fail(FM_ERR_GPU_ALLOC, "batch buffers", e);
+        }
+        b->d_desc = b->arena.d;
+        b->d_len = reinterpret_cast<unsigned long long*>(b->arena.d + o_len);
+        b->d_res = reinterpret_cast<unsigned long long*>(b->arena.d + o_res);
+        b->d_status = reinterpret_cast<int*>(b->arena.d + o_st);
+        b->d_done = reinterpret_cast<uint32_t*>(b->arena.d + o_done);
+        b->d_qstate = reinterpret_cast<fm::QState*>(b->arena.d + o_qs);
+        b->h_desc = b->arena.h;
+        b->h_io = b->arena.h + h_io;
+        b->h_qstate = reinterpret_cast<fm::QState*>(b->arena.h + h_qs);
+        memset(b->h_desc, 0, b->desc_bytes);
+        memset(b->h_io, 0, b->io_bytes());
+        *out = b;
+        return FM_OK;
+    }
     // lanes: tables by decreasing work (sum of op sizes, mutations weighted
     // up), each to the lane with the least work so far
     const uint32_t ntab = (uint32_t)b->tables.size();
@@ -1578,14 +1822,14 @@ int fm_batch_capture(fm_batch* b, void* stream) {
     if (b->pending) return fail(FM_ERR_INVALID_ARG, "batch still running: call fm_batch_wait first");
     DeviceGuard dg(b->device);
     cudaStream_t s = (cudaStream_t)stream;
-    int rc = batch_fill(b);  // allocations (scratch growth) happen here, outside the capture
+    int rc = b->qmode ? queue_fill(b) : batch_fill(b);  // allocations (scratch growth) happen here, outside the capture
     if (rc) return rc;
     if (b->exec) cudaGraphExecDestroy(b->exec), b->exec = nullptr;
     if (b->graph) cudaGraphDestroy(b->graph), b->graph = nullptr;
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "begin capture", e);
     const unsigned long long l0 = fm::launch_count();
-    rc = batch_enqueue(b, s, false);
+    rc = b->qmode ? queue_enqueue(b, s) : batch_enqueue(b, s, false);
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(s, &g);
     if (rc) {
@@ -1609,15 +1853,20 @@ int fm_batch_run(fm_batch* b, void* stream) {
     for (fm_table* t : b->tables) cudaStreamSynchronize(t->stream);
     int rc;
     if (b->exec) {
-        rc = batch_fill(b);
+        rc = b->qmode ? queue_fill(b) : batch_fill(b);
         if (rc) return rc;
         cudaError_t e = cudaGraphLaunch(b->exec, s);
         if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "graph launch", e);
         fm::count_launches((unsigned)b->launches_per_run);
     } else {
         TimerScope ts(b->tables.size() == 1 ? b->tables[0] : nullptr);
-        rc = batch_fill(b);
-        if (!rc) rc = batch_enqueue(b, s, true);
+        if (b->qmode) {
+            rc = queue_fill(b);
+            if (!rc) rc = queue_enqueue(b, s);
+        } else {
+            rc = batch_fill(b);
+            if (!rc) rc = batch_enqueue(b, s, true);
+        }
         if (rc) return rc;
     }
     b->last_stream = s;
@@ -1634,6 +1883,9 @@ int fm_batch_wait(fm_batch* b, fm_op* ops) {
     if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch", e);
     int rc = FM_OK;
     for (size_t i = 0; i < b->tables.size(); i++) b->tables[i]->len.store(b->h_len()[i]);
+    if (b->qmode)
+        for (size_t si = 0; si < b->qsteps.size(); si++)
+            if (b->h_qstate[si].err) rc = fail(FM_ERR_DEVICE_TIMEOUT, "batch queue: a dependency wait ran out");
     for (size_t i = 0; i < b->ops.size(); i++) {
         const int st = b->h_status()[i];
         if (ops) {

@@ -13,6 +13,7 @@
 #include <atomic>
 
 #include "fm_internal.h"
+#include "fm_probe.cuh"
 
 namespace fm {
 
@@ -82,12 +83,6 @@ __device__ __forceinline__ void get_query_tile(const TableView& t, const uint8_t
     const uint64_t h = key.hash(ksz, t.hash_mode) & mask;
     uint64_t wbase = h & ~(uint64_t)(T - 1);  // sector-aligned window start
     uint64_t hit = NONE64;
-    // compile-time value sizes: the value of a step's first candidate is read
-    // by the tile while the keys are compared, so the usual hit (the first
-    // candidate) needs no round trip after the compare
-    constexpr int SPEC = (VB > 0 && VB % 16 == 0) ? (VB / 16 + T - 1) / T : 0;  // 16-byte chunks per lane
-    uint4 spec[SPEC > 0 ? SPEC : 1];
-    uint64_t spec_slot = NONE64;
     for (;;) {
         const uint64_t pos = wbase + lane;
         const bool before = pos < h;
@@ -102,16 +97,6 @@ __device__ __forceinline__ void get_query_tile(const TableView& t, const uint8_t
         const bool cand = !before && !past && s == ST_OCC && dist_matches(f, p);
         const uint32_t tm = (__ballot_sync(tmask, term) >> tbase) & TM;
         const uint32_t lim = tm ? (uint32_t)(__ffs(tm) - 1) : (uint32_t)T;
-        if constexpr (SPEC > 0) {
-            const uint32_t cm = (__ballot_sync(tmask, cand && lane < lim) >> tbase) & TM;
-            if (ov && cm) {
-                spec_slot = __shfl_sync(tmask, slot, tbase + __ffs(cm) - 1);
-                const uint4* src = reinterpret_cast<const uint4*>(t.vals + spec_slot * VB);
-#pragma unroll
-                for (int u = 0; u < SPEC; u++)
-                    if ((int)lane + u * T < VB / 16) spec[u] = __ldg(src + lane + u * T);
-            }
-        }
         const bool m = cand && lane < lim && key.eq(t.keys + slot * ksz, ksz);
         const uint32_t mm = (__ballot_sync(tmask, m) >> tbase) & TM;
         if (mm) {
@@ -122,15 +107,6 @@ __device__ __forceinline__ void get_query_tile(const TableView& t, const uint8_t
         wbase += T;
     }
     if (ov) {
-        if constexpr (SPEC > 0) {
-            if (hit != NONE64 && hit == spec_slot) {
-#pragma unroll
-                for (int u = 0; u < SPEC; u++)
-                    if ((int)lane + u * T < VB / 16) reinterpret_cast<uint4*>(ov)[lane + u * T] = spec[u];
-                if (of && lane == 0) *of = 1;
-                return;
-            }
-        }
         if (hit != NONE64) tile_copy<VB, T>(ov, t.vals + hit * vsz, vsz, lane);
         else tile_zero<VB, T>(ov, vsz, lane);
     }
@@ -162,62 +138,6 @@ __global__ void __launch_bounds__(BLOCK) k_count(const uint32_t* __restrict__ fl
         for (int w = 0; w < BLOCK / 32; w++) s += part[w];
         if (s) atomicAdd(&ctl->occupied, (unsigned long long)s);
     }
-}
-
-// bulk_get with one thread per query (compile-time shapes, capacity >= 8).
-// Each step reads the 8-slot metadata window that holds the probe position as
-// two 16-byte loads (one 32-byte sector, aligned), walks it in registers, and
-// compares keys only where the stored distance equals the probe depth.  With
-// one query per thread about eight times as many queries are in flight per SM
-// as with one query per 8-lane tile, which is what a chain of dependent
-// random reads (key -> metadata -> key -> value) needs.
-// The value of a candidate slot is loaded together with its key (when
-// values are wanted): a hit then costs no round trip after the key compare,
-// and a candidate whose key differs wastes one value read.
-template <int KB, int VB>
-__device__ __forceinline__ void get_query_thread(const TableView& t, const uint8_t* __restrict__ qk,
-                                                 uint8_t* __restrict__ ov, uint8_t* __restrict__ of) {
-    const uint64_t mask = t.mask;
-    RegKey<KB> key;
-    key.load(qk, KB);
-    const uint64_t h = key.hash(KB, t.hash_mode) & mask;
-    uint64_t wb = h & ~7ull;
-    bool hit = false;
-    bool done = false;
-    while (!done) {
-        const uint4* fp = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
-        const uint4 a = __ldg(fp), b = __ldg(fp + 1);
-        const uint32_t f8[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-#pragma unroll
-        for (int l = 0; l < 8; l++) {
-            const uint64_t pos = wb + l;
-            if (done || pos < h) continue;
-            const uint64_t p = pos - h;
-            const uint32_t f = f8[l];
-            const uint32_t s = st_of(f);
-            // Terminators: probe past the capacity, EMPTY, or OCCUPIED with
-            // p > dist (rayon_cpu.rs:91-111); tombstones are skipped.
-            if (p > mask || s == ST_EMPTY || (s == ST_OCC && p > dist_of(f))) {
-                done = true;
-            } else if (s == ST_OCC && dist_matches(f, p)) {
-                const uint64_t slot = pos & mask;
-                RegVal<VB> cv;
-                if (ov) cv.load_ro(t.vals + slot * VB);
-                if (key.eq(t.keys + slot * KB, KB)) {
-                    hit = true;
-                    done = true;
-                    if (ov) cv.store(ov, VB);
-                }
-            }
-        }
-        wb += 8;
-    }
-    if (ov && !hit) {
-        RegVal<VB> z;
-        z.zero();
-        z.store(ov, VB);
-    }
-    if (of) *of = hit ? 1 : 0;
 }
 
 template <int KB, int VB>

@@ -34,6 +34,7 @@
 #include <utility>
 
 #include "fm_rounds.cuh"
+#include "fm_probe.cuh"
 
 namespace fm {
 namespace {
@@ -1948,7 +1949,7 @@ constexpr uint32_t DX_ABS = 0x80000000u;   // seg_cnt: the free slot is in an ea
 constexpr uint32_t DX_CNT = 0x7FFFFFFFu;
 constexpr uint32_t DX_ROOT = 0x80000000u;  // warp-pass list entry: a component's leader
 constexpr int DX_LCH = 16;                 // evictions of a walk on the thread path
-constexpr int DX_LCMP = 2;                 // possible updates of a walk on the thread path
+constexpr int DX_LCMP = 6;                 // possible updates of a walk on the thread path
 constexpr int DX_LTRIPS = 4;               // 16-slot metadata reads of a walk on the thread path
 constexpr int DX_GATHER = 64;              // ops of a component the warp pass runs itself
 constexpr int DX_THREADS = 256;            // threads of an exec block
@@ -2054,6 +2055,16 @@ __global__ void __launch_bounds__(RBLOCK) k_dx_flow(TableView t, uint32_t n0, Op
     }
 }
 
+// The thread path's per-thread lists (shared memory, one column per thread):
+// eviction slots and depths, possible-update slots and the evictions before
+// each.
+struct DxLaneSmem {
+    uint32_t pos[DX_LCH][DX_THREADS];
+    uint32_t dep[DX_LCH][DX_THREADS];
+    uint32_t cpos[DX_LCMP][DX_THREADS];
+    uint32_t cst[DX_LCMP][DX_THREADS];
+};
+
 // A record (key and value) held in registers for a move.
 template <int KB, int VB>
 struct DxRec {
@@ -2079,20 +2090,21 @@ struct DxRec {
 // the carried entry (the op's home first), a resident whose home r exceeds H
 // is evicted (the carried entry takes its slot at depth position - H, and the
 // resident is carried on: H = r), one with r == H is a possible update, and F
-// takes the last carried entry.  The possible updates are compared in one
-// round trip (the first equal key in walk order ends the walk in place), then
-// the records move highest first, two per round trip: move m writes P_m (the
-// m-th eviction slot; the end slot for the last) from P_(m-1) (the new entry
-// for m = 0), and a pair loads both sources before storing either, which
-// keeps each slot's read before its write.  Returns 1 (claimed F), 0 (updated
-// in place) or -1 with nothing written when the walk needs more than
+// takes the last carried entry.  The possible updates are compared first on
+// the keys' first 8 bytes, all in one round trip, and in full only where
+// those agree (the first equal key in walk order ends the walk in place);
+// then the records move highest first, DX_MB per round trip: move m writes
+// P_m (the m-th eviction slot; the end slot for the last) from P_(m-1) (the
+// new entry for m = 0), and a batch loads all its sources before it stores,
+// which keeps each slot's read before its write.  Returns 1 (claimed F), 0
+// (updated in place) or -1 with nothing written when the walk needs more than
 // DX_LTRIPS metadata reads, DX_LCH evictions or DX_LCMP possible updates, or
 // when the metadata does not show F as the first free slot.  Needs capacity
 // >= 8 and below 2^28 slots.
 template <int KB, int VB>
 __device__ __noinline__ int dx_lane(const TableView& t, const RegKey<KB>& key, uint64_t F, const uint8_t* kin,
-                                    const uint8_t* vin, uint32_t (*s_pos)[DX_THREADS],
-                                    uint32_t (*s_dep)[DX_THREADS], ExecAcc& acc) {
+                                    const uint8_t* vin, DxLaneSmem& sl, ExecAcc& acc) {
+    constexpr int MB = (KB + VB) <= 16 ? 8 : ((KB + VB) <= 64 ? 4 : 2);  // moves per round trip
     const uint64_t mask = t.mask;
     const uint32_t me = threadIdx.x;
     const uint64_t h = key.hash(KB, t.hash_mode) & mask;
@@ -2100,8 +2112,6 @@ __device__ __noinline__ int dx_lane(const TableView& t, const RegKey<KB>& key, u
     const uint64_t wb = h & ~7ull;
     if (e - wb >= 16ull * DX_LTRIPS) return -1;
     uint32_t k = 0, nc = 0;
-    uint64_t cpos0 = 0, cpos1 = 0;
-    uint32_t cst0 = 0, cst1 = 0;
     long long H = (long long)h;
     bool end_tomb = false;
     for (uint64_t w = wb; w <= e; w += 16) {
@@ -2123,59 +2133,75 @@ __device__ __noinline__ int dx_lane(const TableView& t, const RegKey<KB>& key, u
             const long long r = (long long)pos - (long long)dist_of(f16[l]);
             if (r > H) {
                 if (k == (uint32_t)DX_LCH) return -1;
-                s_pos[k][me] = (uint32_t)(pos & mask);
-                s_dep[k][me] = (uint32_t)((long long)pos - H);
+                sl.pos[k][me] = (uint32_t)(pos & mask);
+                sl.dep[k][me] = (uint32_t)((long long)pos - H);
                 ++k;
                 H = r;
             } else if (r == H) {
                 if (nc == (uint32_t)DX_LCMP) return -1;
-                if (nc == 0) cpos0 = pos, cst0 = k;
-                else cpos1 = pos, cst1 = k;
+                sl.cpos[nc][me] = (uint32_t)(pos & mask);
+                sl.cst[nc][me] = k;
                 ++nc;
             }
         }
     }
-    // possible updates: the resident keys and the carried keys, one round trip
+    // possible updates: 8-byte prefixes of the resident and the carried keys
+    // in one round trip, full keys only where the prefixes agree
     int kind = 1;
     uint64_t end_slot = e & mask;
     uint32_t kk = k;
     if (nc) {
-        RegKey<KB> r0, r1, c0, c1;
-        r0.load_table(t.keys + (cpos0 & mask) * KB, KB);
-        if (cst0) c0.load_table(t.keys + (uint64_t)s_pos[cst0 - 1][me] * KB, KB);
-        else c0 = key;
-        if (nc > 1) {
-            r1.load_table(t.keys + (cpos1 & mask) * KB, KB);
-            if (cst1) c1.load_table(t.keys + (uint64_t)s_pos[cst1 - 1][me] * KB, KB);
-            else c1 = key;
+        uint2 rp[DX_LCMP], cp[DX_LCMP];
+        const uint2 kp = make_uint2(key.w[0], KB >= 8 ? key.w[1] : 0u);
+#pragma unroll
+        for (int c = 0; c < DX_LCMP; c++) {
+            if (c < (int)nc) {
+                rp[c] = *reinterpret_cast<const uint2*>(t.keys + (uint64_t)sl.cpos[c][me] * KB);
+                const uint32_t st = sl.cst[c][me];
+                cp[c] = st ? *reinterpret_cast<const uint2*>(t.keys + (uint64_t)sl.pos[st - 1][me] * KB) : kp;
+            }
         }
-        if (c0.same(r0)) {
-            kind = 2, end_slot = cpos0 & mask, kk = cst0;
-        } else if (nc > 1 && c1.same(r1)) {
-            kind = 2, end_slot = cpos1 & mask, kk = cst1;
+        for (int c = 0; c < (int)nc; c++) {
+            bool agree = false;
+#pragma unroll
+            for (int q = 0; q < DX_LCMP; q++)
+                if (q == c) agree = rp[q].x == cp[q].x && rp[q].y == cp[q].y;
+            if (!agree) continue;
+            const uint32_t st = sl.cst[c][me];
+            const uint64_t cs = sl.cpos[c][me];
+            RegKey<KB> ck;
+            if (st) ck.load_table(t.keys + (uint64_t)sl.pos[st - 1][me] * KB, KB);
+            else ck = key;
+            if (ck.eq(t.keys + cs * KB, KB)) {
+                kind = 2, end_slot = cs, kk = st;
+                break;
+            }
         }
     }
-    // moves, highest first, two per round trip
-    for (int m = (int)kk; m >= 0; m -= 2) {
-        DxRec<KB, VB> ra, rb;
-        const bool vo = kind == 2 && m == (int)kk;  // the update writes the value only
-        const uint64_t da = m < (int)kk ? (uint64_t)s_pos[m][me] : end_slot;
-        if (m == 0) ra.load_in(kin, vin);
-        else ra.load_slot(t, s_pos[m - 1][me], vo);
-        const bool two = m >= 1;
-        uint64_t db = 0;
-        if (two) {
-            db = s_pos[m - 1][me];
-            if (m == 1) rb.load_in(kin, vin);
-            else rb.load_slot(t, s_pos[m - 2][me], false);
+    // moves, highest first, MB per round trip
+    for (int top = (int)kk; top >= 0; top -= MB) {
+        DxRec<KB, VB> rec[MB];
+#pragma unroll
+        for (int b = 0; b < MB; b++) {
+            const int m = top - b;
+            if (m < 0) continue;
+            const bool vo = kind == 2 && m == (int)kk;  // the update writes the value only
+            if (m == 0) rec[b].load_in(kin, vin);
+            else rec[b].load_slot(t, sl.pos[m - 1][me], vo);
         }
-        ra.store_slot(t, da, vo);
-        if (two) rb.store_slot(t, db, false);
+#pragma unroll
+        for (int b = 0; b < MB; b++) {
+            const int m = top - b;
+            if (m < 0) continue;
+            const bool vo = kind == 2 && m == (int)kk;
+            const uint64_t d = m < (int)kk ? (uint64_t)sl.pos[m][me] : end_slot;
+            rec[b].store_slot(t, d, vo);
+        }
     }
     uint32_t md = 0;
     for (uint32_t i = 0; i < kk; i++) {
-        const uint32_t d = s_dep[i][me];
-        t.flags[s_pos[i][me]] = mk_flag(ST_OCC, d);
+        const uint32_t d = sl.dep[i][me];
+        t.flags[sl.pos[i][me]] = mk_flag(ST_OCC, d);
         md = max(md, d);
     }
     if (kind == 1) {
@@ -2194,8 +2220,7 @@ template <int KB, int VB>
 __global__ void __launch_bounds__(DX_THREADS, 2) k_dx_exec(TableView t, const uint8_t* __restrict__ keys,
                                                            const uint8_t* __restrict__ vals, uint32_t n0,
                                                            OpScratch sc, Ctl* ctl) {
-    __shared__ uint32_t s_pos[DX_LCH][DX_THREADS];
-    __shared__ uint32_t s_dep[DX_LCH][DX_THREADS];
+    __shared__ DxLaneSmem s_lane;
     __shared__ uint32_t s_tmp[DX_THREADS / 32];
     dx_wait_prev();
     dx_let_next();
@@ -2221,8 +2246,7 @@ __global__ void __launch_bounds__(DX_THREADS, 2) k_dx_exec(TableView t, const ui
                     key.load(keys + (uint64_t)j * KB, KB);
                     int c = -1;
                     if (lanes_ok)
-                        c = dx_lane<KB, VB>(t, key, F, keys + (uint64_t)j * KB, vals + (uint64_t)j * VB, s_pos,
-                                            s_dep, a);
+                        c = dx_lane<KB, VB>(t, key, F, keys + (uint64_t)j * KB, vals + (uint64_t)j * VB, s_lane, a);
                     if (c < 0) defer = true, item = j;
                     else a.claimed += (uint32_t)c;
                     t.seg_min[F] = IDLE;
@@ -2345,6 +2369,422 @@ __global__ void __launch_bounds__(RBLOCK, FM_P4_MIN_BLOCKS) k_dx_warp(TableView 
     }
     block_add_count(ctl, a.claimed, s_tmp);
     publish_rare(ctl, a.maxd, a.tomb, a.limit);
+}
+
+// ---- persistent batch: one launch drains a queue of bulk ops ---------------
+//
+// The host plans every op of a batch into a chain of phases (QPhase, in
+// fm_internal.h), each of some number of work units, and lists the phases of
+// all ops in an order where every phase follows the phase it waits for: the
+// previous phase of its op, or the last phase of the previous op on its
+// table.  k_queue's blocks take units from one counter in that order; a block
+// that takes a unit waits (bounded) until the phase it depends on has
+// finished all its units, runs the unit and counts it finished.  A unit is
+// taken only by a running block and waits only for units handed out before
+// it, so the waits end whether or not all blocks are resident at once.
+//
+// Units (all block-wide, QTHREADS threads):
+//   QP_GET    QG_UNIT queries, one thread per query (the thread probe);
+//   QP_BEGIN  the op's control block reset and, for a counted insert, the
+//             TableFull precheck against the table's count at this point;
+//   QP_IFIND / QP_IFLOW / QP_IEXEC  QI_UNIT ops of the direct insert's find,
+//             flow and exec passes;
+//   QP_IWARP  8 warps over the exec pass's list, strided over the phase's
+//             units (lone long walks and components as tile walks);
+//   QP_RFIND / QP_REXEC  QI_UNIT ops of the direct remove;
+//   QP_END    what the direct passes left (every op when some op found no
+//             free slot / EMPTY slot, or the ops of oversized groups) in index
+//             order on this block, then the op's result, status and the
+//             table's count.
+constexpr int QTHREADS = 256;
+constexpr uint32_t QG_UNIT = 1024;  // queries per lookup unit
+constexpr uint32_t QI_UNIT = 512;   // ops per find / flow / exec unit
+constexpr uint64_t QWAIT_NS = 2000000000ull;  // bound of one dependency wait
+
+__device__ __forceinline__ uint64_t q_now() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+struct QSmem {
+    union {
+        DxLaneSmem exec;
+        struct {
+            P4Chain<32> chain[QTHREADS / 32];
+            uint32_t ops[QTHREADS / 32][DX_GATHER];
+        } warp;
+        struct {
+            uint32_t buf[QTHREADS];
+            uint32_t woff[33];
+            TileChain chain;
+        } serial;
+    };
+    uint32_t tmp[QTHREADS / 32];
+};
+static_assert(DX_THREADS == QTHREADS, "exec pass buffers");
+
+// A lookup on a table of fewer than 8 slots, slot by slot.
+template <int KB, int VB>
+__device__ __noinline__ void q_get_small(const TableView& t, const uint8_t* qk, uint8_t* ov, uint8_t* of) {
+    RegKey<KB> key;
+    key.load(qk, KB);
+    const uint64_t h = key.hash(KB, t.hash_mode) & t.mask;
+    uint64_t hit = NONE64;
+    for (uint64_t p = 0; p <= t.mask; ++p) {
+        const uint64_t s = (h + p) & t.mask;
+        const uint32_t f = t.flags[s];
+        if (st_of(f) == ST_EMPTY || (st_of(f) == ST_OCC && p > dist_of(f))) break;
+        if (st_of(f) == ST_OCC && dist_matches(f, p) && key.eq(t.keys + s * KB, KB)) {
+            hit = s;
+            break;
+        }
+    }
+    if (ov) {
+        RegVal<VB> v;
+        if (hit != NONE64) v.load(t.vals + hit * VB, VB);
+        else v.zero();
+        v.store(ov, VB);
+    }
+    if (of) *of = hit != NONE64 ? 1 : 0;
+}
+
+template <int KB, int VB>
+__device__ __noinline__ void q_get(const QOp& o, uint32_t c) {
+    const TableView& t = o.t;
+    const uint64_t q0 = (uint64_t)c * QG_UNIT;
+    const uint64_t q1 = min((uint64_t)o.n, q0 + QG_UNIT);
+#pragma unroll 1
+    for (uint64_t q = q0 + threadIdx.x; q < q1; q += QTHREADS) {
+        uint8_t* ov = o.out_vals ? o.out_vals + q * VB : nullptr;
+        uint8_t* of = o.out_found ? o.out_found + q : nullptr;
+        if (t.mask >= 7) get_query_thread<KB, VB>(t, o.keys + q * KB, ov, of);
+        else q_get_small<KB, VB>(t, o.keys + q * KB, ov, of);
+    }
+}
+
+__device__ __noinline__ void q_begin(const QOp& o) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(o.ctl);
+    for (uint32_t i = threadIdx.x; i < CTL_CALL_BYTES / 4; i += blockDim.x) w[i] = 0u;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t n0 = o.n;
+        int st = STATUS_OK;
+        if (o.kind == 1 && o.counted && *o.len + o.n > o.t.mask + 1) {  // gpu.rs:198-206
+            n0 = 0;
+            st = STATUS_TABLE_FULL;
+        }
+        o.ctl->n0 = n0;
+        *o.status = st;
+        *o.result = 0;
+    }
+}
+
+__device__ __forceinline__ uint32_t q_n0(const QOp& o) { return *(volatile const uint32_t*)&o.ctl->n0; }
+
+template <int KB>
+__device__ __noinline__ void q_ifind(const QOp& o, uint32_t c) {
+    const uint32_t n0 = q_n0(o);
+    const uint32_t j = c * QI_UNIT + threadIdx.x;
+    bool no_free = false;
+    for (uint32_t k = 0; k < QI_UNIT / QTHREADS; k++) {
+        const uint32_t jj = j + k * QTHREADS;
+        if (jj >= n0) break;
+        const uint64_t F = find_free<KB>(o.t, o.keys, jj);
+        o.sc.op_slot[jj] = F;
+        uint8_t lead = 0;
+        uint32_t next = IDLE;
+        if (F == NONE64) {
+            no_free = true;
+        } else {
+            lead = atomicAdd(&o.t.seg_cnt[F], 1u) == 0u ? 1 : 0;
+            next = atomicExch(&o.t.seg_min[F], jj);
+        }
+        o.sc.op_word[jj] = next;
+        o.sc.op_flag[jj] = lead;
+    }
+    if (no_free) o.ctl->serial[0] = 1u;
+}
+
+__device__ __noinline__ void q_iflow(const QOp& o, uint32_t c) {
+    const uint32_t n0 = q_n0(o);
+    if (*(volatile uint32_t*)&o.ctl->serial[0]) return;
+    const TableView& t = o.t;
+    for (uint32_t k = 0; k < QI_UNIT / QTHREADS; k++) {
+        const uint32_t j = c * QI_UNIT + threadIdx.x + k * QTHREADS;
+        if (j >= n0) break;
+        if (!o.sc.op_flag[j]) continue;
+        const uint64_t F = o.sc.op_slot[j];
+        const uint32_t cnt = t.seg_cnt[F] & DX_CNT;
+        if (cnt < 2) continue;
+        uint64_t flow = cnt - 1, a = F + 1, budget = t.mask;
+        for (;;) {
+            const uint64_t at = dx_next_free(t, a, budget);
+            if (at == NONE64) {
+                o.ctl->serial[0] = 1u;
+                break;
+            }
+            const uint64_t F2 = at & t.mask;
+            const uint32_t w2 = t.seg_cnt[F2];
+            const uint32_t c2 = w2 & DX_CNT;
+            if (c2) {
+                if (t.seg_min[F2] >= n0) {
+                    atomicOr(&o.ctl->err, ERR_SCRATCH);
+                    break;
+                }
+                if (!(w2 & DX_ABS)) atomicOr(&t.seg_cnt[F2], DX_ABS);
+            }
+            flow = flow + c2 - 1;
+            if (flow == 0) break;
+            a = at + 1;
+        }
+    }
+}
+
+template <int KB, int VB>
+__device__ __noinline__ void q_iexec(const QOp& o, uint32_t c, QSmem& sm) {
+    const uint32_t n0 = q_n0(o);
+    const TableView& t = o.t;
+    const bool serial = *(volatile uint32_t*)&o.ctl->serial[0] != 0;
+    const bool lanes_ok = t.mask >= 7 && t.mask < (uint64_t)DIST_MASK;
+    ExecAcc a;
+    for (uint32_t k = 0; k < QI_UNIT / QTHREADS; k++) {  // block-uniform trip count
+        const uint32_t j = c * QI_UNIT + threadIdx.x + k * QTHREADS;
+        uint32_t item = 0;
+        bool defer = false;
+        if (j < n0) {
+            const uint64_t F = o.sc.op_slot[j];
+            if (F != NONE64) {
+                const uint32_t w = t.seg_cnt[F];
+                if (serial) {
+                    t.seg_min[F] = IDLE;
+                    t.seg_cnt[F] = 0;
+                    o.sc.op_word[j] = IDLE;
+                } else if (w == 1u) {
+                    RegKey<KB> key;
+                    key.load(o.keys + (uint64_t)j * KB, KB);
+                    int r = -1;
+                    if (lanes_ok)
+                        r = dx_lane<KB, VB>(t, key, F, o.keys + (uint64_t)j * KB, o.vals + (uint64_t)j * VB,
+                                            sm.exec, a);
+                    if (r < 0) defer = true, item = j;
+                    else a.claimed += (uint32_t)r;
+                    t.seg_min[F] = IDLE;
+                    t.seg_cnt[F] = 0;
+                    o.sc.op_word[j] = IDLE;
+                } else if (o.sc.op_flag[j] && !(w & DX_ABS)) {
+                    defer = true, item = j | DX_ROOT;
+                }
+            }
+        }
+        append(o.sc.long_list, &o.ctl->nlong[0], item, defer);
+    }
+    block_add_count(o.ctl, a.claimed, sm.tmp);
+    publish_rare(o.ctl, a.maxd, a.tomb, a.limit);
+}
+
+template <int KB, int VB>
+__device__ __noinline__ void q_iwarp(const QOp& o, uint32_t c, uint32_t units, QSmem& sm) {
+    const uint32_t n = *(volatile const uint32_t*)&o.ctl->nlong[0];
+    const uint32_t n0 = q_n0(o);
+    const Tile<32> tl;
+    const uint32_t wi = threadIdx.x >> 5;
+    ExecAcc a;
+    for (uint32_t i = c * (QTHREADS / 32) + wi; i < n; i += units * (QTHREADS / 32)) {
+        const uint32_t item = o.sc.long_list[i];
+        uint32_t g = 1;
+        if (item & DX_ROOT) {
+            g = dx_gather(o.t, item & ~DX_ROOT, n0, o.sc, o.ctl, sm.warp.ops[wi], tl);
+        } else {
+            if (tl.lane == 0) sm.warp.ops[wi][0] = item;
+            tl.sync();
+        }
+        for (uint32_t q = 0; q < g; q++)
+            dx_run_tile<KB, VB>(o.t, o.keys, o.vals, sm.warp.ops[wi][q], tl, sm.warp.chain[wi], a);
+    }
+    block_add_count(o.ctl, a.claimed, sm.tmp);
+    publish_rare(o.ctl, a.maxd, a.tomb, a.limit);
+}
+
+template <int KB>
+__device__ __noinline__ void q_rfind(const QOp& o, uint32_t c) {
+    const uint32_t n0 = q_n0(o);
+    bool no_empty = false;
+    for (uint32_t k = 0; k < QI_UNIT / QTHREADS; k++) {
+        const uint32_t j = c * QI_UNIT + threadIdx.x + k * QTHREADS;
+        if (j >= n0) break;
+        RegKey<KB> key;
+        const uint64_t E = rx_first_empty(o.t, home_of<KB>(o.t, o.keys, j, key));
+        o.sc.op_slot[j] = E;
+        uint8_t lead = 0;
+        uint32_t next = IDLE;
+        if (E == NONE64) {
+            no_empty = true;
+        } else {
+            lead = atomicAdd(&o.t.seg_cnt[E], 1u) == 0u ? 1 : 0;
+            next = atomicExch(&o.t.seg_min[E], j);
+        }
+        o.sc.op_word[j] = next;
+        o.sc.op_flag[j] = lead;
+    }
+    if (no_empty) o.ctl->serial[0] = 1u;
+}
+
+template <int KB>
+__device__ __noinline__ void q_rexec(const QOp& o, uint32_t c, QSmem& sm) {
+    const uint32_t n0 = q_n0(o);
+    const TableView& t = o.t;
+    const bool serial = *(volatile uint32_t*)&o.ctl->serial[0] != 0;
+    uint32_t removed = 0;
+    for (uint32_t k = 0; k < QI_UNIT / QTHREADS; k++) {
+        const uint32_t j = c * QI_UNIT + threadIdx.x + k * QTHREADS;
+        if (j >= n0) break;
+        const uint64_t E = o.sc.op_slot[j];
+        if (E == NONE64) continue;
+        if (serial) {
+            t.seg_min[E] = IDLE;
+            t.seg_cnt[E] = 0;
+            o.sc.op_word[j] = IDLE;
+            continue;
+        }
+        if (!o.sc.op_flag[j]) continue;
+        const uint32_t cnt = t.seg_cnt[E];
+        uint32_t ids[RX_GATHER];
+        uint32_t x = t.seg_min[E];
+        uint32_t g = 0;
+        for (uint32_t q = 0; q < cnt && x != IDLE; q++) {
+            if (x >= n0) {
+                atomicOr(&o.ctl->err, ERR_SCRATCH);
+                break;
+            }
+            const uint32_t nx = o.sc.op_word[x];
+            o.sc.op_word[x] = IDLE;
+            if (cnt <= RX_GATHER) ids[g++] = x;
+            else o.sc.pend[1][atomicAdd(&o.ctl->npend[1], 1u)] = x;
+            x = nx;
+        }
+        t.seg_min[E] = IDLE;
+        t.seg_cnt[E] = 0;
+        for (uint32_t p = 1; p < g; p++) {
+            const uint32_t v = ids[p];
+            uint32_t b = p;
+            for (; b > 0 && ids[b - 1] > v; --b) ids[b] = ids[b - 1];
+            ids[b] = v;
+        }
+        for (uint32_t q = 0; q < g; q++) {
+            RegKey<KB> key;
+            const uint64_t h = home_of<KB>(t, o.keys, ids[q], key);
+            removed += rx_probe<KB>(t, key, h);
+        }
+    }
+    block_add_count(o.ctl, removed, sm.tmp);
+}
+
+// The leftovers in index order on this block, then the result write-back.
+template <int KB, int VB>
+__device__ __noinline__ void q_end(const QOp& o, QSmem& sm) {
+    const uint32_t n0 = q_n0(o);
+    const bool serial = *(volatile uint32_t*)&o.ctl->serial[0] != 0;
+    const uint32_t left = serial ? n0 : *(volatile uint32_t*)&o.ctl->npend[1];
+    const uint32_t* list = serial ? nullptr : o.sc.pend[1];
+    if (left) {
+        if (o.kind == 1) {
+            ExecAcc a;
+            serial_process<KB, VB>(o.t, o.keys, o.vals, list, left, n0, o.sc, a, sm.serial.buf, sm.serial.woff,
+                                   &sm.serial.chain);
+            __syncthreads();
+            if (a.claimed) atomicAdd(&o.ctl->count, (unsigned long long)a.claimed);
+            if (a.maxd > *(volatile uint32_t*)&o.ctl->dmax) atomicMax(&o.ctl->dmax, a.maxd);
+            if (a.tomb) o.ctl->tomb_claimed = 1u;
+            if (a.limit) atomicOr(&o.ctl->err, ERR_WALK_LIMIT);
+        } else {
+            // removes: mark, list in index order, probe one after another
+            for (uint32_t i = threadIdx.x; i < left; i += blockDim.x) o.sc.op_flag[list ? list[i] : i] = 3;
+            __syncthreads();
+            uint32_t removed = 0;
+            for (uint32_t base = 0; base < n0; base += blockDim.x) {
+                const uint32_t j = base + threadIdx.x;
+                const bool take = j < n0 && o.sc.op_flag[j] == 3;
+                const uint32_t cnt = block_compact(j, take, sm.serial.buf, sm.serial.woff);
+                if (threadIdx.x == 0) {
+                    for (uint32_t q = 0; q < cnt; q++) {
+                        const uint32_t jj = sm.serial.buf[q];
+                        o.sc.op_flag[jj] = 0;
+                        RegKey<KB> key;
+                        removed += rx_probe<KB>(o.t, key, home_of<KB>(o.t, o.keys, jj, key));
+                    }
+                }
+                __syncthreads();
+            }
+            if (threadIdx.x == 0 && removed) atomicAdd(&o.ctl->count, (unsigned long long)removed);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (*o.status == STATUS_OK) {
+            const unsigned long long cnt = o.ctl->total_count();
+            *o.result = cnt;
+            if (o.kind == 1) *o.len += o.counted ? cnt : (unsigned long long)o.n;
+            else *o.len -= cnt;
+            const uint32_t err = o.ctl->err;
+            if (err & (ERR_SCRATCH | ERR_NO_PROGRESS)) *o.status = STATUS_KERNEL;
+            else if (err & ERR_WALK_LIMIT) *o.status = STATUS_PROBE_LIMIT;
+        }
+        o.ctl->npend[0] = o.ctl->npend[1] = 0;
+    }
+}
+
+template <int KB, int VB>
+__global__ void __launch_bounds__(QTHREADS, 2) k_queue(const QPhase* __restrict__ ph, uint64_t total,
+                                                       const QOp* __restrict__ ops, uint32_t* done, QState* st) {
+    __shared__ QSmem sm;
+    __shared__ unsigned long long s_u;
+    __shared__ uint32_t s_pe;
+    uint32_t cursor = 0;  // the phase of the last unit taken: units come in increasing order
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const unsigned long long u = atomicAdd(&st->next, 1ull);
+            s_u = u;
+            if (u < total) {
+                while (ph[cursor].base + ph[cursor].units <= u) ++cursor;
+                s_pe = cursor;
+                const int32_t d = ph[cursor].dep;
+                if (d >= 0) {
+                    const uint32_t need = ph[d].units;
+                    const uint64_t t0 = q_now();
+                    while (*(volatile uint32_t*)&done[d] < need) {
+                        __nanosleep(200);
+                        if (q_now() - t0 > QWAIT_NS) {  // reported to the host; the unit still runs
+                            atomicOr(&st->err, 1u);
+                            break;
+                        }
+                    }
+                    __threadfence();
+                }
+            }
+        }
+        __syncthreads();
+        const unsigned long long u = s_u;
+        if (u >= total) break;
+        const QPhase p = ph[s_pe];
+        const QOp& o = ops[p.op];
+        const uint32_t c = (uint32_t)(u - p.base);
+        switch (p.kind) {
+            case QP_GET: q_get<KB, VB>(o, c); break;
+            case QP_BEGIN: q_begin(o); break;
+            case QP_IFIND: q_ifind<KB>(o, c); break;
+            case QP_IFLOW: q_iflow(o, c); break;
+            case QP_IEXEC: q_iexec<KB, VB>(o, c, sm); break;
+            case QP_IWARP: q_iwarp<KB, VB>(o, c, p.units, sm); break;
+            case QP_RFIND: q_rfind<KB>(o, c); break;
+            case QP_REXEC: q_rexec<KB>(o, c, sm); break;
+            default: q_end<KB, VB>(o, sm); break;
+        }
+        __threadfence();  // this unit's writes before its count
+        __syncthreads();
+        if (threadIdx.x == 0) atomicAdd(&done[s_pe], 1u);
+    }
 }
 
 constexpr int INS_T = 32;  // lanes per insert in the single-block tail
@@ -2729,6 +3169,43 @@ cudaError_t launch_ins_direct(const TableView& t, Shape sh, const uint8_t* keys,
 #define FM_CALL(K, V) direct_shape<K, V>(t, keys, vals, n0, sc, ctl, s)
     FM_SHAPE_SWITCH(sh, FM_CALL)
 #undef FM_CALL
+    return cudaGetLastError();
+}
+
+uint32_t queue_units(uint32_t kind, uint32_t n) {
+    switch (kind) {
+        case QP_GET: return (n + QG_UNIT - 1) / QG_UNIT;
+        case QP_BEGIN:
+        case QP_END: return 1;
+        case QP_IWARP: return (n + 63) / 64;  // 8 warps per unit: a warp per 8 ops the exec pass may list
+        default: return (n + QI_UNIT - 1) / QI_UNIT;
+    }
+}
+
+cudaError_t launch_queue(Shape sh, const QPhase* ph, uint32_t nph, uint64_t total_units, const QOp* ops,
+                         uint32_t* done, QState* st, cudaStream_t s) {
+    if (nph == 0 || total_units == 0) return cudaSuccess;
+    (void)nph;
+    auto go = [&](auto kernel) {
+        static int per_sm = 0;  // resident blocks per SM of this instantiation
+        if (per_sm == 0) {
+            int b = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, QTHREADS, 0) != cudaSuccess || b < 1) b = 1;
+            per_sm = b;
+        }
+        const uint64_t want = (uint64_t)num_sms() * per_sm;
+        const unsigned grid = (unsigned)(total_units < want ? total_units : want);
+        kernel<<<grid, QTHREADS, 0, s>>>(ph, total_units, ops, done, st);
+    };
+    switch (sh) {
+        case SHAPE_8_8: go(k_queue<8, 8>); break;
+        case SHAPE_32_128: go(k_queue<32, 128>); break;
+        case SHAPE_32_64: go(k_queue<32, 64>); break;
+        case SHAPE_32_32: go(k_queue<32, 32>); break;
+        case SHAPE_8_32: go(k_queue<8, 32>); break;
+        default: return cudaErrorInvalidValue;
+    }
+    count_launches(1);
     return cudaGetLastError();
 }
 

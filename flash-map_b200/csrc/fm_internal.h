@@ -207,6 +207,60 @@ cudaError_t launch_grp_get(Shape sh, const GroupGet* ops, const uint64_t* prefix
 // GRP_SERIAL (inserts): every op's ops pending at round r0 one at a time in
 // index order, one block per op (for rounds that stopped making progress).
 enum { GRP_BEGIN = 0, GRP_ROUNDS = 1, GRP_END = 2, GRP_SERIAL = 3 };
+// ---- persistent batch (one launch per record shape drains a queue) --------
+//
+// Every op of a batch is a chain of phases; each phase has `units` work units
+// (one block each); the phases of all ops are listed in an order where every
+// phase follows the one it waits for (`dep`: the previous phase of its op, or
+// the last phase of the previous op on its table; -1: none).  `base` is the
+// first global unit of the phase (the prefix of the units before it).
+enum QPhaseKind : uint32_t {
+    QP_GET = 0,  // lookups
+    QP_BEGIN,    // control block reset; inserts: the TableFull precheck
+    QP_IFIND,    // direct insert: find, flow, exec, warp passes
+    QP_IFLOW,
+    QP_IEXEC,
+    QP_IWARP,
+    QP_RFIND,    // direct remove: find, exec
+    QP_REXEC,
+    QP_END,      // leftovers in index order, result write-back
+};
+struct QPhase {
+    uint64_t base;
+    uint32_t units;
+    uint32_t op;
+    uint32_t kind;
+    int32_t dep;
+};
+// One op of the queue (device descriptor).
+struct QOp {
+    TableView t;
+    const uint8_t* keys;
+    const uint8_t* vals;         // inserts
+    uint8_t* out_vals;           // gets (may be null)
+    uint8_t* out_found;          // gets (may be null)
+    OpScratch sc;
+    Ctl* ctl;
+    unsigned long long* len;     // the table's count within the batch
+    unsigned long long* result;  // new / removed keys
+    int* status;
+    uint32_t n;
+    uint32_t kind;               // 0 get, 1 insert, 2 remove
+    uint32_t counted;
+    uint32_t pad_;
+};
+struct QState {
+    unsigned long long next;  // the next unit to hand out
+    uint32_t err;             // 1: a dependency wait ran out
+    uint32_t pad_;
+};
+// Units of each phase kind for an op of n keys.
+uint32_t queue_units(uint32_t kind, uint32_t n);
+// One persistent launch over phases [0, nph) of ops of one record shape;
+// `done` holds nph zeroed counters and `st` a zeroed QState.
+cudaError_t launch_queue(Shape sh, const QPhase* ph, uint32_t nph, uint64_t total_units, const QOp* ops,
+                         uint32_t* done, QState* st, cudaStream_t s);
+
 cudaError_t launch_grp_ins(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, int phase, uint32_t r0,
                            uint32_t nrounds, cudaStream_t s);
 cudaError_t launch_grp_rem(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, int phase, uint32_t r0,

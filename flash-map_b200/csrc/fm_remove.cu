@@ -17,16 +17,10 @@
 //
 // Control: as fm_insert.cu (two grid rounds, then a single-block tail).
 #include "fm_rounds.cuh"
+#include "fm_probe.cuh"
 
 namespace fm {
 namespace {
-
-template <int KB>
-__device__ __forceinline__ uint64_t home_of(const TableView& t, const uint8_t* keys, uint32_t j, RegKey<KB>& key) {
-    const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
-    key.load(keys + (uint64_t)j * ksz, ksz);
-    return key.hash(ksz, t.hash_mode) & t.mask;
-}
 
 // The call's chunk summaries, or null when the call did not build them.
 __device__ __forceinline__ uint32_t* rsum_of(const OpScratch& sc, const Ctl* ctl) {
@@ -534,83 +528,6 @@ void rounds_shape(const TableView& t, const uint8_t* keys, uint32_t n0, uint32_t
 // table) leaves every op to the rounds (Ctl::serial[0]); a group of more than
 // RX_GATHER ops leaves its ops to them (pend[1], Ctl::npend[1]).  Every
 // registration and list word is idle again when the two kernels end.
-constexpr uint32_t RX_GATHER = 32;
-
-// First EMPTY slot at or after home h, NONE64 when the table has none (two
-// aligned 8-slot windows per round trip with capacity >= 8).
-__device__ __forceinline__ uint64_t rx_first_empty(const TableView& t, uint64_t h) {
-    const uint64_t mask = t.mask;
-    if (mask >= 7) {
-        uint64_t wb = h & ~7ull;
-        for (uint64_t w = 0; w <= (mask >> 4) + 1; ++w, wb += 16) {
-            const uint4* p0 = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
-            const uint4* p1 = reinterpret_cast<const uint4*>(t.flags + ((wb + 8) & mask));
-            const uint4 a = p0[0], b = p0[1], c = p1[0], d = p1[1];
-            const uint32_t f16[16] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w};
-#pragma unroll
-            for (int l = 0; l < 16; l++) {
-                const uint64_t pos = wb + l;
-                if (pos < h) continue;
-                if (pos - h > mask) return NONE64;
-                if (st_of(f16[l]) == ST_EMPTY) return pos & mask;
-            }
-        }
-        return NONE64;
-    }
-    for (uint64_t p = 0; p <= mask; ++p)
-        if (st_of(t.flags[(h + p) & mask]) == ST_EMPTY) return (h + p) & mask;
-    return NONE64;
-}
-
-// The sequential remove of one key (rayon_cpu.rs:273-328): skip TOMBSTONEs,
-// stop at EMPTY or at the Robin Hood exit (OCCUPIED with depth > stored
-// distance), and turn the first OCCUPIED slot holding the key (its stored
-// distance equal to the depth) into the whole word TOMBSTONE.  Returns 1 when
-// it did.
-template <int KB>
-__device__ __forceinline__ uint32_t rx_probe(const TableView& t, const RegKey<KB>& key, uint64_t h) {
-    const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
-    const uint64_t mask = t.mask;
-    if (mask >= 7) {
-        for (uint64_t wb = h & ~7ull;; wb += 8) {
-            const uint4* fp = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
-            const uint4 a = fp[0], b = fp[1];
-            const uint32_t f8[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-#pragma unroll
-            for (int l = 0; l < 8; l++) {
-                const uint64_t pos = wb + l;
-                if (pos < h) continue;
-                const uint64_t p = pos - h;
-                if (p > mask) return 0;
-                const uint32_t f = f8[l];
-                const uint32_t st = st_of(f);
-                if (st == ST_EMPTY) return 0;
-                if (st == ST_OCC) {
-                    if (p > dist_of(f)) return 0;
-                    const uint64_t slot = pos & mask;
-                    if (dist_matches(f, p) && key.eq(t.keys + slot * ksz, ksz)) {
-                        t.flags[slot] = ST_TOMB;
-                        return 1;
-                    }
-                }
-            }
-        }
-    }
-    for (uint64_t p = 0; p <= mask; ++p) {
-        const uint64_t slot = (h + p) & mask;
-        const uint32_t f = t.flags[slot];
-        const uint32_t st = st_of(f);
-        if (st == ST_EMPTY) return 0;
-        if (st == ST_OCC) {
-            if (p > dist_of(f)) return 0;
-            if (dist_matches(f, p) && key.eq(t.keys + slot * ksz, ksz)) {
-                t.flags[slot] = ST_TOMB;
-                return 1;
-            }
-        }
-    }
-    return 0;
-}
 
 template <int KB>
 __global__ void __launch_bounds__(RBLOCK) k_rx_find(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,

@@ -237,3 +237,65 @@ def test_batch_run_time_record_sizes():
         gf, gk, gv = t["g"].snapshot()
         of_, ok, ov = t["o"].snapshot()
         assert np.array_equal(gf, of_) and np.array_equal(gk, ok) and np.array_equal(gv, ov)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batch_sixteen_tables_up_to_2_20_slots(graph):
+    """16 tables of 2^12..2^20 slots, 150 ops of up to 50,000 keys: the
+    persistent queue kernel (every shape here is a compile-time one) against
+    the oracle replaying the queue in order."""
+    import flash_map as F
+
+    tables, queue = make_queue(21, ntables=16, nops=150, cap_bits=(12, 20), sizes=(16, 50_000))
+    g_res, g_out = run_batch(tables, queue, graph)
+    o_res, o_out = oracle_replay(tables, queue)
+    for i, ((ti, kind, k, v), gr, orr) in enumerate(zip(queue, g_res, o_res)):
+        assert gr == orr, f"op {i} kind {kind} n {len(k)}: gpu {gr} oracle {orr}"
+        if kind == F.batch.GET and len(k):
+            ov, of = g_out[i]
+            ev, ef = o_out[i]
+            assert np.array_equal(of.astype(bool), ef) and np.array_equal(ov, ev), f"op {i}"
+    for t in tables:
+        assert t["g"].len() == t["o"].len()
+        for x, y in zip(t["g"].snapshot(), t["o"].snapshot()):
+            assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batch_near_full_inserts_between_queue_launches(graph):
+    """Inserts that take their tables to load 0.97 and beyond run on the
+    component path between persistent launches; gets and removes on the same
+    and other tables before and after them keep queue order."""
+    import flash_map as F
+
+    rng = np.random.default_rng(33)
+    tables = []
+    for i, (ks, vs) in enumerate([(8, 8), (32, 128), (8, 8)]):
+        cap = 1 << 13
+        g, o = gpu_map(cap, ks, vs), OracleAdapter(cap, ks, vs)
+        k, v = _keys(rng, int(cap * 0.85), ks), _keys(rng, int(cap * 0.85), vs)
+        assert g.bulk_insert(k, v) == o.bulk_insert(k, v)
+        tables.append({"g": g, "o": o, "ks": ks, "vs": vs, "known": [k]})
+    queue = []
+    for rep in range(3):
+        for ti, t in enumerate(tables):
+            cap = t["g"].capacity()
+            n = int(cap * (0.05 if rep < 2 else 0.2))  # the last round is oversized for some
+            k, v = _keys(rng, n, t["ks"]), _keys(rng, n, t["vs"])
+            queue.append((ti, F.batch.INSERT, k, v))
+            t["known"].append(k)
+            known = np.concatenate(t["known"])
+            queue.append((ti, F.batch.GET, known[rng.integers(0, len(known), 3000)], None))
+            queue.append((ti, F.batch.REMOVE, known[rng.integers(0, len(known), 300)], None))
+    g_res, g_out = run_batch(tables, queue, graph)
+    o_res, o_out = oracle_replay(tables, queue)
+    for i, ((ti, kind, k, v), gr, orr) in enumerate(zip(queue, g_res, o_res)):
+        assert gr == orr, f"op {i} kind {kind} n {len(k)}: gpu {gr} oracle {orr}"
+        if kind == F.batch.GET:
+            ov, of = g_out[i]
+            ev, ef = o_out[i]
+            assert np.array_equal(of.astype(bool), ef) and np.array_equal(ov, ev), f"op {i}"
+    for t in tables:
+        assert t["g"].len() == t["o"].len()
+        for x, y in zip(t["g"].snapshot(), t["o"].snapshot()):
+            assert np.array_equal(x, y)
