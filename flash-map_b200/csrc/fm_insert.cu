@@ -2750,7 +2750,9 @@ __global__ void __launch_bounds__(QTHREADS, 2) k_queue(const QPhase* __restrict_
                 while (ph[cursor].base + ph[cursor].units <= u) ++cursor;
                 s_pe = cursor;
                 const int32_t d = ph[cursor].dep;
-                if (d >= 0) {
+                // after one wait has run out the rest skip theirs, so a broken
+                // plan ends at once (reported to the host)
+                if (d >= 0 && !*(volatile uint32_t*)&st->err) {
                     const uint32_t need = ph[d].units;
                     const uint64_t t0 = q_now();
                     while (*(volatile uint32_t*)&done[d] < need) {
