@@ -2419,6 +2419,7 @@ struct QSmem {
             uint32_t woff[33];
             TileChain chain;
         } serial;
+        uint32_t rgrp[QTHREADS / 32][RX_GMAX];
     };
     uint32_t tmp[QTHREADS / 32];
 };
@@ -2636,45 +2637,38 @@ __device__ __noinline__ void q_rexec(const QOp& o, uint32_t c, QSmem& sm) {
     const TableView& t = o.t;
     const bool serial = *(volatile uint32_t*)&o.ctl->serial[0] != 0;
     uint32_t removed = 0;
-    for (uint32_t k = 0; k < QI_UNIT / QTHREADS; k++) {
+    for (uint32_t k = 0; k < QI_UNIT / QTHREADS; k++) {  // block-uniform trip count
         const uint32_t j = c * QI_UNIT + threadIdx.x + k * QTHREADS;
-        if (j >= n0) break;
-        const uint64_t E = o.sc.op_slot[j];
-        if (E == NONE64) continue;
-        if (serial) {
-            t.seg_min[E] = IDLE;
-            t.seg_cnt[E] = 0;
-            o.sc.op_word[j] = IDLE;
-            continue;
-        }
-        if (!o.sc.op_flag[j]) continue;
-        const uint32_t cnt = t.seg_cnt[E];
-        uint32_t ids[RX_GATHER];
-        uint32_t x = t.seg_min[E];
-        uint32_t g = 0;
-        for (uint32_t q = 0; q < cnt && x != IDLE; q++) {
-            if (x >= n0) {
-                atomicOr(&o.ctl->err, ERR_SCRATCH);
-                break;
+        uint64_t E = NONE64;
+        uint32_t cnt = 0;
+        bool lead = false;
+        if (j < n0) {
+            E = o.sc.op_slot[j];
+            if (E != NONE64) {
+                if (serial) {
+                    t.seg_min[E] = IDLE;
+                    t.seg_cnt[E] = 0;
+                    o.sc.op_word[j] = IDLE;
+                } else if (o.sc.op_flag[j]) {
+                    cnt = t.seg_cnt[E];
+                    if (cnt == 1) {
+                        RegKey<KB> key;
+                        removed += rx_probe<KB>(t, key, home_of<KB>(t, o.keys, j, key));
+                        t.seg_min[E] = IDLE;
+                        t.seg_cnt[E] = 0;
+                        o.sc.op_word[j] = IDLE;
+                    } else {
+                        lead = true;
+                    }
+                }
             }
-            const uint32_t nx = o.sc.op_word[x];
-            o.sc.op_word[x] = IDLE;
-            if (cnt <= RX_GATHER) ids[g++] = x;
-            else o.sc.pend[1][atomicAdd(&o.ctl->npend[1], 1u)] = x;
-            x = nx;
         }
-        t.seg_min[E] = IDLE;
-        t.seg_cnt[E] = 0;
-        for (uint32_t p = 1; p < g; p++) {
-            const uint32_t v = ids[p];
-            uint32_t b = p;
-            for (; b > 0 && ids[b - 1] > v; --b) ids[b] = ids[b - 1];
-            ids[b] = v;
-        }
-        for (uint32_t q = 0; q < g; q++) {
-            RegKey<KB> key;
-            const uint64_t h = home_of<KB>(t, o.keys, ids[q], key);
-            removed += rx_probe<KB>(t, key, h);
+        for (uint32_t lm = __ballot_sync(0xFFFFFFFFu, lead); lm; lm &= lm - 1) {
+            const int L = __ffs(lm) - 1;
+            const uint64_t EL = __shfl_sync(0xFFFFFFFFu, E, L);
+            const uint32_t cL = __shfl_sync(0xFFFFFFFFu, cnt, L);
+            const uint32_t r = rx_group<KB>(t, o.keys, n0, o.sc, o.ctl, EL, cL, sm.rgrp[threadIdx.x >> 5]);
+            if ((threadIdx.x & 31u) == 0) removed += r;
         }
     }
     block_add_count(o.ctl, removed, sm.tmp);

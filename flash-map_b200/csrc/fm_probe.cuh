@@ -102,13 +102,15 @@ __device__ __forceinline__ uint64_t rx_first_empty(const TableView& t, uint64_t 
     return NONE64;
 }
 
-// The sequential remove of one key (rayon_cpu.rs:273-328): skip TOMBSTONEs,
-// stop at EMPTY or at the Robin Hood exit (OCCUPIED with depth > stored
-// distance), and turn the first OCCUPIED slot holding the key (its stored
-// distance equal to the depth) into the whole word TOMBSTONE.  Returns 1 when
-// it did.
+// The probe of one remove (rayon_cpu.rs:273-328): skip TOMBSTONEs, stop at
+// EMPTY or at the Robin Hood exit (OCCUPIED with depth > stored distance) or
+// at the first OCCUPIED slot holding the key (its stored distance equal to the
+// depth).  Returns that slot (NONE64: a miss) and, in *stop, the slot where
+// the probe stopped (the match, the terminator, or NONE64 when it went round
+// the whole table).  With `commit` the match becomes the whole word TOMBSTONE.
 template <int KB>
-__device__ __forceinline__ uint32_t rx_probe(const TableView& t, const RegKey<KB>& key, uint64_t h) {
+__device__ __forceinline__ uint64_t rx_look(const TableView& t, const RegKey<KB>& key, uint64_t h, bool commit,
+                                            uint64_t* stop) {
     const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
     const uint64_t mask = t.mask;
     if (mask >= 7) {
@@ -121,17 +123,21 @@ __device__ __forceinline__ uint32_t rx_probe(const TableView& t, const RegKey<KB
                 const uint64_t pos = wb + l;
                 if (pos < h) continue;
                 const uint64_t p = pos - h;
-                if (p > mask) return 0;
+                if (p > mask) {
+                    *stop = NONE64;
+                    return NONE64;
+                }
                 const uint32_t f = f8[l];
                 const uint32_t st = st_of(f);
-                if (st == ST_EMPTY) return 0;
-                if (st == ST_OCC) {
-                    if (p > dist_of(f)) return 0;
-                    const uint64_t slot = pos & mask;
-                    if (dist_matches(f, p) && key.eq(t.keys + slot * ksz, ksz)) {
-                        t.flags[slot] = ST_TOMB;
-                        return 1;
-                    }
+                const uint64_t slot = pos & mask;
+                if (st == ST_EMPTY || (st == ST_OCC && p > dist_of(f))) {
+                    *stop = slot;
+                    return NONE64;
+                }
+                if (st == ST_OCC && dist_matches(f, p) && key.eq(t.keys + slot * ksz, ksz)) {
+                    if (commit) t.flags[slot] = ST_TOMB;
+                    *stop = slot;
+                    return slot;
                 }
             }
         }
@@ -140,16 +146,120 @@ __device__ __forceinline__ uint32_t rx_probe(const TableView& t, const RegKey<KB
         const uint64_t slot = (h + p) & mask;
         const uint32_t f = t.flags[slot];
         const uint32_t st = st_of(f);
-        if (st == ST_EMPTY) return 0;
-        if (st == ST_OCC) {
-            if (p > dist_of(f)) return 0;
-            if (dist_matches(f, p) && key.eq(t.keys + slot * ksz, ksz)) {
-                t.flags[slot] = ST_TOMB;
-                return 1;
-            }
+        if (st == ST_EMPTY || (st == ST_OCC && p > dist_of(f))) {
+            *stop = slot;
+            return NONE64;
+        }
+        if (st == ST_OCC && dist_matches(f, p) && key.eq(t.keys + slot * ksz, ksz)) {
+            if (commit) t.flags[slot] = ST_TOMB;
+            *stop = slot;
+            return slot;
         }
     }
-    return 0;
+    *stop = NONE64;
+    return NONE64;
+}
+
+// The sequential remove of one key: 1 when it tombstoned a slot.
+template <int KB>
+__device__ __forceinline__ uint32_t rx_probe(const TableView& t, const RegKey<KB>& key, uint64_t h) {
+    uint64_t stop;
+    return rx_look<KB>(t, key, h, true, &stop) != NONE64 ? 1u : 0u;
+}
+
+// Ops of a group of removes (equal first EMPTY slot) a warp runs itself.
+constexpr uint32_t RX_GMAX = 256;
+
+// The removes of the group at EMPTY slot E (c ops listed from seg_min[E]
+// through the per-op words) on one warp: lane 0 gathers the list into
+// s_grp (registrations set idle), the warp sorts it by index, then, 32 at a
+// time, every lane probes its op on the table as it is (no writes) and the
+// warp commits the ops in index order: an op whose probe range [home, stop]
+// holds a slot that an earlier op of its chunk tombstoned probes again on the
+// current table; any other op's probe is unchanged by them (removes change
+// nothing but those slots), so its result stands.  Returns the ops removed;
+// a group of more than RX_GMAX ops goes to pend[1] instead (0 returned).
+// Warp-uniform call.
+template <int KB>
+__device__ __noinline__ uint32_t rx_group(const TableView& t, const uint8_t* keys, uint32_t n0, const OpScratch& sc,
+                                          Ctl* ctl, uint64_t E, uint32_t c, uint32_t* s_grp) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t mask = t.mask;
+    uint32_t g = 0;
+    if (lane == 0) {
+        uint32_t x = t.seg_min[E];
+        for (uint32_t q = 0; q < c && x != IDLE; q++) {
+            if (x >= n0) {
+                atomicOr(&ctl->err, ERR_SCRATCH);
+                break;
+            }
+            const uint32_t nx = sc.op_word[x];
+            sc.op_word[x] = IDLE;
+            if (c <= RX_GMAX) s_grp[g++] = x;
+            else sc.pend[1][atomicAdd(&ctl->npend[1], 1u)] = x;
+            x = nx;
+        }
+        t.seg_min[E] = IDLE;
+        t.seg_cnt[E] = 0;
+    }
+    g = __shfl_sync(0xFFFFFFFFu, g, 0);
+    __syncwarp();
+    if (g == 0) return 0;
+    // index order: the rank of each entry among the group
+    uint32_t v[RX_GMAX / 32], r[RX_GMAX / 32];
+#pragma unroll
+    for (int u = 0; u < (int)(RX_GMAX / 32); u++) {
+        const uint32_t q = lane + 32 * u;
+        v[u] = q < g ? s_grp[q] : 0u;
+        r[u] = 0;
+    }
+    for (uint32_t q = 0; q < g; q++) {
+        const uint32_t y = s_grp[q];
+#pragma unroll
+        for (int u = 0; u < (int)(RX_GMAX / 32); u++) r[u] += y < v[u] ? 1u : 0u;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < (int)(RX_GMAX / 32); u++)
+        if (lane + 32 * u < g) s_grp[r[u]] = v[u];
+    __syncwarp();
+    uint32_t removed = 0;
+    for (uint32_t c0 = 0; c0 < g; c0 += 32) {
+        const uint32_t cnt = min(32u, g - c0);
+        const bool mine = lane < cnt;
+        RegKey<KB> key;
+        uint64_t h = 0, stop = 0, tgt = NONE64;
+        if (mine) {
+            h = home_of<KB>(t, keys, s_grp[c0 + lane], key);
+            tgt = rx_look<KB>(t, key, h, false, &stop);
+        }
+        // distances before E: a slot s lies in [h, stop] when d(h) >= d(s) >= d(stop)
+        const uint64_t dh = (E - h) & mask;
+        const uint64_t ds = stop == NONE64 ? 0 : ((E - stop) & mask);
+        uint64_t dt = tgt == NONE64 ? NONE64 : ((E - tgt) & mask);
+        bool done_t = false;  // this lane's op has tombstoned its target (in this chunk)
+        for (uint32_t i = 0; i < cnt; i++) {
+            const uint64_t hi = __shfl_sync(0xFFFFFFFFu, dh, i);
+            const uint64_t si = __shfl_sync(0xFFFFFFFFu, ds, i);
+            const bool hit_range = done_t && dt != NONE64 && dt <= hi && dt >= si;
+            const bool conflict = __ballot_sync(0xFFFFFFFFu, (int)lane < (int)i && hit_range) != 0;
+            if (lane == i) {
+                if (conflict) {  // an earlier op changed a slot of this probe: probe again
+                    uint64_t st2;
+                    tgt = rx_look<KB>(t, key, h, true, &st2);
+                    dt = tgt == NONE64 ? NONE64 : ((E - tgt) & mask);
+                } else if (tgt != NONE64) {
+                    t.flags[tgt] = ST_TOMB;
+                }
+                if (tgt != NONE64) {
+                    done_t = true;
+                    ++removed;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    return removed;
 }
 
 }  // namespace fm

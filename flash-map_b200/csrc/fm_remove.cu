@@ -555,50 +555,44 @@ template <int KB>
 __global__ void __launch_bounds__(RBLOCK) k_rx_exec(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
                                                     OpScratch sc, Ctl* ctl) {
     __shared__ uint32_t s_tmp[RBLOCK / 32];
+    __shared__ uint32_t s_grp[RBLOCK / 32][RX_GMAX];
     const bool serial = *(volatile uint32_t*)&ctl->serial[0] != 0;
     uint32_t removed = 0;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t iters = (n0 + stride - 1) / stride;
-    for (uint32_t it = 0; it < iters; it++) {
+    for (uint32_t it = 0; it < iters; it++) {  // warp-uniform trip count
         const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x + it * stride;
-        if (j >= n0) continue;
-        const uint64_t E = sc.op_slot[j];
-        if (E == NONE64) continue;
-        if (serial) {  // registrations back to idle; the rounds run every op
-            t.seg_min[E] = IDLE;
-            t.seg_cnt[E] = 0;
-            sc.op_word[j] = IDLE;
-            continue;
-        }
-        if (!sc.op_flag[j]) continue;  // the leader of E runs this op
-        const uint32_t c = t.seg_cnt[E];
-        uint32_t ops[RX_GATHER];
-        uint32_t x = t.seg_min[E];
-        uint32_t g = 0;
-        for (uint32_t q = 0; q < c && x != IDLE; q++) {
-            if (x >= n0) {  // registrations come only from this call's ops
-                atomicOr(&ctl->err, ERR_SCRATCH);
-                break;
+        uint64_t E = NONE64;
+        uint32_t c = 0;
+        bool lead = false;
+        if (j < n0) {
+            E = sc.op_slot[j];
+            if (E != NONE64) {
+                if (serial) {  // registrations back to idle; the rounds run every op
+                    t.seg_min[E] = IDLE;
+                    t.seg_cnt[E] = 0;
+                    sc.op_word[j] = IDLE;
+                } else if (sc.op_flag[j]) {  // the leader of E runs its group
+                    c = t.seg_cnt[E];
+                    if (c == 1) {
+                        RegKey<KB> key;
+                        removed += rx_probe<KB>(t, key, home_of<KB>(t, keys, j, key));
+                        t.seg_min[E] = IDLE;
+                        t.seg_cnt[E] = 0;
+                        sc.op_word[j] = IDLE;
+                    } else {
+                        lead = true;
+                    }
+                }
             }
-            const uint32_t nx = sc.op_word[x];
-            sc.op_word[x] = IDLE;
-            if (c <= RX_GATHER) ops[g++] = x;
-            else sc.pend[1][atomicAdd(&ctl->npend[1], 1u)] = x;
-            x = nx;
         }
-        t.seg_min[E] = IDLE;
-        t.seg_cnt[E] = 0;
-        // index order (insertion sort of at most RX_GATHER ops), then the probes
-        for (uint32_t a = 1; a < g; a++) {
-            const uint32_t v = ops[a];
-            uint32_t b = a;
-            for (; b > 0 && ops[b - 1] > v; --b) ops[b] = ops[b - 1];
-            ops[b] = v;
-        }
-        for (uint32_t q = 0; q < g; q++) {
-            RegKey<KB> key;
-            const uint64_t h = home_of<KB>(t, keys, ops[q], key);
-            removed += rx_probe<KB>(t, key, h);
+        // groups of two or more: one at a time on the whole warp
+        for (uint32_t lm = __ballot_sync(0xFFFFFFFFu, lead); lm; lm &= lm - 1) {
+            const int L = __ffs(lm) - 1;
+            const uint64_t EL = __shfl_sync(0xFFFFFFFFu, E, L);
+            const uint32_t cL = __shfl_sync(0xFFFFFFFFu, c, L);
+            const uint32_t r = rx_group<KB>(t, keys, n0, sc, ctl, EL, cL, s_grp[threadIdx.x >> 5]);
+            if ((threadIdx.x & 31u) == 0) removed += r;
         }
     }
     block_add_count(ctl, removed, s_tmp);

@@ -69,3 +69,73 @@ def test_remove_groups_round_the_end_of_the_table():
     assert whole == parts
     for x, y in zip(a.snapshot(), b.snapshot()):
         assert np.array_equal(x, y)
+
+
+def _look(flags, keys, cap, key, h):
+    """The probe of one remove (rayon_cpu.rs:273-328) on raw arrays: (target
+    slot or None, stop slot)."""
+    mask = cap - 1
+    for p in range(cap):
+        s = (h + p) & mask
+        f = int(flags[s])
+        st, d = f & 0xF, f >> 4
+        if st == 0 or (st == 1 and p > d):
+            return None, s
+        if st == 1 and d == p and bytes(keys[s]) == key:
+            return s, s
+    return None, None
+
+
+def group_commit(flags, keys, cap, ops, E, chunk=32):
+    """rx_group of flash-map_b200/csrc/fm_probe.cuh restated: the group's ops
+    (key, home) in index order, chunk by chunk: probe all on the table as it
+    is, then commit in order; an op whose [home, stop] holds a slot an earlier
+    op of its chunk tombstoned probes again.  Returns the count removed."""
+    mask = cap - 1
+    removed = 0
+    for c0 in range(0, len(ops), chunk):
+        part = ops[c0:c0 + chunk]
+        pre = [_look(flags, keys, cap, k, h) for k, h in part]
+        done = []  # distances before E of this chunk's tombstones
+        for (k, h), (tgt, stop) in zip(part, pre):
+            dh, ds = (E - h) & mask, ((E - stop) & mask) if stop is not None else 0
+            if any(ds <= dt <= dh for dt in done):
+                tgt, _ = _look(flags, keys, cap, k, h)
+            if tgt is not None:
+                flags[tgt] = 2
+                done.append((E - tgt) & mask)
+                removed += 1
+    return removed
+
+
+@pytest.mark.parametrize("load", [0.7, 0.85, 0.95])
+@pytest.mark.parametrize("chunk", [4, 32])
+def test_group_commit_equals_sequential(load, chunk):
+    """Duplicates, absent keys and removes of one another's exits inside
+    groups: the commit rule gives the sequential result slot for slot."""
+    cap = 1 << 10
+    rng = np.random.default_rng(int(load * 100) + chunk)
+    a, b = OracleAdapter(cap, 8, 8), OracleAdapter(cap, 8, 8)
+    pk = rng.integers(0, 256, (int(cap * load), 8), dtype=np.uint8)
+    for m in (a, b):
+        m.bulk_insert(pk, pk)
+        m.bulk_remove(pk[::9])
+    n = cap // 3
+    k = np.concatenate([pk[rng.integers(0, len(pk), n - n // 5)], rng.integers(0, 256, (n // 5, 8), dtype=np.uint8)])
+    k[rng.choice(n, n // 8)] = k[rng.integers(0, n, n // 8)]
+    homes = (k.view("<u8").reshape(-1) & np.uint64(cap - 1)).astype(np.int64)
+    flags = b.m.flags()  # the oracle's own arrays, written in place
+    keys = b.m.keys()
+    st = flags & 0xF
+    eidx = np.nonzero(st == 0)[0]
+    pos = np.searchsorted(eidx, homes)
+    E = eidx[np.where(pos < len(eidx), pos, 0)]
+    whole = a.bulk_remove(k)
+    parts = 0
+    for e in np.unique(E):
+        idx = np.nonzero(E == e)[0]  # index order
+        parts += group_commit(flags, keys, cap, [(bytes(k[j]), int(homes[j])) for j in idx], int(e), chunk)
+    b.m.set_len(len(b.m) - parts)
+    assert whole == parts
+    for x, y in zip(a.snapshot(), b.snapshot()):
+        assert np.array_equal(x, y)
