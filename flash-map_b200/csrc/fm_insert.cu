@@ -73,6 +73,33 @@ __device__ __forceinline__ uint64_t find_free(const TableView& t, const uint8_t*
     return NONE64;
 }
 
+// The same from a known home h (with capacity >= 8, two aligned windows per
+// round trip).
+__device__ __forceinline__ uint64_t find_free_from(const TableView& t, uint64_t h) {
+    if (t.mask >= 7) {
+        uint64_t wb = h & ~7ull;
+        for (uint64_t w = 0; w <= (t.mask >> 4) + 1; ++w, wb += 16) {
+            const uint4* p0 = reinterpret_cast<const uint4*>(t.flags + (wb & t.mask));
+            const uint4* p1 = reinterpret_cast<const uint4*>(t.flags + ((wb + 8) & t.mask));
+            const uint4 a = p0[0], b = p0[1], c = p1[0], d = p1[1];
+            const uint32_t f16[16] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w};
+#pragma unroll
+            for (int l = 0; l < 16; l++) {
+                const uint64_t pos = wb + l;
+                if (pos < h) continue;
+                if (pos - h > t.mask) return NONE64;
+                if (is_free(f16[l])) return pos & t.mask;
+            }
+        }
+        return NONE64;
+    }
+    for (uint64_t p = 0; p <= t.mask; ++p) {
+        const uint64_t s = (h + p) & t.mask;
+        if (is_free(t.flags[s])) return s;
+    }
+    return NONE64;
+}
+
 __device__ __forceinline__ void register_op(const TableView& t, uint32_t j, uint64_t F, uint64_t* op_slot) {
     op_slot[j] = F;
     if (F != NONE64) {
@@ -2006,8 +2033,12 @@ __global__ void __launch_bounds__(RBLOCK) k_dx_find(TableView t, const uint8_t* 
     dx_let_next();
     bool no_free = false;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n0; j += gridDim.x * blockDim.x) {
-        const uint64_t F = find_free<KB>(t, keys, j);
+        RegKey<KB> key;
+        key.load(keys + (uint64_t)j * KB, KB);
+        const uint64_t h = key.hash(KB, t.hash_mode) & t.mask;
+        const uint64_t F = find_free_from(t, h);
         sc.op_slot[j] = F;
+        sc.op_pt[(uint64_t)j * PT_MAX] = (uint32_t)h;  // the exec pass starts from it
         uint8_t lead = 0;
         uint32_t next = IDLE;
         if (F == NONE64) {
@@ -2101,13 +2132,24 @@ struct DxRec {
 // DX_LTRIPS metadata reads, DX_LCH evictions or DX_LCMP possible updates, or
 // when the metadata does not show F as the first free slot.  Needs capacity
 // >= 8 and below 2^28 slots.
+// The first metadata window of a walk from home h (two aligned 8-slot
+// windows), loaded while the caller's other loads are in flight.
+struct DxWin {
+    uint4 a, b, c, d;
+    __device__ __forceinline__ void load(const TableView& t, uint64_t w) {
+        const uint4* p0 = reinterpret_cast<const uint4*>(t.flags + (w & t.mask));
+        const uint4* p1 = reinterpret_cast<const uint4*>(t.flags + ((w + 8) & t.mask));
+        a = p0[0], b = p0[1], c = p1[0], d = p1[1];
+    }
+};
+
 template <int KB, int VB>
-__device__ __noinline__ int dx_lane(const TableView& t, const RegKey<KB>& key, uint64_t F, const uint8_t* kin,
-                                    const uint8_t* vin, DxLaneSmem& sl, ExecAcc& acc) {
+__device__ __noinline__ int dx_lane(const TableView& t, const RegKey<KB>& key, uint64_t h, uint64_t F,
+                                    const DxWin& w0, const uint8_t* kin, const uint8_t* vin, DxLaneSmem& sl,
+                                    ExecAcc& acc) {
     constexpr int MB = (KB + VB) <= 16 ? 8 : ((KB + VB) <= 64 ? 4 : 2);  // moves per round trip
     const uint64_t mask = t.mask;
     const uint32_t me = threadIdx.x;
-    const uint64_t h = key.hash(KB, t.hash_mode) & mask;
     const uint64_t e = h + ((F - h) & mask);  // F, unwrapped
     const uint64_t wb = h & ~7ull;
     if (e - wb >= 16ull * DX_LTRIPS) return -1;
@@ -2115,9 +2157,9 @@ __device__ __noinline__ int dx_lane(const TableView& t, const RegKey<KB>& key, u
     long long H = (long long)h;
     bool end_tomb = false;
     for (uint64_t w = wb; w <= e; w += 16) {
-        const uint4* p0 = reinterpret_cast<const uint4*>(t.flags + (w & mask));
-        const uint4* p1 = reinterpret_cast<const uint4*>(t.flags + ((w + 8) & mask));
-        const uint4 fa = p0[0], fb = p0[1], fc = p1[0], fd = p1[1];
+        DxWin win = w0;
+        if (w != wb) win.load(t, w);
+        const uint4 fa = win.a, fb = win.b, fc = win.c, fd = win.d;
         const uint32_t f16[16] = {fa.x, fa.y, fa.z, fa.w, fb.x, fb.y, fb.z, fb.w,
                                   fc.x, fc.y, fc.z, fc.w, fd.x, fd.y, fd.z, fd.w};
 #pragma unroll
@@ -2234,19 +2276,25 @@ __global__ void __launch_bounds__(DX_THREADS, 2) k_dx_exec(TableView t, const ui
         uint32_t item = 0;
         bool defer = false;
         if (j < n0) {
+            // independent loads together: free slot, home, key; then the
+            // registration count with the first metadata window
             const uint64_t F = sc.op_slot[j];
+            const uint64_t h = sc.op_pt[(uint64_t)j * PT_MAX];
+            RegKey<KB> key;
+            key.load(keys + (uint64_t)j * KB, KB);
             if (F != NONE64) {
+                DxWin w0;
+                if (lanes_ok && !serial) w0.load(t, h & ~7ull);
                 const uint32_t w = t.seg_cnt[F];
                 if (serial) {  // registrations back to idle; the component path runs every op
                     t.seg_min[F] = IDLE;
                     t.seg_cnt[F] = 0;
                     sc.op_word[j] = IDLE;
                 } else if (w == 1u) {  // alone at F, and F in no other op's component
-                    RegKey<KB> key;
-                    key.load(keys + (uint64_t)j * KB, KB);
                     int c = -1;
                     if (lanes_ok)
-                        c = dx_lane<KB, VB>(t, key, F, keys + (uint64_t)j * KB, vals + (uint64_t)j * VB, s_lane, a);
+                        c = dx_lane<KB, VB>(t, key, h, F, w0, keys + (uint64_t)j * KB, vals + (uint64_t)j * VB,
+                                            s_lane, a);
                     if (c < 0) defer = true, item = j;
                     else a.claimed += (uint32_t)c;
                     t.seg_min[F] = IDLE;
@@ -2491,8 +2539,12 @@ __device__ __noinline__ void q_ifind(const QOp& o, uint32_t c) {
     for (uint32_t k = 0; k < QI_UNIT / QTHREADS; k++) {
         const uint32_t jj = j + k * QTHREADS;
         if (jj >= n0) break;
-        const uint64_t F = find_free<KB>(o.t, o.keys, jj);
+        RegKey<KB> key;
+        key.load(o.keys + (uint64_t)jj * KB, KB);
+        const uint64_t h = key.hash(KB, o.t.hash_mode) & o.t.mask;
+        const uint64_t F = find_free_from(o.t, h);
         o.sc.op_slot[jj] = F;
+        o.sc.op_pt[(uint64_t)jj * PT_MAX] = (uint32_t)h;
         uint8_t lead = 0;
         uint32_t next = IDLE;
         if (F == NONE64) {
@@ -2555,18 +2607,21 @@ __device__ __noinline__ void q_iexec(const QOp& o, uint32_t c, QSmem& sm) {
         bool defer = false;
         if (j < n0) {
             const uint64_t F = o.sc.op_slot[j];
+            const uint64_t h = o.sc.op_pt[(uint64_t)j * PT_MAX];
+            RegKey<KB> key;
+            key.load(o.keys + (uint64_t)j * KB, KB);
             if (F != NONE64) {
+                DxWin w0;
+                if (lanes_ok && !serial) w0.load(t, h & ~7ull);
                 const uint32_t w = t.seg_cnt[F];
                 if (serial) {
                     t.seg_min[F] = IDLE;
                     t.seg_cnt[F] = 0;
                     o.sc.op_word[j] = IDLE;
                 } else if (w == 1u) {
-                    RegKey<KB> key;
-                    key.load(o.keys + (uint64_t)j * KB, KB);
                     int r = -1;
                     if (lanes_ok)
-                        r = dx_lane<KB, VB>(t, key, F, o.keys + (uint64_t)j * KB, o.vals + (uint64_t)j * VB,
+                        r = dx_lane<KB, VB>(t, key, h, F, w0, o.keys + (uint64_t)j * KB, o.vals + (uint64_t)j * VB,
                                             sm.exec, a);
                     if (r < 0) defer = true, item = j;
                     else a.claimed += (uint32_t)r;
