@@ -73,28 +73,63 @@ __device__ __forceinline__ uint64_t find_free(const TableView& t, const uint8_t*
     return NONE64;
 }
 
-// The same from a known home h (with capacity >= 8, two aligned windows per
-// round trip).
+// The same from a known home h.  With capacity >= 64: two aligned 8-slot
+// windows in the first round trip (most walks end there), then four per
+// round trip, so a long walk takes fewer trips; smaller tables two windows
+// per trip, or slot by slot below 8 slots.
 __device__ __forceinline__ uint64_t find_free_from(const TableView& t, uint64_t h) {
-    if (t.mask >= 7) {
+    const uint64_t mask = t.mask;
+    if (mask >= 63) {
         uint64_t wb = h & ~7ull;
-        for (uint64_t w = 0; w <= (t.mask >> 4) + 1; ++w, wb += 16) {
-            const uint4* p0 = reinterpret_cast<const uint4*>(t.flags + (wb & t.mask));
-            const uint4* p1 = reinterpret_cast<const uint4*>(t.flags + ((wb + 8) & t.mask));
+        {
+            const uint4* p0 = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
+            const uint4* p1 = reinterpret_cast<const uint4*>(t.flags + ((wb + 8) & mask));
+            const uint4 a = p0[0], b = p0[1], c = p1[0], d = p1[1];
+            const uint32_t f16[16] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w};
+#pragma unroll
+            for (int l = 0; l < 16; l++)
+                if (wb + l >= h && is_free(f16[l])) return (wb + l) & mask;
+        }
+        for (wb += 16; wb - h <= mask; wb += 32) {
+            uint4 x[8];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const uint4* pq = reinterpret_cast<const uint4*>(t.flags + ((wb + 8 * q) & mask));
+                x[2 * q] = pq[0];
+                x[2 * q + 1] = pq[1];
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const uint32_t f4[4] = {x[q].x, x[q].y, x[q].z, x[q].w};
+#pragma unroll
+                for (int l = 0; l < 4; l++) {
+                    const uint64_t pos = wb + 4 * q + l;
+                    if (pos - h > mask) return NONE64;
+                    if (is_free(f4[l])) return pos & mask;
+                }
+            }
+        }
+        return NONE64;
+    }
+    if (mask >= 7) {
+        uint64_t wb = h & ~7ull;
+        for (uint64_t w = 0; w <= (mask >> 4) + 1; ++w, wb += 16) {
+            const uint4* p0 = reinterpret_cast<const uint4*>(t.flags + (wb & mask));
+            const uint4* p1 = reinterpret_cast<const uint4*>(t.flags + ((wb + 8) & mask));
             const uint4 a = p0[0], b = p0[1], c = p1[0], d = p1[1];
             const uint32_t f16[16] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w};
 #pragma unroll
             for (int l = 0; l < 16; l++) {
                 const uint64_t pos = wb + l;
                 if (pos < h) continue;
-                if (pos - h > t.mask) return NONE64;
-                if (is_free(f16[l])) return pos & t.mask;
+                if (pos - h > mask) return NONE64;
+                if (is_free(f16[l])) return pos & mask;
             }
         }
         return NONE64;
     }
-    for (uint64_t p = 0; p <= t.mask; ++p) {
-        const uint64_t s = (h + p) & t.mask;
+    for (uint64_t p = 0; p <= mask; ++p) {
+        const uint64_t s = (h + p) & mask;
         if (is_free(t.flags[s])) return s;
     }
     return NONE64;
