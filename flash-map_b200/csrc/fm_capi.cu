@@ -61,6 +61,16 @@ constexpr uint64_t OP_CHUNK = 1ull << 30;
 #ifndef FM_DIRECT_LOAD
 #define FM_DIRECT_LOAD 0.97  // load from which an insert call skips the rounds
 #endif
+// Queue mode: an insert of at least FM_QUEUE_INS_OPS keys, or one that can
+// take its table to FM_QUEUE_INS_LOAD, runs between persistent launches on the
+// direct passes (launch overhead is small beside it, and its components can
+// outgrow a warp); from FM_DIRECT_LOAD on it runs on the component path.
+#ifndef FM_QUEUE_INS_OPS
+#define FM_QUEUE_INS_OPS (1u << 18)
+#endif
+#ifndef FM_QUEUE_INS_LOAD
+#define FM_QUEUE_INS_LOAD 0.9
+#endif
 #ifndef FM_HANDOFF_LOAD
 #define FM_HANDOFF_LOAD 0.9  // load from which the insert tail hands stalled rounds back
 #endif
@@ -355,7 +365,7 @@ int run_rounds_inner(fm_table* t, bool insert, const uint8_t* d_k, const uint8_t
             // index order per component; what the kernels leave (a table with
             // no free slot for some op, components too large for a warp) runs
             // on the component path
-            e = fm::launch_ins_direct(v, sh, kk, vv, m, t->sc, t->d_ctl, s);
+            e = fm::launch_ins_direct(v, sh, kk, vv, m, t->sc, t->d_ctl, reach, s);
             if (e == cudaSuccess) e = cudaMemcpyAsync(t->h_ctl, t->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
             if (e == cudaSuccess) e = cudaStreamSynchronize(s);
             if (e == cudaSuccess && fault_at(FM_FAULT_ROUND)) e = cudaErrorLaunchFailure;
@@ -1239,7 +1249,9 @@ struct fm_batch {
     // segment and runs on the component path between launches.
     bool qmode = false;
     struct QStep {
-        bool external = false;  // a near-full insert on the component path
+        bool external = false;  // an insert run between persistent launches
+        bool direct = false;    // external: the direct passes (else the component path)
+        double load = 0.0;      // external: the load it can reach (tuned tile width)
         uint32_t op = 0;        // external: the op
         fm::Shape shape = fm::SHAPE_GENERIC;
         uint32_t ph0 = 0, nph = 0;  // persistent launch: its phases (and done counters)
@@ -1404,12 +1416,18 @@ int queue_enqueue(fm_batch* b, cudaStream_t s) {
         if (!st.external) {
             e = fm::launch_queue(st.shape, dph + st.ph0, st.nph, st.units, dq, b->d_done + st.ph0, b->d_qstate + si, s);
         } else {
-            // precheck, the component path, then the write-back (its rounds
-            // see no op left)
+            // precheck; the direct passes with the component path over what
+            // they leave (pend[1]), or the component path over every op; then
+            // the write-back (its rounds see no op left)
             const fm::GroupOp& h = hg[st.ext];
             e = fm::launch_grp_ins(st.shape, dg + st.ext, 1, h.n, fm::GRP_BEGIN, 0, 0, s);
-            if (e == cudaSuccess)
+            if (e == cudaSuccess && st.direct) {
+                e = fm::launch_ins_direct_ctl(h.t, st.shape, h.keys, h.vals, h.n, h.sc, h.ctl, st.load, s);
+                if (e == cudaSuccess)
+                    e = fm::launch_ins_comp(h.t, st.shape, h.keys, h.vals, fm::CMP_N0_CTL, 1, h.n, h.sc, h.ctl, s);
+            } else if (e == cudaSuccess) {
                 e = fm::launch_ins_comp(h.t, st.shape, h.keys, h.vals, fm::CMP_N0_CTL, 0, h.n, h.sc, h.ctl, s);
+            }
             if (e == cudaSuccess) e = cudaMemsetAsync(&h.ctl->n0, 0, sizeof(uint32_t), s);
             if (e == cudaSuccess) e = fm::launch_grp_ins(st.shape, dg + st.ext, 1, h.n, fm::GRP_END, 0, 0, s);
         }
@@ -1424,7 +1442,8 @@ int queue_enqueue(fm_batch* b, cudaStream_t s) {
     return FM_OK;
 }
 
-// Queue mode plan: segments of ops closed by near-full inserts; per segment
+// Queue mode plan: segments of ops closed by the inserts that run between
+// persistent launches (large or able to fill their table); per segment
 // and record shape, the phases of every table's chain of ops listed level by
 // level (the first phase of every chain, then the second, ...), each waiting
 // for the one before it in its chain.
@@ -1450,6 +1469,7 @@ void queue_plan(fm_batch* b) {
                     p.op = i;
                     p.kind = kind;
                     p.units = fm::queue_units(kind, n);
+                    p.per = fm::queue_per(kind, n);
                     c.push_back(p);
                 };
                 if (o.kind == FM_OP_GET) {
@@ -1493,11 +1513,13 @@ void queue_plan(fm_batch* b) {
         if (o.kind == FM_OP_INSERT) {
             const double cap = (double)b->tables[ti]->cap;
             est[ti] += (double)o.n;
-            if (est[ti] >= FM_DIRECT_LOAD * cap) {
+            if (est[ti] >= FM_QUEUE_INS_LOAD * cap || o.n >= FM_QUEUE_INS_OPS) {
                 est[ti] = std::min(est[ti], cap);
                 flush();
                 fm_batch::QStep st;
                 st.external = true;
+                st.direct = est[ti] < FM_DIRECT_LOAD * cap;
+                st.load = est[ti] / cap;
                 st.op = i;
                 st.shape = o.table->shape;
                 st.ext = (uint32_t)b->qext_ops.size();

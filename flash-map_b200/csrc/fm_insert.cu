@@ -2063,9 +2063,10 @@ __device__ __forceinline__ uint64_t dx_next_free(const TableView& t, uint64_t a,
 }
 
 template <int KB>
-__global__ void __launch_bounds__(RBLOCK) k_dx_find(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
+__global__ void __launch_bounds__(RBLOCK) k_dx_find(TableView t, const uint8_t* __restrict__ keys, uint32_t n0_arg,
                                                     OpScratch sc, Ctl* ctl) {
     dx_let_next();
+    const uint32_t n0 = cmp_n0(n0_arg, ctl);
     bool no_free = false;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n0; j += gridDim.x * blockDim.x) {
         RegKey<KB> key;
@@ -2088,10 +2089,11 @@ __global__ void __launch_bounds__(RBLOCK) k_dx_find(TableView t, const uint8_t* 
     if (no_free) ctl->serial[0] = 1u;
 }
 
-__global__ void __launch_bounds__(RBLOCK) k_dx_flow(TableView t, uint32_t n0, OpScratch sc, Ctl* ctl) {
+__global__ void __launch_bounds__(RBLOCK) k_dx_flow(TableView t, uint32_t n0_arg, OpScratch sc, Ctl* ctl) {
     dx_wait_prev();
     dx_let_next();
     if (*(volatile uint32_t*)&ctl->serial[0]) return;  // every op goes to the component path
+    const uint32_t n0 = cmp_n0(n0_arg, ctl);
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n0; j += gridDim.x * blockDim.x) {
         if (!sc.op_flag[j]) continue;
         const uint64_t F = sc.op_slot[j];
@@ -2295,12 +2297,17 @@ __device__ __noinline__ int dx_lane(const TableView& t, const RegKey<KB>& key, u
 // warp-aggregated appends).
 template <int KB, int VB>
 __global__ void __launch_bounds__(DX_THREADS, 2) k_dx_exec(TableView t, const uint8_t* __restrict__ keys,
-                                                           const uint8_t* __restrict__ vals, uint32_t n0,
+                                                           const uint8_t* __restrict__ vals, uint32_t n0_arg,
                                                            OpScratch sc, Ctl* ctl) {
     __shared__ DxLaneSmem s_lane;
     __shared__ uint32_t s_tmp[DX_THREADS / 32];
     dx_wait_prev();
     dx_let_next();
+    const uint32_t n0 = cmp_n0(n0_arg, ctl);
+    // with the count in the control block (a device-driven call) the ops of a
+    // call that found no free slot go to pend[1] for the component path
+    // launched after this pass; otherwise the host reruns every op
+    const bool to_pend = n0_arg == CMP_N0_CTL;
     const bool serial = *(volatile uint32_t*)&ctl->serial[0] != 0;
     const bool lanes_ok = t.mask >= 7 && t.mask < (uint64_t)DIST_MASK;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -2310,6 +2317,7 @@ __global__ void __launch_bounds__(DX_THREADS, 2) k_dx_exec(TableView t, const ui
         const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x + it * stride;
         uint32_t item = 0;
         bool defer = false;
+        if (j < n0 && serial && to_pend) sc.pend[1][atomicAdd(&ctl->npend[1], 1u)] = j;
         if (j < n0) {
             // independent loads together: free slot, home, key; then the
             // registration count with the first metadata window
@@ -2347,13 +2355,13 @@ __global__ void __launch_bounds__(DX_THREADS, 2) k_dx_exec(TableView t, const ui
 }
 
 // One op on a warp: the tile walk (the scalar walk on small tables).
-template <int KB, int VB>
+template <int KB, int VB, int T = 32>
 __device__ __forceinline__ void dx_run_tile(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t j,
-                                            const Tile<32>& tl, P4Chain<32>& s, ExecAcc& a) {
+                                            const Tile<T>& tl, P4Chain<T>& s, ExecAcc& a) {
     RegKey<KB> key;
     key.load(keys + (uint64_t)j * KB, KB);
-    if (t.mask >= 4 * 32 - 1) {
-        if (exec_tile<KB, VB, 32, P4Chain<32>>(t, key, vals, j, tl, s, a) == 5) a.limit = true;
+    if (t.mask >= 4 * T - 1) {
+        if (exec_tile<KB, VB, T, P4Chain<T>>(t, key, vals, j, tl, s, a) == 5) a.limit = true;
     } else if (tl.lane == 0) {
         a.claimed += exec_insert_key<KB, VB>(t, key, vals + (uint64_t)j * VB, a);
     }
@@ -2366,8 +2374,9 @@ __device__ __forceinline__ void dx_run_tile(const TableView& t, const uint8_t* k
 // and list words set idle on the way; then sorted into index order by the
 // warp.  Returns their count, or 0 when there are more than DX_GATHER (their
 // ops then go to pend[1] for the component path).
+template <int T = 32>
 __device__ __noinline__ uint32_t dx_gather(const TableView& t, uint32_t j, uint32_t n0, const OpScratch& sc,
-                                           Ctl* ctl, uint32_t* s_ops, const Tile<32>& tl) {
+                                           Ctl* ctl, uint32_t* s_ops, const Tile<T>& tl) {
     uint32_t g = 0;
     if (tl.lane == 0) {
         const uint64_t mask = t.mask;
@@ -2408,47 +2417,65 @@ __device__ __noinline__ uint32_t dx_gather(const TableView& t, uint32_t j, uint3
     g = tl.shfl(g, 0);
     tl.sync();
     if (g > (uint32_t)DX_GATHER) return 0;
+    // index order: each lane ranks DX_GATHER / T entries
+    constexpr int PER = DX_GATHER / T;
     const uint32_t lane = tl.lane;
-    const uint32_t v0 = lane < g ? s_ops[lane] : 0u;
-    const uint32_t v1 = lane + 32 < g ? s_ops[lane + 32] : 0u;
-    uint32_t r0 = 0, r1 = 0;
+    uint32_t v[PER], r[PER];
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+        v[u] = lane + T * u < g ? s_ops[lane + T * u] : 0u;
+        r[u] = 0;
+    }
     for (uint32_t q = 0; q < g; q++) {
         const uint32_t x = s_ops[q];
-        r0 += x < v0 ? 1u : 0u;
-        r1 += x < v1 ? 1u : 0u;
+#pragma unroll
+        for (int u = 0; u < PER; u++) r[u] += x < v[u] ? 1u : 0u;
     }
     tl.sync();
-    if (lane < g) s_ops[r0] = v0;
-    if (lane + 32 < g) s_ops[r1] = v1;
+#pragma unroll
+    for (int u = 0; u < PER; u++)
+        if (lane + T * u < g) s_ops[r[u]] = v[u];
     tl.sync();
     return g;
 }
 
-// The warp pass: a warp per entry of the list the exec pass built.
-template <int KB, int VB>
+// The warp pass: a tile of T lanes per entry of the list the exec pass built
+// (T: 32, 16 or 8, chosen per record shape and load by the autotuner; a
+// narrower tile reads fewer slots per round trip but runs more entries at
+// once).
+template <int KB, int VB, int T>
 __global__ void __launch_bounds__(RBLOCK, FM_P4_MIN_BLOCKS) k_dx_warp(TableView t, const uint8_t* __restrict__ keys,
-                                                                      const uint8_t* __restrict__ vals, uint32_t n0,
+                                                                      const uint8_t* __restrict__ vals, uint32_t n0_arg,
                                                                       OpScratch sc, Ctl* ctl) {
-    constexpr int NW = RBLOCK / 32;
-    __shared__ P4Chain<32> s_chain[NW];
-    __shared__ uint32_t s_ops[NW][DX_GATHER];
-    __shared__ uint32_t s_tmp[NW];
+    constexpr int NT = RBLOCK / T;
+    __shared__ P4Chain<T> s_chain[NT];
+    __shared__ uint32_t s_ops[NT][DX_GATHER];
+    __shared__ uint32_t s_tmp[RBLOCK / 32];
     dx_wait_prev();
     const uint32_t n = *(volatile const uint32_t*)&ctl->nlong[0];
     if (n == 0) return;  // block-uniform
-    const Tile<32> tl;
-    const uint32_t wi = threadIdx.x >> 5;
+    const uint32_t n0 = cmp_n0(n0_arg, ctl);
+    const Tile<T> tl;
+    const uint32_t ti = threadIdx.x / T;
     ExecAcc a;
-    for (uint32_t i = blockIdx.x * NW + wi; i < n; i += gridDim.x * NW) {
-        const uint32_t item = sc.long_list[i];
-        uint32_t g = 1;  // a lone op, or a component's ops in index order
-        if (item & DX_ROOT) {
-            g = dx_gather(t, item & ~DX_ROOT, n0, sc, ctl, s_ops[wi], tl);
-        } else {
-            if (tl.lane == 0) s_ops[wi][0] = item;
-            tl.sync();
+    // uniform trip count per warp: all tiles of a warp loop together
+    const uint32_t ntiles = gridDim.x * NT;
+    const uint32_t iters = (n + ntiles - 1) / ntiles;
+    for (uint32_t it = 0; it < iters; it++) {
+        const uint32_t i = blockIdx.x * NT + ti + it * ntiles;
+        uint32_t g = 0;  // a lone op, or a component's ops in index order
+        if (i < n) {
+            const uint32_t item = sc.long_list[i];
+            if (item & DX_ROOT) {
+                g = dx_gather<T>(t, item & ~DX_ROOT, n0, sc, ctl, s_ops[ti], tl);
+            } else {
+                if (tl.lane == 0) s_ops[ti][0] = item;
+                g = 1;
+            }
         }
-        for (uint32_t q = 0; q < g; q++) dx_run_tile<KB, VB>(t, keys, vals, s_ops[wi][q], tl, s_chain[wi], a);
+        tl.sync();
+        for (uint32_t q = 0; q < g; q++) dx_run_tile<KB, VB, T>(t, keys, vals, s_ops[ti][q], tl, s_chain[ti], a);
+        __syncwarp();
     }
     block_add_count(ctl, a.claimed, s_tmp);
     publish_rare(ctl, a.maxd, a.tomb, a.limit);
@@ -2467,21 +2494,24 @@ __global__ void __launch_bounds__(RBLOCK, FM_P4_MIN_BLOCKS) k_dx_warp(TableView 
 // it, so the waits end whether or not all blocks are resident at once.
 //
 // Units (all block-wide, QTHREADS threads):
-//   QP_GET    QG_UNIT queries, one thread per query (the thread probe);
+//   QP_GET    up to QG_UNIT queries, QG_Q per thread probed in lockstep;
 //   QP_BEGIN  the op's control block reset and, for a counted insert, the
 //             TableFull precheck against the table's count at this point;
-//   QP_IFIND / QP_IFLOW / QP_IEXEC  QI_UNIT ops of the direct insert's find,
+//   QP_IFIND / QP_IFLOW / QP_IEXEC  up to QI_UNIT ops of the direct insert's find,
 //             flow and exec passes;
 //   QP_IWARP  8 warps over the exec pass's list, strided over the phase's
 //             units (lone long walks and components as tile walks);
-//   QP_RFIND / QP_REXEC  QI_UNIT ops of the direct remove;
+//   QP_RFIND / QP_REXEC  up to QI_UNIT ops of the direct remove;
 //   QP_END    what the direct passes left (every op when some op found no
 //             free slot / EMPTY slot, or the ops of oversized groups) in index
 //             order on this block, then the op's result, status and the
 //             table's count.
 constexpr int QTHREADS = 256;
-constexpr uint32_t QG_UNIT = 1024;  // queries per lookup unit
-constexpr uint32_t QI_UNIT = 512;   // ops per find / flow / exec unit
+constexpr uint32_t QG_UNIT = 2048;  // largest lookup unit (queries)
+constexpr uint32_t QSPREAD = 296;   // units a phase is cut into where it can be (two blocks per SM)
+template <int KB>
+constexpr int QG_Q = 4;  // lookups per thread in lockstep
+constexpr uint32_t QI_UNIT = 512;   // largest find / flow / exec unit (ops)
 constexpr uint64_t QWAIT_NS = 2000000000ull;  // bound of one dependency wait
 
 __device__ __forceinline__ uint64_t q_now() {
@@ -2534,16 +2564,23 @@ __device__ __noinline__ void q_get_small(const TableView& t, const uint8_t* qk, 
 }
 
 template <int KB, int VB>
-__device__ __noinline__ void q_get(const QOp& o, uint32_t c) {
+__device__ __noinline__ void q_get(const QOp& o, uint32_t c, uint32_t per) {
     const TableView& t = o.t;
-    const uint64_t q0 = (uint64_t)c * QG_UNIT;
-    const uint64_t q1 = min((uint64_t)o.n, q0 + QG_UNIT);
+    const uint64_t q0 = (uint64_t)c * per;
+    const uint64_t q1 = min((uint64_t)o.n, q0 + per);
+    if (t.mask >= 7) {
+        // QG_Q queries per thread in lockstep: two resident blocks of
+        // QTHREADS per SM keep QG_Q times as many probes in flight
+#pragma unroll 1
+        for (uint64_t q = q0 + threadIdx.x; q < q1; q += (uint64_t)QTHREADS * QG_Q<KB>)
+            get_queries_lockstep<KB, VB, QG_Q<KB>>(t, o.keys, q, QTHREADS, q1, o.out_vals, o.out_found);
+        return;
+    }
 #pragma unroll 1
     for (uint64_t q = q0 + threadIdx.x; q < q1; q += QTHREADS) {
         uint8_t* ov = o.out_vals ? o.out_vals + q * VB : nullptr;
         uint8_t* of = o.out_found ? o.out_found + q : nullptr;
-        if (t.mask >= 7) get_query_thread<KB, VB>(t, o.keys + q * KB, ov, of);
-        else q_get_small<KB, VB>(t, o.keys + q * KB, ov, of);
+        q_get_small<KB, VB>(t, o.keys + q * KB, ov, of);
     }
 }
 
@@ -2567,11 +2604,11 @@ __device__ __noinline__ void q_begin(const QOp& o) {
 __device__ __forceinline__ uint32_t q_n0(const QOp& o) { return *(volatile const uint32_t*)&o.ctl->n0; }
 
 template <int KB>
-__device__ __noinline__ void q_ifind(const QOp& o, uint32_t c) {
+__device__ __noinline__ void q_ifind(const QOp& o, uint32_t c, uint32_t per) {
     const uint32_t n0 = q_n0(o);
-    const uint32_t j = c * QI_UNIT + threadIdx.x;
+    const uint32_t j = c * per + threadIdx.x;
     bool no_free = false;
-    for (uint32_t k = 0; k < QI_UNIT / QTHREADS; k++) {
+    for (uint32_t k = 0; k < per / QTHREADS; k++) {
         const uint32_t jj = j + k * QTHREADS;
         if (jj >= n0) break;
         RegKey<KB> key;
@@ -2594,12 +2631,12 @@ __device__ __noinline__ void q_ifind(const QOp& o, uint32_t c) {
     if (no_free) o.ctl->serial[0] = 1u;
 }
 
-__device__ __noinline__ void q_iflow(const QOp& o, uint32_t c) {
+__device__ __noinline__ void q_iflow(const QOp& o, uint32_t c, uint32_t per) {
     const uint32_t n0 = q_n0(o);
     if (*(volatile uint32_t*)&o.ctl->serial[0]) return;
     const TableView& t = o.t;
-    for (uint32_t k = 0; k < QI_UNIT / QTHREADS; k++) {
-        const uint32_t j = c * QI_UNIT + threadIdx.x + k * QTHREADS;
+    for (uint32_t k = 0; k < per / QTHREADS; k++) {
+        const uint32_t j = c * per + threadIdx.x + k * QTHREADS;
         if (j >= n0) break;
         if (!o.sc.op_flag[j]) continue;
         const uint64_t F = o.sc.op_slot[j];
@@ -2630,14 +2667,14 @@ __device__ __noinline__ void q_iflow(const QOp& o, uint32_t c) {
 }
 
 template <int KB, int VB>
-__device__ __noinline__ void q_iexec(const QOp& o, uint32_t c, QSmem& sm) {
+__device__ __noinline__ void q_iexec(const QOp& o, uint32_t c, uint32_t per, QSmem& sm) {
     const uint32_t n0 = q_n0(o);
     const TableView& t = o.t;
     const bool serial = *(volatile uint32_t*)&o.ctl->serial[0] != 0;
     const bool lanes_ok = t.mask >= 7 && t.mask < (uint64_t)DIST_MASK;
     ExecAcc a;
-    for (uint32_t k = 0; k < QI_UNIT / QTHREADS; k++) {  // block-uniform trip count
-        const uint32_t j = c * QI_UNIT + threadIdx.x + k * QTHREADS;
+    for (uint32_t k = 0; k < per / QTHREADS; k++) {  // block-uniform trip count
+        const uint32_t j = c * per + threadIdx.x + k * QTHREADS;
         uint32_t item = 0;
         bool defer = false;
         if (j < n0) {
@@ -2698,11 +2735,11 @@ __device__ __noinline__ void q_iwarp(const QOp& o, uint32_t c, uint32_t units, Q
 }
 
 template <int KB>
-__device__ __noinline__ void q_rfind(const QOp& o, uint32_t c) {
+__device__ __noinline__ void q_rfind(const QOp& o, uint32_t c, uint32_t per) {
     const uint32_t n0 = q_n0(o);
     bool no_empty = false;
-    for (uint32_t k = 0; k < QI_UNIT / QTHREADS; k++) {
-        const uint32_t j = c * QI_UNIT + threadIdx.x + k * QTHREADS;
+    for (uint32_t k = 0; k < per / QTHREADS; k++) {
+        const uint32_t j = c * per + threadIdx.x + k * QTHREADS;
         if (j >= n0) break;
         RegKey<KB> key;
         const uint64_t E = rx_first_empty(o.t, home_of<KB>(o.t, o.keys, j, key));
@@ -2722,13 +2759,13 @@ __device__ __noinline__ void q_rfind(const QOp& o, uint32_t c) {
 }
 
 template <int KB>
-__device__ __noinline__ void q_rexec(const QOp& o, uint32_t c, QSmem& sm) {
+__device__ __noinline__ void q_rexec(const QOp& o, uint32_t c, uint32_t per, QSmem& sm) {
     const uint32_t n0 = q_n0(o);
     const TableView& t = o.t;
     const bool serial = *(volatile uint32_t*)&o.ctl->serial[0] != 0;
     uint32_t removed = 0;
-    for (uint32_t k = 0; k < QI_UNIT / QTHREADS; k++) {  // block-uniform trip count
-        const uint32_t j = c * QI_UNIT + threadIdx.x + k * QTHREADS;
+    for (uint32_t k = 0; k < per / QTHREADS; k++) {  // block-uniform trip count
+        const uint32_t j = c * per + threadIdx.x + k * QTHREADS;
         uint64_t E = NONE64;
         uint32_t cnt = 0;
         bool lead = false;
@@ -2857,14 +2894,14 @@ __global__ void __launch_bounds__(QTHREADS, 2) k_queue(const QPhase* __restrict_
         const QOp& o = ops[p.op];
         const uint32_t c = (uint32_t)(u - p.base);
         switch (p.kind) {
-            case QP_GET: q_get<KB, VB>(o, c); break;
+            case QP_GET: q_get<KB, VB>(o, c, p.per); break;
             case QP_BEGIN: q_begin(o); break;
-            case QP_IFIND: q_ifind<KB>(o, c); break;
-            case QP_IFLOW: q_iflow(o, c); break;
-            case QP_IEXEC: q_iexec<KB, VB>(o, c, sm); break;
+            case QP_IFIND: q_ifind<KB>(o, c, p.per); break;
+            case QP_IFLOW: q_iflow(o, c, p.per); break;
+            case QP_IEXEC: q_iexec<KB, VB>(o, c, p.per, sm); break;
             case QP_IWARP: q_iwarp<KB, VB>(o, c, p.units, sm); break;
-            case QP_RFIND: q_rfind<KB>(o, c); break;
-            case QP_REXEC: q_rexec<KB>(o, c, sm); break;
+            case QP_RFIND: q_rfind<KB>(o, c, p.per); break;
+            case QP_REXEC: q_rexec<KB>(o, c, p.per, sm); break;
             default: q_end<KB, VB>(o, sm); break;
         }
         __threadfence();  // this unit's writes before its count
@@ -3197,17 +3234,24 @@ void launch_dependent(void (*k)(P...), unsigned grid, unsigned block, cudaStream
 
 // The direct insert of a call (compile-time shapes): find, flow, exec, warp.
 template <int KB, int VB>
-void direct_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, const OpScratch& sc,
-                  Ctl* ctl, cudaStream_t s) {
+constexpr Shape sh_of() {
+    return (KB == 8 && VB == 8) ? SHAPE_8_8
+         : (KB == 32 && VB == 128) ? SHAPE_32_128
+         : (KB == 32 && VB == 64) ? SHAPE_32_64
+         : (KB == 32 && VB == 32) ? SHAPE_32_32
+         : (KB == 8 && VB == 32) ? SHAPE_8_32 : SHAPE_GENERIC;
+}
+
+template <int KB, int VB>
+void direct_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, uint32_t n0, uint32_t nmax,
+                  const OpScratch& sc, Ctl* ctl, float load, bool pdl_ok, cudaStream_t s) {
     if constexpr (KB == 0 || VB == 0) {
         return;
     } else {
-        const unsigned g = grid_for(n0, 8);
-        // a warp per entry the exec pass may list, up to the blocks resident at once
-        const unsigned gw = grid_for((uint64_t)n0 * 32, FM_P4_MIN_BLOCKS);
+        const unsigned g = grid_for(nmax, 8);
         // with per-kernel timing on, events sit between the kernels, so they
         // run as plain launches
-        const bool pdl = FM_DX_PDL && !kt_active();
+        const bool pdl = pdl_ok && FM_DX_PDL && !kt_active();
         {
             KtScope kt(KC_INS_FIND, s);
             k_dx_find<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
@@ -3222,7 +3266,11 @@ void direct_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, 
         }
         {
             KtScope kt(KC_INS_LONG, s);
-            launch_dependent(k_dx_warp<KB, VB>, gw, RBLOCK, s, pdl, t, keys, vals, n0, sc, ctl);
+            const int tw = tuned_ins_cfg(sh_of<KB, VB>(), (double)load).tile;
+            const unsigned gwt = grid_for((uint64_t)nmax * tw, FM_P4_MIN_BLOCKS);
+            if (tw == 8) launch_dependent(k_dx_warp<KB, VB, 8>, gwt, RBLOCK, s, pdl, t, keys, vals, n0, sc, ctl);
+            else if (tw == 16) launch_dependent(k_dx_warp<KB, VB, 16>, gwt, RBLOCK, s, pdl, t, keys, vals, n0, sc, ctl);
+            else launch_dependent(k_dx_warp<KB, VB, 32>, gwt, RBLOCK, s, pdl, t, keys, vals, n0, sc, ctl);
         }
         count_launches(4);
     }
@@ -3250,21 +3298,52 @@ cudaError_t launch_ins_rounds(const TableView& t, Shape sh, const uint8_t* keys,
 }
 
 cudaError_t launch_ins_direct(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
-                              const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+                              const OpScratch& sc, Ctl* ctl, double load, cudaStream_t s) {
     if (sh == SHAPE_GENERIC || !sc.comp) return cudaErrorInvalidValue;
-#define FM_CALL(K, V) direct_shape<K, V>(t, keys, vals, n0, sc, ctl, s)
+#define FM_CALL(K, V) direct_shape<K, V>(t, keys, vals, n0, n0, sc, ctl, (float)load, true, s)
     FM_SHAPE_SWITCH(sh, FM_CALL)
 #undef FM_CALL
     return cudaGetLastError();
 }
 
+cudaError_t launch_ins_direct_ctl(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals,
+                                  uint32_t nmax, const OpScratch& sc, Ctl* ctl, double load, cudaStream_t s) {
+    if (sh == SHAPE_GENERIC || !sc.comp) return cudaErrorInvalidValue;
+#define FM_CALL(K, V) direct_shape<K, V>(t, keys, vals, CMP_N0_CTL, nmax, sc, ctl, (float)load, false, s)
+    FM_SHAPE_SWITCH(sh, FM_CALL)
+#undef FM_CALL
+    return cudaGetLastError();
+}
+
+// Tuned insert configurations, per shape and load bucket (tile 0: not measured).
+InsCfg g_ins_tuned[SHAPE_GENERIC + 1][LOAD_BUCKETS];
+
+InsCfg tuned_ins_cfg(Shape sh, double load) {
+    InsCfg c = g_ins_tuned[sh][load_bucket(load)];
+    if (c.tile != 8 && c.tile != 16 && c.tile != 32) c.tile = 32;
+    return c;
+}
+
+void set_tuned_ins_cfg(Shape sh, int bucket, InsCfg cfg) { g_ins_tuned[sh][bucket] = cfg; }
+
+uint32_t queue_per(uint32_t kind, uint32_t n) {
+    // about QSPREAD units per phase where the op is large enough, in whole
+    // multiples of QTHREADS items, at most the kind's largest unit
+    const uint32_t most = kind == QP_GET ? QG_UNIT : QI_UNIT;
+    const uint32_t want = (n + QSPREAD - 1) / QSPREAD;
+    const uint32_t per = (want + QTHREADS - 1) / QTHREADS * QTHREADS;
+    return per < (uint32_t)QTHREADS ? QTHREADS : (per > most ? most : per);
+}
+
 uint32_t queue_units(uint32_t kind, uint32_t n) {
     switch (kind) {
-        case QP_GET: return (n + QG_UNIT - 1) / QG_UNIT;
         case QP_BEGIN:
         case QP_END: return 1;
         case QP_IWARP: return (n + 63) / 64;  // 8 warps per unit: a warp per 8 ops the exec pass may list
-        default: return (n + QI_UNIT - 1) / QI_UNIT;
+        default: {
+            const uint32_t per = queue_per(kind, n);
+            return (n + per - 1) / per;
+        }
     }
 }
 

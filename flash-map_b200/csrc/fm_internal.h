@@ -110,7 +110,13 @@ cudaError_t launch_ins_rounds(const TableView& t, Shape sh, const uint8_t* keys,
 // Ctl::npend[1] ops (components too large for a warp) are left in pend[1]
 // for launch_ins_comp at round 1.
 cudaError_t launch_ins_direct(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals, uint32_t n0,
-                              const OpScratch& sc, Ctl* ctl, cudaStream_t s);
+                              const OpScratch& sc, Ctl* ctl, double load, cudaStream_t s);
+// The same passes with the op count read from Ctl::n0 (a grouped call after
+// its precheck; nmax bounds it and sizes the grids) and no host step after
+// them: a call that found no free slot lists every op in pend[1], so
+// launch_ins_comp at round 1 with CMP_N0_CTL completes the call either way.
+cudaError_t launch_ins_direct_ctl(const TableView& t, Shape sh, const uint8_t* keys, const uint8_t* vals,
+                                  uint32_t nmax, const OpScratch& sc, Ctl* ctl, double load, cudaStream_t s);
 // Runs every remaining round starting at r in one block if the pending count
 // is at most TAIL_MAX; otherwise returns without touching anything.  With
 // handoff, rounds that stop progressing are left pending for the host
@@ -191,6 +197,13 @@ void set_tuned_get_cfg(Shape sh, int load_bucket, GetCfg cfg);
 constexpr int LOAD_BUCKETS = 3;  // load < 0.6, < 0.8, >= 0.8
 inline int load_bucket(double load) { return load < 0.6 ? 0 : (load < 0.8 ? 1 : 2); }
 
+// Direct insert configuration: lanes per entry of the warp pass (8, 16 or 32).
+struct InsCfg {
+    int tile = 32;
+};
+InsCfg tuned_ins_cfg(Shape sh, double load);  // defaults when none was measured
+void set_tuned_ins_cfg(Shape sh, int load_bucket, InsCfg cfg);
+
 // Fills `bytes` (a multiple of 8) with seeded pseudo-random words.
 cudaError_t launch_fill_random(void* out, uint64_t bytes, uint64_t seed, cudaStream_t s);
 
@@ -228,6 +241,7 @@ enum QPhaseKind : uint32_t {
 struct QPhase {
     uint64_t base;
     uint32_t units;
+    uint32_t per;  // items (queries / ops) per unit
     uint32_t op;
     uint32_t kind;
     int32_t dep;
@@ -254,7 +268,9 @@ struct QState {
     uint32_t err;             // 1: a dependency wait ran out
     uint32_t pad_;
 };
-// Units of each phase kind for an op of n keys.
+// Items per unit and units of each phase kind for an op of n keys: small
+// ops get small units, so that one op's phase still spreads over the SMs.
+uint32_t queue_per(uint32_t kind, uint32_t n);
 uint32_t queue_units(uint32_t kind, uint32_t n);
 // One persistent launch over phases [0, nph) of ops of one record shape;
 // `done` holds nph zeroed counters and `st` a zeroed QState.

@@ -76,6 +76,109 @@ __device__ __forceinline__ void get_query_thread(const TableView& t, const uint8
     if (of) *of = hit != NONE64 ? 1 : 0;
 }
 
+// Q lookups per thread probed in lockstep (compile-time shapes, capacity >=
+// 8): queries q0, q0 + stride, ... below q1.  Each step loads the 8-slot
+// metadata window of every query still probing (Q independent loads in
+// flight), then compares candidate keys one candidate per query per pass, so
+// a thread keeps Q chains of dependent reads going where get_query_thread
+// keeps one: what a kernel with few resident threads per SM needs.  Table
+// loads are plain (coherent) loads -- the persistent batch kernel runs
+// lookups after writes made by other blocks of the same launch; the query
+// keys are read through the read-only path.  Semantics as get_query_thread.
+template <int KB, int VB, int Q>
+__device__ __forceinline__ void get_queries_lockstep(const TableView& t, const uint8_t* __restrict__ keys,
+                                                     uint64_t q0, uint64_t stride, uint64_t q1,
+                                                     uint8_t* __restrict__ ov, uint8_t* __restrict__ of) {
+    const uint64_t mask = t.mask;
+    RegKey<KB> key[Q];
+    uint64_t h[Q], wb[Q], hit[Q];
+    uint32_t act = 0;
+#pragma unroll
+    for (int i = 0; i < Q; i++) {
+        const uint64_t q = q0 + (uint64_t)i * stride;
+        h[i] = 0;
+        hit[i] = NONE64;
+        if (q < q1) {
+            key[i].load(keys + q * KB, KB);
+            h[i] = key[i].hash(KB, t.hash_mode) & mask;
+            act |= 1u << i;
+        }
+        wb[i] = h[i] & ~7ull;
+    }
+    while (act) {
+        uint4 wa[Q], wz[Q];
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            if (act >> i & 1u) {
+                const uint4* fp = reinterpret_cast<const uint4*>(t.flags + (wb[i] & mask));
+                wa[i] = fp[0];
+                wz[i] = fp[1];
+            }
+        }
+        uint32_t cand[Q];
+        uint32_t stop = 0;
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+            cand[i] = 0;
+            if (!(act >> i & 1u)) continue;
+            const uint32_t f8[8] = {wa[i].x, wa[i].y, wa[i].z, wa[i].w, wz[i].x, wz[i].y, wz[i].z, wz[i].w};
+            bool done = false;
+#pragma unroll
+            for (int l = 0; l < 8; l++) {
+                const uint64_t pos = wb[i] + l;
+                if (done || pos < h[i]) continue;
+                const uint64_t p = pos - h[i];
+                const uint32_t f = f8[l];
+                const uint32_t s = st_of(f);
+                if (p > mask || s == ST_EMPTY || (s == ST_OCC && p > dist_of(f))) done = true;
+                else if (s == ST_OCC && dist_matches(f, p)) cand[i] |= 1u << l;
+            }
+            if (done) stop |= 1u << i;
+        }
+        // candidates in walk order, one per query per pass
+        for (;;) {
+            uint32_t more = 0;
+#pragma unroll
+            for (int i = 0; i < Q; i++) {
+                if (!cand[i]) continue;
+                const uint64_t slot = (wb[i] + (uint64_t)(__ffs(cand[i]) - 1)) & mask;
+                if (key[i].eq(t.keys + slot * KB, KB)) {
+                    hit[i] = slot;
+                    cand[i] = 0;
+                    stop |= 1u << i;
+                } else {
+                    cand[i] &= cand[i] - 1;
+                }
+                more |= cand[i];
+            }
+            if (!more) break;
+        }
+        act &= ~stop;
+#pragma unroll
+        for (int i = 0; i < Q; i++) wb[i] += 8;
+    }
+    // values: a few hits' loads in flight before their stores
+    constexpr int VG = VB >= 64 ? 1 : Q;
+#pragma unroll
+    for (int g = 0; g < Q; g += VG) {
+        RegVal<VB> v[VG];
+#pragma unroll
+        for (int i = 0; i < VG; i++) {
+            if (g + i >= Q) break;
+            if (ov && hit[g + i] != NONE64) v[i].load(t.vals + hit[g + i] * VB, VB);
+            else v[i].zero();
+        }
+#pragma unroll
+        for (int i = 0; i < VG; i++) {
+            if (g + i >= Q) break;
+            const uint64_t q = q0 + (uint64_t)(g + i) * stride;
+            if (q >= q1) continue;
+            if (ov) v[i].store(ov + q * VB, VB);
+            if (of) of[q] = hit[g + i] != NONE64 ? 1 : 0;
+        }
+    }
+}
+
 // First EMPTY slot at or after home h, NONE64 when the table has none (two
 // aligned 8-slot windows per round trip with capacity >= 8).
 __device__ __forceinline__ uint64_t rx_first_empty(const TableView& t, uint64_t h) {
@@ -177,7 +280,8 @@ constexpr uint32_t RX_GMAX = 256;
 // warp commits the ops in index order: an op whose probe range [home, stop]
 // holds a slot that an earlier op of its chunk tombstoned probes again on the
 // current table; any other op's probe is unchanged by them (removes change
-// nothing but those slots), so its result stands.  Returns the ops removed;
+// nothing but those slots), so its result stands.  Returns the ops removed
+// (the group's total, on every lane);
 // a group of more than RX_GMAX ops goes to pend[1] instead (0 returned).
 // Warp-uniform call.
 template <int KB>
@@ -259,7 +363,7 @@ __device__ __noinline__ uint32_t rx_group(const TableView& t, const uint8_t* key
             __syncwarp();
         }
     }
-    return removed;
+    return __reduce_add_sync(0xFFFFFFFFu, removed);  // each lane counted the ops it committed
 }
 
 }  // namespace fm

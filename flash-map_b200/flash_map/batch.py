@@ -52,10 +52,11 @@ class FlashMapBatch:
             a.table = o.table._h.value
             a.kind = int(o.kind)
             a.n = int(o.n)
-            a.d_keys = _dev_ptr(o.keys) if o.keys is not None else None
-            a.d_values = _dev_ptr(o.values) if o.values is not None else None
-            a.d_out_values = _dev_ptr(o.out_values) if o.out_values is not None else None
-            a.d_out_found = _dev_ptr(o.out_found) if o.out_found is not None else None
+            n, ks, vs = int(o.n), o.table.key_size, o.table.value_size
+            a.d_keys = _dev_ptr(o.keys, n * ks, f"op {i} keys") if o.keys is not None else None
+            a.d_values = _dev_ptr(o.values, n * vs, f"op {i} values") if o.values is not None else None
+            a.d_out_values = _dev_ptr(o.out_values, n * vs, f"op {i} out_values") if o.out_values is not None else None
+            a.d_out_found = _dev_ptr(o.out_found, n, f"op {i} out_found") if o.out_found is not None else None
         self._arr = arr
         h = C.c_void_p()
         rc = self._L.fm_batch_create(arr, len(ops), C.byref(h))

@@ -62,11 +62,19 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
 
 
-def _dev_ptr(x) -> int:
-    """Raw device pointer from a torch tensor / object with data_ptr() / int."""
+def _dev_ptr(x, nbytes: Optional[int] = None, what: str = "buffer") -> int:
+    """Raw device pointer from a torch tensor / object with data_ptr() / int.
+    With nbytes, a tensor (anything with numel() and element_size()) must
+    hold at least that many bytes: the kernels read and write count records
+    from the pointer and cannot see the buffer's end (a raw pointer is the
+    caller's to size)."""
     if isinstance(x, int):
         return x
     if hasattr(x, "data_ptr"):
+        if nbytes is not None and hasattr(x, "numel") and hasattr(x, "element_size"):
+            have = int(x.numel()) * int(x.element_size())
+            if have < nbytes:
+                raise ValueError(f"{what}: {have} bytes, the call needs {nbytes}")
         return int(x.data_ptr())
     raise TypeError("device buffer must be a raw pointer or expose data_ptr()")
 
@@ -197,27 +205,32 @@ class FlashMap:
     def bulk_get_device(self, d_keys, count: int, d_out_values, d_out_found, stream=None) -> None:
         """Lookup with keys and outputs in caller-owned device memory.
         Misses write zeros.  Stream-ordered on ``stream``; does not sync."""
-        self._check(self._L.fm_bulk_get_device(self._h, _dev_ptr(d_keys), count, _dev_ptr(d_out_values),
-                                               _dev_ptr(d_out_found), _stream_ptr(stream)))
+        ks, vs = self.key_size, self.value_size
+        self._check(self._L.fm_bulk_get_device(self._h, _dev_ptr(d_keys, count * ks, "keys"), count,
+                                               _dev_ptr(d_out_values, count * vs, "out_values"),
+                                               _dev_ptr(d_out_found, count, "out_found"), _stream_ptr(stream)))
 
     def bulk_get_values_device(self, d_keys, count: int, d_out_values, stream=None) -> None:
-        self._check(self._L.fm_bulk_get_values_device(self._h, _dev_ptr(d_keys), count,
-                                                      _dev_ptr(d_out_values), _stream_ptr(stream)))
+        self._check(self._L.fm_bulk_get_values_device(self._h, _dev_ptr(d_keys, count * self.key_size, "keys"), count,
+                                                      _dev_ptr(d_out_values, count * self.value_size, "out_values"),
+                                                      _stream_ptr(stream)))
 
     def bulk_insert_device(self, d_keys, d_values, count: int, stream=None) -> int:
         out = C.c_uint64(0)
-        self._check(self._L.fm_bulk_insert_device(self._h, _dev_ptr(d_keys), _dev_ptr(d_values), count,
+        self._check(self._L.fm_bulk_insert_device(self._h, _dev_ptr(d_keys, count * self.key_size, "keys"),
+                                                  _dev_ptr(d_values, count * self.value_size, "values"), count,
                                                   C.byref(out), _stream_ptr(stream)))
         return out.value
 
     def bulk_insert_device_uncounted(self, d_keys, d_values, count: int, stream=None) -> None:
-        self._check(self._L.fm_bulk_insert_device_uncounted(self._h, _dev_ptr(d_keys), _dev_ptr(d_values), count,
-                                                            _stream_ptr(stream)))
+        self._check(self._L.fm_bulk_insert_device_uncounted(self._h, _dev_ptr(d_keys, count * self.key_size, "keys"),
+                                                            _dev_ptr(d_values, count * self.value_size, "values"),
+                                                            count, _stream_ptr(stream)))
 
     def bulk_remove_device(self, d_keys, count: int, stream=None) -> int:
         out = C.c_uint64(0)
-        self._check(self._L.fm_bulk_remove_device(self._h, _dev_ptr(d_keys), count, C.byref(out),
-                                                  _stream_ptr(stream)))
+        self._check(self._L.fm_bulk_remove_device(self._h, _dev_ptr(d_keys, count * self.key_size, "keys"), count,
+                                                  C.byref(out), _stream_ptr(stream)))
         return out.value
 
     def recount(self) -> int:

@@ -76,3 +76,20 @@ def test_zero_capacity_before_device_use():
 
     with pytest.raises(F.ZeroCapacity):
         F.FlashMap(0, 8, 8)
+
+
+def test_device_buffers_smaller_than_the_call_are_refused():
+    """The kernels read and write count records from each device pointer and
+    cannot see a buffer's end: a tensor that holds fewer bytes than the call
+    needs is refused on the host, before any launch."""
+    import torch
+
+    from flash_map.map import _dev_ptr
+
+    t = torch.zeros((50, 32), dtype=torch.uint8)
+    assert _dev_ptr(t, 50 * 32, "keys") == t.data_ptr()
+    with pytest.raises(ValueError, match="keys: 1600 bytes, the call needs 3200"):
+        _dev_ptr(t, 100 * 32, "keys")
+    w = torch.zeros(100, dtype=torch.int64)  # sized in bytes, not elements
+    assert _dev_ptr(w, 800, "values") == w.data_ptr()
+    assert _dev_ptr(12345, 1 << 40) == 12345  # a raw pointer is the caller's to size

@@ -299,3 +299,49 @@ def test_batch_near_full_inserts_between_queue_launches(graph):
         assert t["g"].len() == t["o"].len()
         for x, y in zip(t["g"].snapshot(), t["o"].snapshot()):
             assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batch_large_and_high_load_inserts(graph):
+    """The insert routes of the queue, each between gets and removes on the
+    same table: an insert of 2^18 keys and inserts that take a table to load
+    0.9 and 0.96 run between persistent launches on the direct passes (the
+    components they leave on the component path); an insert of 24,000 keys
+    that ends below 0.9 from 0.5 stays in the queue, where components too
+    large for a warp go to the op's last unit."""
+    import flash_map as F
+
+    rng = np.random.default_rng(41)
+    specs = [((8, 8), 1 << 20, 0.5, [1 << 18]),         # large: external direct
+             ((32, 128), 1 << 16, 0.5, [24_000]),         # in queue, ends at 0.87
+             ((8, 8), 1 << 16, 0.6, [int((1 << 16) * 0.3), int((1 << 16) * 0.06)])]  # to 0.9, then 0.96
+    tables, queue = [], []
+    for (ks, vs), cap, load0, sizes in specs:
+        g, o = gpu_map(cap, ks, vs), OracleAdapter(cap, ks, vs)
+        k, v = _keys(rng, int(cap * load0), ks), _keys(rng, int(cap * load0), vs)
+        assert g.bulk_insert(k, v) == o.bulk_insert(k, v)
+        tables.append({"g": g, "o": o, "ks": ks, "vs": vs, "known": [k]})
+    for ti, ((ks, vs), cap, load0, sizes) in enumerate(specs):
+        t = tables[ti]
+        for n in sizes:
+            known = np.concatenate(t["known"])
+            queue.append((ti, F.batch.GET, known[rng.integers(0, len(known), 5000)], None))
+            k, v = _keys(rng, n, ks), _keys(rng, n, vs)
+            k[: n // 20] = known[rng.integers(0, len(known), n // 20)]  # updates
+            queue.append((ti, F.batch.INSERT, k, v))
+            t["known"].append(k)
+            known = np.concatenate(t["known"])
+            queue.append((ti, F.batch.GET, known[rng.integers(0, len(known), 5000)], None))
+            queue.append((ti, F.batch.REMOVE, known[rng.integers(0, len(known), 2000)], None))
+    g_res, g_out = run_batch(tables, queue, graph)
+    o_res, o_out = oracle_replay(tables, queue)
+    for i, ((ti, kind, k, v), gr, orr) in enumerate(zip(queue, g_res, o_res)):
+        assert gr == orr, f"op {i} kind {kind} n {len(k)}: gpu {gr} oracle {orr}"
+        if kind == F.batch.GET:
+            ov, of = g_out[i]
+            ev, ef = o_out[i]
+            assert np.array_equal(of.astype(bool), ef) and np.array_equal(ov, ev), f"op {i}"
+    for t in tables:
+        assert t["g"].len() == t["o"].len()
+        for x, y in zip(t["g"].snapshot(), t["o"].snapshot()):
+            assert np.array_equal(x, y)
