@@ -608,6 +608,7 @@ def batched_leg(torch, F, native, dev, steps, warmup, scale=1, clip=False):
 
     bops = [F.BatchOp(kind, tables[ti], n, k, v, o[0] if o else None, o[1] if o else None)
             for (ti, kind, n, k, v), o in zip(ops, outs[1])]
+    restore()  # the batch is planned from the tables' counts at creation: the start state
     batch = F.FlashMapBatch(bops)
     restore()
     batch.run(stream)  # eager run: records each wave's grid rounds for the capture

@@ -71,6 +71,20 @@ constexpr uint64_t OP_CHUNK = 1ull << 30;
 #ifndef FM_QUEUE_INS_LOAD
 #define FM_QUEUE_INS_LOAD 0.9
 #endif
+// Queue mode: a remove of at least FM_QUEUE_REM_OPS keys runs between
+// persistent launches too (the direct passes, then FM_QUEUE_REM_ROUNDS grid
+// rounds and the tail for what they leave).
+#ifndef FM_QUEUE_REM_OPS
+#define FM_QUEUE_REM_OPS (1u << 18)
+#endif
+// ... and a lookup of at least FM_QUEUE_GET_OPS keys runs as the plain lookup
+// kernel between persistent launches (its occupancy there is the tuned one).
+#ifndef FM_QUEUE_GET_OPS
+#define FM_QUEUE_GET_OPS (1u << 16)
+#endif
+#ifndef FM_QUEUE_REM_ROUNDS
+#define FM_QUEUE_REM_ROUNDS 4u
+#endif
 #ifndef FM_HANDOFF_LOAD
 #define FM_HANDOFF_LOAD 0.9  // load from which the insert tail hands stalled rounds back
 #endif
@@ -1249,14 +1263,17 @@ struct fm_batch {
     // segment and runs on the component path between launches.
     bool qmode = false;
     struct QStep {
-        bool external = false;  // an insert run between persistent launches
-        bool direct = false;    // external: the direct passes (else the component path)
+        bool external = false;  // an insert or remove run between persistent launches
+        bool remove = false;    // external: a remove
+        bool get = false;       // external: a lookup
+        bool direct = false;    // external insert: the direct passes (else the component path)
         double load = 0.0;      // external: the load it can reach (tuned tile width)
         uint32_t op = 0;        // external: the op
         fm::Shape shape = fm::SHAPE_GENERIC;
         uint32_t ph0 = 0, nph = 0;  // persistent launch: its phases (and done counters)
         uint64_t units = 0;
         uint32_t ext = 0;       // external: index of its GroupOp descriptor
+        uint32_t rounds = FM_QUEUE_REM_ROUNDS;  // external remove: grid rounds (eager runs record theirs)
     };
     std::vector<QStep> qsteps;
     std::vector<fm::QPhase> qphases;
@@ -1265,6 +1282,7 @@ struct fm_batch {
     uint32_t* d_done = nullptr;      // one counter per phase
     fm::QState* d_qstate = nullptr;  // one per step
     fm::QState* h_qstate = nullptr;
+    fm::QProf* d_prof = nullptr;     // per-phase timing (fm_batch_profile), one per phase
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     unsigned long long launches_per_run = 0;
@@ -1397,8 +1415,11 @@ int queue_fill(fm_batch* b) {
     return FM_OK;
 }
 
-// Queue mode: uploads, the steps in order on stream s, downloads.
-int queue_enqueue(fm_batch* b, cudaStream_t s) {
+// Queue mode: uploads, the steps in order on stream s, downloads.  adaptive
+// (eager runs): an external remove runs grid rounds two at a time until at
+// most TAIL_MAX ops are pending (a readback per pair) and records how many it
+// needed; otherwise (capture) the recorded count is used.
+int queue_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
     cudaError_t e = cudaMemcpyAsync(b->d_desc, b->h_desc, b->desc_bytes, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->d_len, b->h_len(), b->tables.size() * 8, cudaMemcpyHostToDevice, s);
@@ -1406,20 +1427,60 @@ int queue_enqueue(fm_batch* b, cudaStream_t s) {
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_status, 0, b->ops.size() * 4, s);
     if (e == cudaSuccess && !b->qphases.empty()) e = cudaMemsetAsync(b->d_done, 0, b->qphases.size() * 4, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_qstate, 0, b->qsteps.size() * sizeof(fm::QState), s);
+    if (e == cudaSuccess && b->d_prof) {
+        const size_t np = b->qphases.size();
+        e = cudaMemsetAsync(b->d_prof, 0, np * sizeof(fm::QProf), s);
+        if (e == cudaSuccess)  // first-start times to the largest value (atomicMin)
+            e = cudaMemset2DAsync(&b->d_prof[0].t0, sizeof(fm::QProf), 0xFF, sizeof(unsigned long long), np, s);
+    }
     if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "batch upload", e);
     const auto* dq = reinterpret_cast<const fm::QOp*>(b->d_desc + b->q_ops_off);
     const auto* dph = reinterpret_cast<const fm::QPhase*>(b->d_desc + b->q_ph_off);
     const auto* dg = reinterpret_cast<const fm::GroupOp*>(b->d_desc + b->q_ext_off);
     const auto* hg = reinterpret_cast<const fm::GroupOp*>(b->h_desc + b->q_ext_off);
     for (size_t si = 0; si < b->qsteps.size(); si++) {
-        const fm_batch::QStep& st = b->qsteps[si];
+        fm_batch::QStep& st = b->qsteps[si];
         if (!st.external) {
-            e = fm::launch_queue(st.shape, dph + st.ph0, st.nph, st.units, dq, b->d_done + st.ph0, b->d_qstate + si, s);
+            fm::QProf* pr = b->d_prof ? b->d_prof + st.ph0 : nullptr;
+            e = fm::launch_queue(st.shape, dph + st.ph0, st.nph, st.units, dq, b->d_done + st.ph0, b->d_qstate + si,
+                                 pr, s);
         } else {
             // precheck; the direct passes with the component path over what
             // they leave (pend[1]), or the component path over every op; then
             // the write-back (its rounds see no op left)
+            if (st.get) {
+                const fm::QOp& q = reinterpret_cast<const fm::QOp*>(b->h_desc + b->q_ops_off)[st.op];
+                e = fm::launch_get_cfg(q.t, st.shape, q.keys, q.n, q.out_vals, q.out_found,
+                                       fm::tuned_get_cfg(st.shape, st.load), s);
+                fm::count_launches(1);
+                if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch queue", e);
+                continue;
+            }
             const fm::GroupOp& h = hg[st.ext];
+            if (st.remove) {
+                // the direct remove, the rounds over what it leaves (pend[1]),
+                // the tail, the write-back
+                e = fm::launch_grp_rem(st.shape, dg + st.ext, 1, h.n, fm::GRP_BEGIN, 0, 0, s);
+                if (e == cudaSuccess) e = fm::launch_rem_direct_ctl(h.t, st.shape, h.keys, h.n, h.sc, h.ctl, s);
+                uint32_t r = 1;  // round r reads Ctl::npend[r & 1]
+                if (adaptive) {
+                    fm_table* tb = b->ops[st.op].table;
+                    while (e == cudaSuccess) {
+                        e = cudaMemcpyAsync(tb->h_ctl, h.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+                        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                        if (e != cudaSuccess || tb->h_ctl->npend[r & 1] <= fm::TAIL_MAX) break;
+                        e = fm::launch_grp_rem(st.shape, dg + st.ext, 1, h.n, fm::GRP_ROUNDS, r, 2, s);
+                        r += 2;
+                    }
+                    st.rounds = r - 1;
+                } else if (st.rounds) {
+                    e = fm::launch_grp_rem(st.shape, dg + st.ext, 1, h.n, fm::GRP_ROUNDS, 1, st.rounds, s);
+                    r += st.rounds;
+                }
+                if (e == cudaSuccess) e = fm::launch_grp_rem(st.shape, dg + st.ext, 1, h.n, fm::GRP_END, r, 0, s);
+                if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch queue", e);
+                continue;
+            }
             e = fm::launch_grp_ins(st.shape, dg + st.ext, 1, h.n, fm::GRP_BEGIN, 0, 0, s);
             if (e == cudaSuccess && st.direct) {
                 e = fm::launch_ins_direct_ctl(h.t, st.shape, h.keys, h.vals, h.n, h.sc, h.ctl, st.load, s);
@@ -1475,7 +1536,8 @@ void queue_plan(fm_batch* b) {
                 if (o.kind == FM_OP_GET) {
                     add(fm::QP_GET);
                 } else if (o.kind == FM_OP_INSERT) {
-                    for (uint32_t k : {fm::QP_BEGIN, fm::QP_IFIND, fm::QP_IFLOW, fm::QP_IEXEC, fm::QP_IWARP, fm::QP_END})
+                    for (uint32_t k : {fm::QP_BEGIN, fm::QP_IFIND, fm::QP_IFLOW, fm::QP_IEXEC, fm::QP_IWARP,
+                                       fm::QP_IBIG, fm::QP_END})
                         add(k);
                 } else {
                     for (uint32_t k : {fm::QP_BEGIN, fm::QP_RFIND, fm::QP_REXEC, fm::QP_END}) add(k);
@@ -1527,6 +1589,20 @@ void queue_plan(fm_batch* b) {
                 b->qsteps.push_back(st);
                 continue;
             }
+        }
+        if ((o.kind == FM_OP_REMOVE && o.n >= FM_QUEUE_REM_OPS) || (o.kind == FM_OP_GET && o.n >= FM_QUEUE_GET_OPS)) {
+            flush();
+            fm_batch::QStep st;
+            st.external = true;
+            st.remove = o.kind == FM_OP_REMOVE;
+            st.get = o.kind == FM_OP_GET;
+            st.load = std::min(est[ti], (double)b->tables[ti]->cap) / (double)b->tables[ti]->cap;
+            st.op = i;
+            st.shape = o.table->shape;
+            st.ext = (uint32_t)b->qext_ops.size();
+            b->qext_ops.push_back(i);
+            b->qsteps.push_back(st);
+            continue;
         }
         seg.push_back(i);
     }
@@ -1851,7 +1927,7 @@ int fm_batch_capture(fm_batch* b, void* stream) {
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "begin capture", e);
     const unsigned long long l0 = fm::launch_count();
-    rc = b->qmode ? queue_enqueue(b, s) : batch_enqueue(b, s, false);
+    rc = b->qmode ? queue_enqueue(b, s, false) : batch_enqueue(b, s, false);
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(s, &g);
     if (rc) {
@@ -1884,7 +1960,7 @@ int fm_batch_run(fm_batch* b, void* stream) {
         TimerScope ts(b->tables.size() == 1 ? b->tables[0] : nullptr);
         if (b->qmode) {
             rc = queue_fill(b);
-            if (!rc) rc = queue_enqueue(b, s);
+            if (!rc) rc = queue_enqueue(b, s, true);
         } else {
             rc = batch_fill(b);
             if (!rc) rc = batch_enqueue(b, s, true);
@@ -1933,8 +2009,60 @@ void fm_batch_destroy(fm_batch* b) {
         if (b->ev_join[l]) cudaEventDestroy(b->ev_join[l]);
     }
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->d_prof) cudaFree(b->d_prof);
     arena_give(b->arena);
     delete b;
+}
+
+int fm_batch_profile(fm_batch* b, int on) {
+    if (!b) return fail(FM_ERR_INVALID_ARG, "batch is NULL");
+    if (!b->qmode) return fail(FM_ERR_INVALID_ARG, "batch profile: the batch runs as waves, not as a queue");
+    if (b->pending) return fail(FM_ERR_INVALID_ARG, "batch still running: call fm_batch_wait first");
+    if (b->exec) return fail(FM_ERR_INVALID_ARG, "batch profile: set it before fm_batch_capture");
+    DeviceGuard dg(b->device);
+    if (!on) {
+        if (b->d_prof) cudaFree(b->d_prof);
+        b->d_prof = nullptr;
+        return FM_OK;
+    }
+    if (b->d_prof || b->qphases.empty()) return FM_OK;
+    const cudaError_t e = cudaMalloc((void**)&b->d_prof, b->qphases.size() * sizeof(fm::QProf));
+    if (e != cudaSuccess) {
+        b->d_prof = nullptr;
+        return cuda_fail(FM_ERR_GPU_ALLOC, "batch profile buffer", e);
+    }
+    return FM_OK;
+}
+
+int fm_batch_phase_times(fm_batch* b, uint64_t* rows, uint32_t max_rows, uint32_t* nrows) {
+    if (!b || !nrows) return fail(FM_ERR_INVALID_ARG, "batch or nrows is NULL");
+    if (b->pending) return fail(FM_ERR_INVALID_ARG, "batch still running: call fm_batch_wait first");
+    *nrows = 0;
+    if (!b->d_prof) return FM_OK;
+    DeviceGuard dg(b->device);
+    std::vector<fm::QProf> h(b->qphases.size());
+    const cudaError_t e = cudaMemcpy(h.data(), b->d_prof, h.size() * sizeof(fm::QProf), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(FM_ERR_TRANSFER, "batch profile read", e);
+    uint32_t r = 0;
+    for (size_t si = 0; si < b->qsteps.size(); si++) {
+        const fm_batch::QStep& st = b->qsteps[si];
+        if (st.external) continue;
+        for (uint32_t k = 0; k < st.nph && r < max_rows; k++, r++) {
+            const fm::QPhase& p = b->qphases[st.ph0 + k];
+            const fm::QProf& q = h[st.ph0 + k];
+            uint64_t* w = rows + (size_t)r * 8;
+            w[0] = si;
+            w[1] = p.kind;
+            w[2] = p.op;
+            w[3] = p.units;
+            w[4] = q.t0;
+            w[5] = q.t1;
+            w[6] = q.wait;
+            w[7] = q.busy;
+        }
+    }
+    *nrows = r;
+    return FM_OK;
 }
 
 }  // extern "C"

@@ -2439,6 +2439,101 @@ __device__ __noinline__ uint32_t dx_gather(const TableView& t, uint32_t j, uint3
     return g;
 }
 
+// Ops registered at the free slots the flow from unwrapped position a still
+// reaches, carrying `flow` ops past it (the flow pass's walk, reads only).
+__device__ __forceinline__ uint32_t dx_flow_rest(const TableView& t, uint64_t a, uint64_t budget, uint64_t flow) {
+    uint32_t rest = 0;
+    while (flow > 0) {
+        const uint64_t at = dx_next_free(t, a + 1, budget);
+        if (at == NONE64) break;
+        const uint32_t c = t.seg_cnt[at & t.mask] & DX_CNT;
+        rest += c;
+        flow = flow + c - 1;
+        a = at;
+    }
+    return rest;
+}
+
+// dx_gather for the persistent batch: a component of more than DX_GATHER ops
+// is gathered into a range of pend[1] reserved for it (Ctl::big_ops) and
+// listed in pend[0] (offset, count; Ctl::nbig) for the block pass (QP_IBIG)
+// instead of leaving its ops to a single block at the op's end.  Returns the
+// count gathered into s_ops in index order, or 0 for a listed component.
+__device__ __noinline__ uint32_t dx_gather_q(const TableView& t, uint32_t j, uint32_t n0, const OpScratch& sc,
+                                             Ctl* ctl, uint32_t* s_ops, const Tile<32>& tl) {
+    uint32_t g = 0;
+    if (tl.lane == 0) {
+        const uint64_t mask = t.mask;
+        uint64_t F = sc.op_slot[j];
+        uint64_t a = F, budget = mask;
+        uint64_t flow = 0;
+        uint32_t* big = nullptr;  // the reserved range, once the component outgrows s_ops
+        uint32_t room = 0;
+        for (;;) {
+            const uint32_t c = t.seg_cnt[F] & DX_CNT;
+            uint32_t x = t.seg_min[F];
+            for (uint32_t q = 0; q < c && x != IDLE; q++) {
+                if (x >= n0) {
+                    atomicOr(&ctl->err, ERR_SCRATCH);
+                    break;
+                }
+                if (g == (uint32_t)DX_GATHER && !big) {
+                    // the rest of this slot's list and of the slots the flow
+                    // reaches (registrations still in place)
+                    room = g + (c - q) + dx_flow_rest(t, a, budget, flow + c - 1);
+                    big = sc.pend[1] + atomicAdd(&ctl->big_ops, room);
+                    for (uint32_t i = 0; i < g; i++) big[i] = s_ops[i];
+                }
+                const uint32_t nx = sc.op_word[x];
+                sc.op_word[x] = IDLE;
+                if (!big) s_ops[g] = x;
+                else if (g < room) big[g] = x;
+                else atomicOr(&ctl->err, ERR_SCRATCH);  // more ops than registered: never expected
+                ++g;
+                x = nx;
+            }
+            if (c) {
+                t.seg_min[F] = IDLE;
+                t.seg_cnt[F] = 0;
+            }
+            flow = flow + c - 1;
+            if (flow == 0) break;
+            const uint64_t at = dx_next_free(t, a + 1, budget);
+            if (at == NONE64) break;  // the flow pass found no wrap: not reached
+            a = at;
+            F = at & mask;
+        }
+        if (big) {
+            const uint32_t k = atomicAdd(&ctl->nbig, 1u);
+            sc.pend[0][2 * k] = (uint32_t)(big - sc.pend[1]);
+            sc.pend[0][2 * k + 1] = min(g, room);
+            g = 0;
+        }
+    }
+    g = tl.shfl(g, 0);
+    tl.sync();
+    if (g == 0) return 0;
+    constexpr int PER = DX_GATHER / 32;
+    const uint32_t lane = tl.lane;
+    uint32_t v[PER], r[PER];
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+        v[u] = lane + 32 * u < g ? s_ops[lane + 32 * u] : 0u;
+        r[u] = 0;
+    }
+    for (uint32_t q = 0; q < g; q++) {
+        const uint32_t x = s_ops[q];
+#pragma unroll
+        for (int u = 0; u < PER; u++) r[u] += x < v[u] ? 1u : 0u;
+    }
+    tl.sync();
+#pragma unroll
+    for (int u = 0; u < PER; u++)
+        if (lane + 32 * u < g) s_ops[r[u]] = v[u];
+    tl.sync();
+    return g;
+}
+
 // The warp pass: a tile of T lanes per entry of the list the exec pass built
 // (T: 32, 16 or 8, chosen per record shape and load by the autotuner; a
 // narrower tile reads fewer slots per round trip but runs more entries at
@@ -2458,11 +2553,16 @@ __global__ void __launch_bounds__(RBLOCK, FM_P4_MIN_BLOCKS) k_dx_warp(TableView 
     const Tile<T> tl;
     const uint32_t ti = threadIdx.x / T;
     ExecAcc a;
-    // uniform trip count per warp: all tiles of a warp loop together
-    const uint32_t ntiles = gridDim.x * NT;
-    const uint32_t iters = (n + ntiles - 1) / ntiles;
-    for (uint32_t it = 0; it < iters; it++) {
-        const uint32_t i = blockIdx.x * NT + ti + it * ntiles;
+    // entries taken a warp's worth at a time from a counter (Ctl::nlong[1],
+    // zero at the start of the call): long entries do not hold up a static
+    // share of the list; all tiles of a warp loop together
+    constexpr uint32_t TPW = 32 / T;
+    for (;;) {
+        uint32_t i0 = 0;
+        if ((threadIdx.x & 31u) == 0) i0 = atomicAdd(&ctl->nlong[1], TPW);
+        i0 = __shfl_sync(0xFFFFFFFFu, i0, 0);
+        if (i0 >= n) break;
+        const uint32_t i = i0 + (threadIdx.x & 31u) / T;
         uint32_t g = 0;  // a lone op, or a component's ops in index order
         if (i < n) {
             const uint32_t item = sc.long_list[i];
@@ -2512,7 +2612,8 @@ constexpr uint32_t QSPREAD = 296;   // units a phase is cut into where it can be
 template <int KB>
 constexpr int QG_Q = 4;  // lookups per thread in lockstep
 constexpr uint32_t QI_UNIT = 512;   // largest find / flow / exec unit (ops)
-constexpr uint64_t QWAIT_NS = 2000000000ull;  // bound of one dependency wait
+constexpr uint64_t QWAIT_NS = 20000000000ull;  // bound of one dependency wait (20 s)
+constexpr uint32_t QBIG_MAX = 8192;           // largest component the block pass sorts in shared memory
 
 __device__ __forceinline__ uint64_t q_now() {
     uint64_t t;
@@ -2533,8 +2634,13 @@ struct QSmem {
             TileChain chain;
         } serial;
         uint32_t rgrp[QTHREADS / 32][RX_GMAX];
+        struct {
+            uint32_t list[QBIG_MAX];
+            P4Chain<32> chain;
+        } big;
     };
     uint32_t tmp[QTHREADS / 32];
+    uint32_t word;
 };
 static_assert(DX_THREADS == QTHREADS, "exec pass buffers");
 
@@ -2722,13 +2828,74 @@ __device__ __noinline__ void q_iwarp(const QOp& o, uint32_t c, uint32_t units, Q
         const uint32_t item = o.sc.long_list[i];
         uint32_t g = 1;
         if (item & DX_ROOT) {
-            g = dx_gather(o.t, item & ~DX_ROOT, n0, o.sc, o.ctl, sm.warp.ops[wi], tl);
+            g = dx_gather_q(o.t, item & ~DX_ROOT, n0, o.sc, o.ctl, sm.warp.ops[wi], tl);
         } else {
             if (tl.lane == 0) sm.warp.ops[wi][0] = item;
             tl.sync();
         }
         for (uint32_t q = 0; q < g; q++)
             dx_run_tile<KB, VB>(o.t, o.keys, o.vals, sm.warp.ops[wi][q], tl, sm.warp.chain[wi], a);
+    }
+    block_add_count(o.ctl, a.claimed, sm.tmp);
+    publish_rare(o.ctl, a.maxd, a.tomb, a.limit);
+}
+
+// Sorts a[0..n) (n <= QBIG_MAX) ascending in shared memory: bitonic network
+// over the next power of two, padded with 0xFFFFFFFF.  Block-uniform call.
+__device__ void block_sort_u32(uint32_t* a, uint32_t n) {
+    uint32_t P = 1;
+    while (P < n) P <<= 1;
+    for (uint32_t i = n + threadIdx.x; i < P; i += blockDim.x) a[i] = 0xFFFFFFFFu;
+    __syncthreads();
+    for (uint32_t k = 2; k <= P; k <<= 1) {
+        for (uint32_t d = k >> 1; d > 0; d >>= 1) {
+            for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+                const uint32_t m = i ^ d;
+                if (m > i) {
+                    const uint32_t x = a[i], y = a[m];
+                    if ((x > y) == ((i & k) == 0)) {
+                        a[i] = y;
+                        a[m] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// The block pass: the components the warp pass listed (dx_gather_q), taken
+// one at a time; each is sorted into index order in shared memory and run by
+// warp 0 op after op.  A component of more than QBIG_MAX ops is marked for the
+// op's end unit instead (op_flag 3, Ctl::serial[1]).
+template <int KB, int VB>
+__device__ __noinline__ void q_ibig(const QOp& o, QSmem& sm) {
+    const TableView& t = o.t;
+    ExecAcc a;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const uint32_t k = atomicAdd(&o.ctl->big_next, 1u);
+            sm.word = k < *(volatile uint32_t*)&o.ctl->nbig ? k : 0xFFFFFFFFu;
+        }
+        __syncthreads();
+        const uint32_t k = sm.word;
+        if (k == 0xFFFFFFFFu) break;
+        const uint32_t* src = o.sc.pend[1] + o.sc.pend[0][2 * k];
+        const uint32_t g = o.sc.pend[0][2 * k + 1];
+        if (g > QBIG_MAX) {
+            for (uint32_t i = threadIdx.x; i < g; i += blockDim.x) o.sc.op_flag[src[i]] = 3;
+            if (threadIdx.x == 0) o.ctl->serial[1] = 1u;
+            __syncthreads();
+            continue;
+        }
+        for (uint32_t i = threadIdx.x; i < g; i += blockDim.x) sm.big.list[i] = src[i];
+        __syncthreads();
+        block_sort_u32(sm.big.list, g);
+        if (threadIdx.x < 32) {
+            const Tile<32> tl;
+            for (uint32_t q = 0; q < g; q++) dx_run_tile<KB, VB>(t, o.keys, o.vals, sm.big.list[q], tl, sm.big.chain, a);
+        }
+        __syncthreads();
     }
     block_add_count(o.ctl, a.claimed, sm.tmp);
     publish_rare(o.ctl, a.maxd, a.tomb, a.limit);
@@ -2808,7 +2975,9 @@ __device__ __noinline__ void q_end(const QOp& o, QSmem& sm) {
     const bool serial = *(volatile uint32_t*)&o.ctl->serial[0] != 0;
     const uint32_t left = serial ? n0 : *(volatile uint32_t*)&o.ctl->npend[1];
     const uint32_t* list = serial ? nullptr : o.sc.pend[1];
-    if (left) {
+    // inserts: components the block pass left (already marked op_flag 3)
+    const bool marked = o.kind == 1 && !serial && *(volatile uint32_t*)&o.ctl->serial[1] != 0;
+    if (left || marked) {
         if (o.kind == 1) {
             ExecAcc a;
             serial_process<KB, VB>(o.t, o.keys, o.vals, list, left, n0, o.sc, a, sm.serial.buf, sm.serial.woff,
@@ -2819,22 +2988,19 @@ __device__ __noinline__ void q_end(const QOp& o, QSmem& sm) {
             if (a.tomb) o.ctl->tomb_claimed = 1u;
             if (a.limit) atomicOr(&o.ctl->err, ERR_WALK_LIMIT);
         } else {
-            // removes: mark, list in index order, probe one after another
+            // removes: mark, list in index order, then warp 0 runs them 32 at
+            // a time (parallel probes, commits in index order)
             for (uint32_t i = threadIdx.x; i < left; i += blockDim.x) o.sc.op_flag[list ? list[i] : i] = 3;
             __syncthreads();
             uint32_t removed = 0;
             for (uint32_t base = 0; base < n0; base += blockDim.x) {
                 const uint32_t j = base + threadIdx.x;
                 const bool take = j < n0 && o.sc.op_flag[j] == 3;
+                if (take) o.sc.op_flag[j] = 0;
                 const uint32_t cnt = block_compact(j, take, sm.serial.buf, sm.serial.woff);
-                if (threadIdx.x == 0) {
-                    for (uint32_t q = 0; q < cnt; q++) {
-                        const uint32_t jj = sm.serial.buf[q];
-                        o.sc.op_flag[jj] = 0;
-                        RegKey<KB> key;
-                        removed += rx_probe<KB>(o.t, key, home_of<KB>(o.t, o.keys, jj, key));
-                    }
-                }
+                if (threadIdx.x < 32)
+                    for (uint32_t q = 0; q < cnt; q += 32)
+                        removed += rx_chunk32<KB>(o.t, o.keys, sm.serial.buf + q, min(32u, cnt - q));
                 __syncthreads();
             }
             if (threadIdx.x == 0 && removed) atomicAdd(&o.ctl->count, (unsigned long long)removed);
@@ -2858,11 +3024,13 @@ __device__ __noinline__ void q_end(const QOp& o, QSmem& sm) {
 
 template <int KB, int VB>
 __global__ void __launch_bounds__(QTHREADS, 2) k_queue(const QPhase* __restrict__ ph, uint64_t total,
-                                                       const QOp* __restrict__ ops, uint32_t* done, QState* st) {
+                                                       const QOp* __restrict__ ops, uint32_t* done, QState* st,
+                                                       QProf* prof) {
     __shared__ QSmem sm;
     __shared__ unsigned long long s_u;
     __shared__ uint32_t s_pe;
     uint32_t cursor = 0;  // the phase of the last unit taken: units come in increasing order
+    unsigned long long t_run = 0;  // (thread 0, with prof) when the current unit started
     for (;;) {
         if (threadIdx.x == 0) {
             const unsigned long long u = atomicAdd(&st->next, 1ull);
@@ -2870,6 +3038,7 @@ __global__ void __launch_bounds__(QTHREADS, 2) k_queue(const QPhase* __restrict_
             if (u < total) {
                 while (ph[cursor].base + ph[cursor].units <= u) ++cursor;
                 s_pe = cursor;
+                const unsigned long long t_take = prof ? q_now() : 0ull;
                 const int32_t d = ph[cursor].dep;
                 // after one wait has run out the rest skip theirs, so a broken
                 // plan ends at once (reported to the host)
@@ -2884,6 +3053,11 @@ __global__ void __launch_bounds__(QTHREADS, 2) k_queue(const QPhase* __restrict_
                         }
                     }
                     __threadfence();
+                }
+                if (prof) {
+                    t_run = q_now();
+                    atomicMin(&prof[cursor].t0, t_run);
+                    atomicAdd(&prof[cursor].wait, t_run - t_take);
                 }
             }
         }
@@ -2902,11 +3076,19 @@ __global__ void __launch_bounds__(QTHREADS, 2) k_queue(const QPhase* __restrict_
             case QP_IWARP: q_iwarp<KB, VB>(o, c, p.units, sm); break;
             case QP_RFIND: q_rfind<KB>(o, c, p.per); break;
             case QP_REXEC: q_rexec<KB>(o, c, p.per, sm); break;
+            case QP_IBIG: q_ibig<KB, VB>(o, sm); break;
             default: q_end<KB, VB>(o, sm); break;
         }
         __threadfence();  // this unit's writes before its count
         __syncthreads();
-        if (threadIdx.x == 0) atomicAdd(&done[s_pe], 1u);
+        if (threadIdx.x == 0) {
+            if (prof) {
+                const unsigned long long t_end = q_now();
+                atomicMax(&prof[s_pe].t1, t_end);
+                atomicAdd(&prof[s_pe].busy, t_end - t_run);
+            }
+            atomicAdd(&done[s_pe], 1u);
+        }
     }
 }
 
@@ -3339,6 +3521,10 @@ uint32_t queue_units(uint32_t kind, uint32_t n) {
     switch (kind) {
         case QP_BEGIN:
         case QP_END: return 1;
+        case QP_IBIG: {  // blocks that take the listed components
+            const uint32_t u = n / 4096 + 1;
+            return u < 64 ? u : 64;
+        }
         case QP_IWARP: return (n + 63) / 64;  // 8 warps per unit: a warp per 8 ops the exec pass may list
         default: {
             const uint32_t per = queue_per(kind, n);
@@ -3348,7 +3534,7 @@ uint32_t queue_units(uint32_t kind, uint32_t n) {
 }
 
 cudaError_t launch_queue(Shape sh, const QPhase* ph, uint32_t nph, uint64_t total_units, const QOp* ops,
-                         uint32_t* done, QState* st, cudaStream_t s) {
+                         uint32_t* done, QState* st, QProf* prof, cudaStream_t s) {
     if (nph == 0 || total_units == 0) return cudaSuccess;
     (void)nph;
     auto go = [&](auto kernel) {
@@ -3360,7 +3546,7 @@ cudaError_t launch_queue(Shape sh, const QPhase* ph, uint32_t nph, uint64_t tota
         }
         const uint64_t want = (uint64_t)num_sms() * per_sm;
         const unsigned grid = (unsigned)(total_units < want ? total_units : want);
-        kernel<<<grid, QTHREADS, 0, s>>>(ph, total_units, ops, done, st);
+        kernel<<<grid, QTHREADS, 0, s>>>(ph, total_units, ops, done, st, prof);
     };
     switch (sh) {
         case SHAPE_8_8: go(k_queue<8, 8>); break;

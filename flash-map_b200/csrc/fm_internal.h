@@ -30,7 +30,9 @@ struct Ctl {
     uint32_t n0;             // grouped (batch) calls: the call's op count after the precheck
     uint32_t tail_handoff;   // insert tail: 1 + the round it left pending for the host (0: none)
     uint32_t rsum_on;        // remove: the chunk summaries (OpScratch::rsum) are built for this call
-    uint32_t pad_[3];
+    uint32_t nbig;           // batch queue inserts: components listed for the block pass (pend[0] pairs)
+    uint32_t big_next;       //   the next of them to take
+    uint32_t big_ops;        //   op indices they hold (pend[1])
     unsigned long long count;  // new keys (insert) / removed keys (remove), single-block kernels
     unsigned long long count_part[COUNT_PARTS][4];  // the same from grid kernels, [i][0] used
     // Persistent table facts (survive across calls, reset by clear):
@@ -136,12 +138,17 @@ cudaError_t launch_ins_comp(const TableView& t, Shape sh, const uint8_t* keys, c
                             uint32_t r, uint32_t npend, const OpScratch& sc, Ctl* ctl, cudaStream_t s);
 // A whole remove call of n0 ops without rounds: ops grouped by the first
 // EMPTY slot at or after their home, lone ops run at once, each group in
-// index order on one thread.  On return (stream-ordered) Ctl::serial[0] set
+// index order on one warp.  On return (stream-ordered) Ctl::serial[0] set
 // means nothing ran (an op found no EMPTY slot) and every op is left to the
-// rounds from round 0; otherwise Ctl::npend[1] ops (groups too large for one
-// thread) are left in pend[1] for the rounds from round 1.
+// rounds from round 0; otherwise Ctl::npend[1] ops (groups too large for a
+// warp) are left in pend[1] for the rounds from round 1.
 cudaError_t launch_rem_direct(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, const OpScratch& sc,
                               Ctl* ctl, cudaStream_t s);
+// The same with the op count read from Ctl::n0 (nmax bounds it and sizes the
+// grids) and no host step after it: a call that found no EMPTY slot lists
+// every op in pend[1], so the rounds from round 1 complete the call either way.
+cudaError_t launch_rem_direct_ctl(const TableView& t, Shape sh, const uint8_t* keys, uint32_t nmax,
+                                  const OpScratch& sc, Ctl* ctl, cudaStream_t s);
 cudaError_t launch_rem_rounds(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, uint32_t r0,
                               uint32_t nrounds, uint32_t grid_ops, const OpScratch& sc, Ctl* ctl, cudaStream_t s);
 cudaError_t launch_rem_tail(const TableView& t, Shape sh, const uint8_t* keys, uint32_t n0, uint32_t r,
@@ -237,6 +244,7 @@ enum QPhaseKind : uint32_t {
     QP_RFIND,    // direct remove: find, exec
     QP_REXEC,
     QP_END,      // leftovers in index order, result write-back
+    QP_IBIG,     // direct insert: components too large for a warp, a block each
 };
 struct QPhase {
     uint64_t base;
@@ -268,6 +276,12 @@ struct QState {
     uint32_t err;             // 1: a dependency wait ran out
     uint32_t pad_;
 };
+// Per-phase device timing of a persistent launch (globaltimer ns): first
+// unit start, last unit end, summed dependency waits and summed unit run
+// times.  Instrumentation, recorded only when the launch is given a buffer.
+struct QProf {
+    unsigned long long t0, t1, wait, busy;
+};
 // Items per unit and units of each phase kind for an op of n keys: small
 // ops get small units, so that one op's phase still spreads over the SMs.
 uint32_t queue_per(uint32_t kind, uint32_t n);
@@ -275,7 +289,7 @@ uint32_t queue_units(uint32_t kind, uint32_t n);
 // One persistent launch over phases [0, nph) of ops of one record shape;
 // `done` holds nph zeroed counters and `st` a zeroed QState.
 cudaError_t launch_queue(Shape sh, const QPhase* ph, uint32_t nph, uint64_t total_units, const QOp* ops,
-                         uint32_t* done, QState* st, cudaStream_t s);
+                         uint32_t* done, QState* st, QProf* prof, cudaStream_t s);
 
 cudaError_t launch_grp_ins(Shape sh, const GroupOp* ops, uint32_t nops, uint64_t sum_n, int phase, uint32_t r0,
                            uint32_t nrounds, cudaStream_t s);

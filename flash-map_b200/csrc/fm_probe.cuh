@@ -6,11 +6,6 @@
 
 namespace fm {
 
-// Ops of one group (a run between EMPTY slots) the direct remove runs on one
-// thread; larger groups go to the rounds (or, in a batch, to the op's last
-// unit).
-constexpr uint32_t RX_GATHER = 32;
-
 template <int KB>
 __device__ __forceinline__ uint64_t home_of(const TableView& t, const uint8_t* keys, uint32_t j, RegKey<KB>& key) {
     const uint32_t ksz = KB ? (uint32_t)KB : t.ksz;
@@ -268,6 +263,50 @@ template <int KB>
 __device__ __forceinline__ uint32_t rx_probe(const TableView& t, const RegKey<KB>& key, uint64_t h) {
     uint64_t stop;
     return rx_look<KB>(t, key, h, true, &stop) != NONE64 ? 1u : 0u;
+}
+
+// Up to 32 removes (the indices in ops[0..cnt), in index order) on one warp
+// with the sequential result: every lane probes its op on the table as it is
+// (no writes), then the warp commits the ops in index order.  An op whose
+// probe range [home, stop] (measured from its home, the whole table when its
+// probe went round it) holds a slot an earlier op of these tombstoned probes
+// again on the current table; any other op's probe is unchanged by them
+// (removes change nothing but those slots).  Returns the count removed (on
+// every lane).  Warp-uniform call; the table may have no EMPTY slot.
+template <int KB>
+__device__ __forceinline__ uint32_t rx_chunk32(const TableView& t, const uint8_t* keys, const uint32_t* ops,
+                                               uint32_t cnt) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t mask = t.mask;
+    RegKey<KB> key;
+    uint64_t h = 0, stop = NONE64, tgt = NONE64;
+    if (lane < cnt) {
+        h = home_of<KB>(t, keys, ops[lane], key);
+        tgt = rx_look<KB>(t, key, h, false, &stop);
+    }
+    const uint64_t span = stop == NONE64 ? mask : ((stop - h) & mask);  // probe range, from home
+    bool done_t = false;  // this lane's op tombstoned tgt
+    uint32_t removed = 0;
+    for (uint32_t i = 0; i < cnt; i++) {
+        const uint64_t hi = __shfl_sync(0xFFFFFFFFu, h, i);
+        const uint64_t si = __shfl_sync(0xFFFFFFFFu, span, i);
+        const bool hit_range = done_t && ((tgt - hi) & mask) <= si;
+        const bool conflict = __ballot_sync(0xFFFFFFFFu, lane < i && hit_range) != 0;
+        if (lane == i) {
+            if (conflict) {
+                uint64_t st2;
+                tgt = rx_look<KB>(t, key, h, true, &st2);
+            } else if (tgt != NONE64) {
+                t.flags[tgt] = ST_TOMB;
+            }
+            if (tgt != NONE64) {
+                done_t = true;
+                ++removed;
+            }
+        }
+        __syncwarp();
+    }
+    return __reduce_add_sync(0xFFFFFFFFu, removed);
 }
 
 // Ops of a group of removes (equal first EMPTY slot) a warp runs itself.

@@ -522,16 +522,18 @@ void rounds_shape(const TableView& t, const uint8_t* keys, uint32_t n0, uint32_t
 //        the ops at E, seg_min[E] heads a list linked through op_word, and
 //        the first op to arrive leads E (op_flag 1).
 //   exec (a thread per op)  an op alone at its E runs its probe at once; the
-//        leader of an E with c >= 2 ops gathers them from the list, orders
-//        them by index and runs their probes one after another.
+//        leader of an E with c >= 2 ops is listed for
+//   group (a warp per listed E)  gathers its ops from the list, orders them
+//        by index and runs them in chunks of 32 (rx_group).
 // A call where some op finds no EMPTY slot (its probe could go round the
 // table) leaves every op to the rounds (Ctl::serial[0]); a group of more than
-// RX_GATHER ops leaves its ops to them (pend[1], Ctl::npend[1]).  Every
-// registration and list word is idle again when the two kernels end.
+// RX_GMAX ops leaves its ops to them (pend[1], Ctl::npend[1]).  Every
+// registration and list word is idle again when the three kernels end.
 
 template <int KB>
-__global__ void __launch_bounds__(RBLOCK) k_rx_find(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
+__global__ void __launch_bounds__(RBLOCK) k_rx_find(TableView t, const uint8_t* __restrict__ keys, uint32_t n0_arg,
                                                     OpScratch sc, Ctl* ctl) {
+    const uint32_t n0 = n0_arg != CMP_N0_CTL ? n0_arg : *(volatile const uint32_t*)&ctl->n0;
     bool no_empty = false;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n0; j += gridDim.x * blockDim.x) {
         RegKey<KB> key;
@@ -552,10 +554,14 @@ __global__ void __launch_bounds__(RBLOCK) k_rx_find(TableView t, const uint8_t* 
 }
 
 template <int KB>
-__global__ void __launch_bounds__(RBLOCK) k_rx_exec(TableView t, const uint8_t* __restrict__ keys, uint32_t n0,
+__global__ void __launch_bounds__(RBLOCK) k_rx_exec(TableView t, const uint8_t* __restrict__ keys, uint32_t n0_arg,
                                                     OpScratch sc, Ctl* ctl) {
     __shared__ uint32_t s_tmp[RBLOCK / 32];
-    __shared__ uint32_t s_grp[RBLOCK / 32][RX_GMAX];
+    const uint32_t n0 = n0_arg != CMP_N0_CTL ? n0_arg : *(volatile const uint32_t*)&ctl->n0;
+    // with the count in the control block (a device-driven call) the ops of a
+    // call that found no EMPTY slot go to pend[1] for the rounds launched
+    // after this pass; otherwise the host runs every op from round 0
+    const bool to_pend = n0_arg == CMP_N0_CTL;
     const bool serial = *(volatile uint32_t*)&ctl->serial[0] != 0;
     uint32_t removed = 0;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -565,6 +571,7 @@ __global__ void __launch_bounds__(RBLOCK) k_rx_exec(TableView t, const uint8_t* 
         uint64_t E = NONE64;
         uint32_t c = 0;
         bool lead = false;
+        if (j < n0 && serial && to_pend) sc.pend[1][atomicAdd(&ctl->npend[1], 1u)] = j;
         if (j < n0) {
             E = sc.op_slot[j];
             if (E != NONE64) {
@@ -586,22 +593,41 @@ __global__ void __launch_bounds__(RBLOCK) k_rx_exec(TableView t, const uint8_t* 
                 }
             }
         }
-        // groups of two or more: one at a time on the whole warp
-        for (uint32_t lm = __ballot_sync(0xFFFFFFFFu, lead); lm; lm &= lm - 1) {
-            const int L = __ffs(lm) - 1;
-            const uint64_t EL = __shfl_sync(0xFFFFFFFFu, E, L);
-            const uint32_t cL = __shfl_sync(0xFFFFFFFFu, c, L);
-            const uint32_t r = rx_group<KB>(t, keys, n0, sc, ctl, EL, cL, s_grp[threadIdx.x >> 5]);
-            if ((threadIdx.x & 31u) == 0) removed += r;
-        }
+        // groups of two or more: their leaders to the group pass
+        append(sc.long_list, &ctl->nlong[0], j, lead);
+    }
+    block_add_count(ctl, removed, s_tmp);
+}
+
+// The group pass: a warp per group the exec pass listed, groups taken from a
+// counter (Ctl::nlong[1], zero at the start of the call) so that a warp that
+// drew a large group does not hold up a static share of the list.
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_rx_warp(TableView t, const uint8_t* __restrict__ keys, uint32_t n0_arg,
+                                                    OpScratch sc, Ctl* ctl) {
+    __shared__ uint32_t s_tmp[RBLOCK / 32];
+    __shared__ uint32_t s_grp[RBLOCK / 32][RX_GMAX];
+    const uint32_t n0 = n0_arg != CMP_N0_CTL ? n0_arg : *(volatile const uint32_t*)&ctl->n0;
+    const uint32_t n = *(volatile const uint32_t*)&ctl->nlong[0];
+    uint32_t removed = 0;
+    for (;;) {
+        uint32_t i = 0;
+        if ((threadIdx.x & 31u) == 0) i = atomicAdd(&ctl->nlong[1], 1u);
+        i = __shfl_sync(0xFFFFFFFFu, i, 0);
+        if (i >= n) break;
+        const uint32_t j = sc.long_list[i];
+        const uint64_t E = sc.op_slot[j];
+        const uint32_t c = t.seg_cnt[E];
+        const uint32_t r = rx_group<KB>(t, keys, n0, sc, ctl, E, c, s_grp[threadIdx.x >> 5]);
+        if ((threadIdx.x & 31u) == 0) removed += r;
     }
     block_add_count(ctl, removed, s_tmp);
 }
 
 template <int KB>
-void direct_shape(const TableView& t, const uint8_t* keys, uint32_t n0, const OpScratch& sc, Ctl* ctl,
+void direct_shape(const TableView& t, const uint8_t* keys, uint32_t n0, uint32_t nmax, const OpScratch& sc, Ctl* ctl,
                   cudaStream_t s) {
-    const unsigned g = grid_for(n0, 8);
+    const unsigned g = grid_for(nmax, 8);
     {
         KtScope kt(KC_REM_MARK, s);
         k_rx_find<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
@@ -609,8 +635,10 @@ void direct_shape(const TableView& t, const uint8_t* keys, uint32_t n0, const Op
     {
         KtScope kt(KC_REM_EXEC, s);
         k_rx_exec<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
+        // a warp per group, as many warps as can be resident
+        k_rx_warp<KB><<<grid_for((uint64_t)nmax * 32, 8), RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
     }
-    count_launches(2);
+    count_launches(3);
 }
 
 }  // namespace
@@ -646,11 +674,24 @@ cudaError_t launch_rem_direct(const TableView& t, Shape sh, const uint8_t* keys,
                               Ctl* ctl, cudaStream_t s) {
     switch (sh) {
         case SHAPE_8_8:
-        case SHAPE_8_32: direct_shape<8>(t, keys, n0, sc, ctl, s); break;
+        case SHAPE_8_32: direct_shape<8>(t, keys, n0, n0, sc, ctl, s); break;
         case SHAPE_32_128:
         case SHAPE_32_64:
-        case SHAPE_32_32: direct_shape<32>(t, keys, n0, sc, ctl, s); break;
-        default: direct_shape<0>(t, keys, n0, sc, ctl, s); break;
+        case SHAPE_32_32: direct_shape<32>(t, keys, n0, n0, sc, ctl, s); break;
+        default: direct_shape<0>(t, keys, n0, n0, sc, ctl, s); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rem_direct_ctl(const TableView& t, Shape sh, const uint8_t* keys, uint32_t nmax,
+                                  const OpScratch& sc, Ctl* ctl, cudaStream_t s) {
+    switch (sh) {
+        case SHAPE_8_8:
+        case SHAPE_8_32: direct_shape<8>(t, keys, CMP_N0_CTL, nmax, sc, ctl, s); break;
+        case SHAPE_32_128:
+        case SHAPE_32_64:
+        case SHAPE_32_32: direct_shape<32>(t, keys, CMP_N0_CTL, nmax, sc, ctl, s); break;
+        default: direct_shape<0>(t, keys, CMP_N0_CTL, nmax, sc, ctl, s); break;
     }
     return cudaGetLastError();
 }

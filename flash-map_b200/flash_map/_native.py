@@ -25,7 +25,7 @@ EXPORTS = (
     "fm_bulk_insert_device_noalloc", "fm_kernel_timing", "fm_kernel_times", "fm_kernel_times_reset",
     "fm_kernel_class_name", "fm_batch_create", "fm_batch_capture", "fm_batch_run", "fm_batch_wait",
     "fm_batch_waves", "fm_batch_destroy", "fm_autotune", "fm_tuned_get_config", "fm_copy",
-    "fm_inject_fault",
+    "fm_inject_fault", "fm_batch_profile", "fm_batch_phase_times",
 )
 
 
@@ -112,6 +112,10 @@ def _declare(L) -> None:
     L.fm_batch_waves.argtypes = [vp]
     L.fm_batch_destroy.restype = None
     L.fm_batch_destroy.argtypes = [vp]
+    L.fm_batch_profile.restype = i32
+    L.fm_batch_profile.argtypes = [vp, i32]
+    L.fm_batch_phase_times.restype = i32
+    L.fm_batch_phase_times.argtypes = [vp, C.POINTER(C.c_uint64), u32, C.POINTER(u32)]
     L.fm_copy.restype = i32
     L.fm_copy.argtypes = [vp, vp, vp]
     L.fm_autotune.restype = i32

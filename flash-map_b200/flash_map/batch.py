@@ -90,6 +90,34 @@ class FlashMapBatch:
             raise_for_status(rc, _native.last_error(), 0, 0)
         return [(int(a.result), int(a.status)) for a in self._arr]
 
+    PHASE_KINDS = ("get", "begin", "ins_find", "ins_flow", "ins_exec", "ins_warp", "rem_find", "rem_exec", "end",
+                   "ins_big")
+
+    def profile(self, on: bool = True) -> None:
+        """Record per-phase device times of the persistent launches (queue
+        mode only; set before capture)."""
+        rc = self._L.fm_batch_profile(self._h, 1 if on else 0)
+        if rc:
+            raise_for_status(rc, _native.last_error(), 0, 0)
+
+    def phase_times(self) -> List[dict]:
+        """Per phase of the last run (after wait): step, kind, op, units and
+        device times in ns (start of the first unit, end of the last, summed
+        dependency waits, summed unit run times)."""
+        cap = 1 << 16
+        rows = (C.c_uint64 * (8 * cap))()
+        n = C.c_uint32(0)
+        rc = self._L.fm_batch_phase_times(self._h, rows, cap, C.byref(n))
+        if rc:
+            raise_for_status(rc, _native.last_error(), 0, 0)
+        out = []
+        for r in range(n.value):
+            w = rows[8 * r: 8 * r + 8]
+            out.append({"step": int(w[0]), "kind": self.PHASE_KINDS[int(w[1])], "op": int(w[2]),
+                        "units": int(w[3]), "t0": int(w[4]), "t1": int(w[5]), "wait": int(w[6]),
+                        "busy": int(w[7])})
+        return out
+
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
             self._L.fm_batch_destroy(self._h)

@@ -223,6 +223,16 @@ int fm_batch_capture(fm_batch* b, void* stream);
 int fm_batch_run(fm_batch* b, void* stream);
 int fm_batch_wait(fm_batch* b, fm_op* ops);
 uint32_t fm_batch_waves(const fm_batch* b);
+/* Instrumentation (no counterpart in the reference).  fm_batch_profile(b, 1)
+ * before fm_batch_capture (or for eager runs) makes the persistent launches
+ * of a queue-mode batch record, per phase, device times (globaltimer ns);
+ * after fm_batch_wait, fm_batch_phase_times writes up to max_rows rows of 8
+ * words: step, phase kind (0 get, 1 begin, 2-5 insert find / flow / exec /
+ * warp, 6-7 remove find / exec, 8 end, 9 insert block pass), op index, units, first unit start,
+ * last unit end, summed dependency waits, summed unit run times.  A wave-mode
+ * batch refuses profiling (FM_ERR_INVALID_ARG). */
+int fm_batch_profile(fm_batch* b, int on);
+int fm_batch_phase_times(fm_batch* b, uint64_t* rows, uint32_t max_rows, uint32_t* nrows);
 void fm_batch_destroy(fm_batch* b);
 
 /* Device-side copy of a whole table (no counterpart in gpu.rs): dst takes

@@ -345,3 +345,59 @@ def test_batch_large_and_high_load_inserts(graph):
         assert t["g"].len() == t["o"].len()
         for x, y in zip(t["g"].snapshot(), t["o"].snapshot()):
             assert np.array_equal(x, y)
+
+
+def _clustered(cap, n, first_home, span, ks, salt=0):
+    """n distinct keys whose identity-hash homes lie in [first_home,
+    first_home + span): one run of n entries, one insert component."""
+    homes = first_home + (np.arange(n, dtype=np.uint64) % np.uint64(span))
+    x = (np.arange(n, dtype=np.uint64) + np.uint64(1 + salt)) * np.uint64(cap) + homes
+    out = np.zeros((n, ks), np.uint8)
+    out[:, :8] = x.view(np.uint8).reshape(n, 8)
+    return out
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batch_queue_fallbacks(graph):
+    """The queue's slow paths against the oracle: an insert whose component
+    (10,000 ops homed in 100 slots) is too large for the block pass and runs
+    on the op's end unit; a remove of 3,000 keys of that cluster (one group
+    between EMPTY slots, too large for a warp) and removes on a table with no
+    EMPTY slot at all, both on the end unit's ordered 32-op chunks; gets after
+    each."""
+    import flash_map as F
+
+    rng = np.random.default_rng(43)
+    tables = []
+    ca, cb = 1 << 14, 1 << 12
+    ga, oa = gpu_map(ca, 8, 8), OracleAdapter(ca, 8, 8)
+    k0 = _keys(rng, ca // 4, 8)
+    assert ga.bulk_insert(k0, k0) == oa.bulk_insert(k0, k0)
+    tables.append({"g": ga, "o": oa, "ks": 8, "vs": 8, "known": [k0]})
+    gb, ob = gpu_map(cb, 32, 128), OracleAdapter(cb, 32, 128)
+    kb, vb = _keys(rng, cb, 32), _keys(rng, cb, 128)
+    assert gb.bulk_insert(kb, vb) == ob.bulk_insert(kb, vb) == cb  # full: no EMPTY slot
+    rm0 = kb[rng.choice(cb, 100, replace=False)]
+    assert gb.bulk_remove(rm0) == ob.bulk_remove(rm0) == 100  # tombstones, still no EMPTY slot
+    tables.append({"g": gb, "o": ob, "ks": 32, "vs": 128, "known": [kb]})
+    kc = _clustered(ca, 10_000, 1000, 100, 8)
+    kc = kc[rng.permutation(len(kc))]
+    vc = _keys(rng, len(kc), 8)
+    queue = [(0, F.batch.INSERT, kc, vc),
+             (0, F.batch.GET, np.concatenate([kc[:3000], k0[:1000]]), None),
+             (0, F.batch.REMOVE, kc[rng.choice(len(kc), 3000, replace=False)], None),
+             (0, F.batch.GET, kc, None),
+             (1, F.batch.REMOVE, np.concatenate([kb[rng.choice(cb, 700, replace=False)], _keys(rng, 300, 32)]), None),
+             (1, F.batch.GET, kb, None)]
+    g_res, g_out = run_batch(tables, queue, graph)
+    o_res, o_out = oracle_replay(tables, queue)
+    for i, ((ti, kind, k, v), gr, orr) in enumerate(zip(queue, g_res, o_res)):
+        assert gr == orr, f"op {i} kind {kind} n {len(k)}: gpu {gr} oracle {orr}"
+        if kind == F.batch.GET:
+            ov, of = g_out[i]
+            ev, ef = o_out[i]
+            assert np.array_equal(of.astype(bool), ef) and np.array_equal(ov, ev), f"op {i}"
+    for t in tables:
+        assert t["g"].len() == t["o"].len()
+        for x, y in zip(t["g"].snapshot(), t["o"].snapshot()):
+            assert np.array_equal(x, y)
