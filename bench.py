@@ -317,7 +317,7 @@ def max_over_ranks(value, dist, device):
 
 
 INSERT_KERNELS = ("ins_find", "ins_flow", "ins_exec", "ins_warp", "k_ins_tail", "k_ins_serial")
-REMOVE_KERNELS = ("k_rem_p1", "k_rem_p2", "k_rem_p3", "k_rem_tail")
+REMOVE_KERNELS = ("k_rem_p1", "k_rem_p2", "k_rem_p3", "k_rem_tail", "rem_group")
 
 # DRAM traffic (ncu dram__bytes_read.sum + dram__bytes_write.sum) per op of
 # each kernel set, from captures of the same kernels on a 2^22-slot table at

@@ -950,6 +950,8 @@ int fm_kernel_timing(fm_table* t, int on) {
     return FM_OK;
 }
 
+static_assert(FM_KERNEL_CLASSES == (unsigned)fm::KC_N, "kernel classes of the header and the library");
+
 int fm_kernel_times(fm_table* t, double* total_ms, uint64_t* launches, uint32_t n) {
     if (!t) return fail(FM_ERR_INVALID_ARG, "table is NULL");
     DeviceGuard dg(t->device);
@@ -977,7 +979,8 @@ const char* fm_kernel_class_name(uint32_t cls) {
     // insert classes: the direct kernels (k_dx_*) or the round kernels (k_ins_p1..p4)
     static const char* names[fm::KC_N] = {"k_get",      "ins_find",   "ins_flow",     "ins_exec",
                                           "ins_warp",   "k_ins_tail", "k_ins_serial", "k_rem_p1",
-                                          "k_rem_p2",   "k_rem_p3",   "k_rem_tail",   "k_count"};
+                                          "k_rem_p2",   "k_rem_p3",   "k_rem_tail",   "k_count",
+                                          "rem_group"};
     return cls < (uint32_t)fm::KC_N ? names[cls] : nullptr;
 }
 

@@ -311,11 +311,12 @@ enum KernelClass : int {
     KC_INS_LONG,    // k_dx_warp / k_ins_p4: warp-per-op execution (long walks, components)
     KC_INS_TAIL,    // k_ins_tail: remaining rounds in one block
     KC_INS_SERIAL,  // k_ins_serial
-    KC_REM_MARK,    // k_rem_p1
+    KC_REM_MARK,    // k_rx_find / k_rem_p1
     KC_REM_CHECK,   // k_rem_p2
-    KC_REM_EXEC,    // k_rem_p3
+    KC_REM_EXEC,    // k_rx_exec / k_rem_p3
     KC_REM_TAIL,    // k_rem_tail
     KC_COUNT_OCC,   // k_count
+    KC_REM_GROUP,   // k_rx_warp: a warp per group of removes
     KC_N
 };
 void kt_mark(int cls, bool begin, cudaStream_t s);

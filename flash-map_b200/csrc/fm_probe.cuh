@@ -312,6 +312,10 @@ __device__ __forceinline__ uint32_t rx_chunk32(const TableView& t, const uint8_t
 // Ops of a group of removes (equal first EMPTY slot) a warp runs itself.
 constexpr uint32_t RX_GMAX = 256;
 
+template <int KB>
+__device__ __noinline__ uint32_t rx_group_run(const TableView& t, const uint8_t* keys, uint64_t E, uint32_t g,
+                                              uint32_t* s_grp);
+
 // The removes of the group at EMPTY slot E (c ops listed from seg_min[E]
 // through the per-op words) on one warp: lane 0 gathers the list into
 // s_grp (registrations set idle), the warp sorts it by index, then, 32 at a
@@ -327,7 +331,6 @@ template <int KB>
 __device__ __noinline__ uint32_t rx_group(const TableView& t, const uint8_t* keys, uint32_t n0, const OpScratch& sc,
                                           Ctl* ctl, uint64_t E, uint32_t c, uint32_t* s_grp) {
     const uint32_t lane = threadIdx.x & 31u;
-    const uint64_t mask = t.mask;
     uint32_t g = 0;
     if (lane == 0) {
         uint32_t x = t.seg_min[E];
@@ -347,6 +350,17 @@ __device__ __noinline__ uint32_t rx_group(const TableView& t, const uint8_t* key
     }
     g = __shfl_sync(0xFFFFFFFFu, g, 0);
     __syncwarp();
+    return rx_group_run<KB>(t, keys, E, g, s_grp);
+}
+
+// The g ops of a group (indices in s_grp[0..g), any order, g <= RX_GMAX) at
+// EMPTY slot E, sorted into index order by the warp and run in chunks of 32
+// as rx_group describes.  Returns the count removed (on every lane).
+template <int KB>
+__device__ __noinline__ uint32_t rx_group_run(const TableView& t, const uint8_t* keys, uint64_t E, uint32_t g,
+                                              uint32_t* s_grp) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t mask = t.mask;
     if (g == 0) return 0;
     // index order: the rank of each entry among the group
     uint32_t v[RX_GMAX / 32], r[RX_GMAX / 32];

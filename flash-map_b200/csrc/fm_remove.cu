@@ -518,17 +518,20 @@ void rounds_shape(const TableView& t, const uint8_t* keys, uint32_t n0, uint32_t
 // whole word TOMBSTONE).  Removes make no EMPTY slot, so E stays the same for
 // the whole call, and ops with different E read and write disjoint slots.
 // So the ops are grouped by E, without rounds:
-//   find (a thread per op)  E, then the op joins E's list: seg_cnt[E] counts
-//        the ops at E, seg_min[E] heads a list linked through op_word, and
-//        the first op to arrive leads E (op_flag 1).
+//   find (a thread per op)  E, and the op's place in E's group
+//        (atomicAdd on seg_cnt[E], kept in op_word); place 0 leads E.
 //   exec (a thread per op)  an op alone at its E runs its probe at once; the
-//        leader of an E with c >= 2 ops is listed for
-//   group (a warp per listed E)  gathers its ops from the list, orders them
-//        by index and runs them in chunks of 32 (rx_group).
+//        leader of an E with c >= 2 ops takes a segment of c words of pend[0]
+//        (one atomic per warp on Ctl::big_ops), keeps its offset in seg_min[E]
+//        and lists E for the group pass.
+//   place (a thread per op)  each op of a group writes its index at its place
+//        in its group's segment.
+//   group (a warp per listed E)  reads the segment, orders it by index and
+//        runs the ops in chunks of 32 (rx_group_run).
 // A call where some op finds no EMPTY slot (its probe could go round the
 // table) leaves every op to the rounds (Ctl::serial[0]); a group of more than
 // RX_GMAX ops leaves its ops to them (pend[1], Ctl::npend[1]).  Every
-// registration and list word is idle again when the three kernels end.
+// registration and list word is idle again when the four kernels end.
 
 template <int KB>
 __global__ void __launch_bounds__(RBLOCK) k_rx_find(TableView t, const uint8_t* __restrict__ keys, uint32_t n0_arg,
@@ -540,14 +543,14 @@ __global__ void __launch_bounds__(RBLOCK) k_rx_find(TableView t, const uint8_t* 
         const uint64_t E = rx_first_empty(t, home_of<KB>(t, keys, j, key));
         sc.op_slot[j] = E;
         uint8_t lead = 0;
-        uint32_t next = IDLE;
+        uint32_t place = IDLE;
         if (E == NONE64) {
             no_empty = true;
         } else {
-            lead = atomicAdd(&t.seg_cnt[E], 1u) == 0u ? 1 : 0;
-            next = atomicExch(&t.seg_min[E], j);
+            place = atomicAdd(&t.seg_cnt[E], 1u);
+            lead = place == 0u ? 1 : 0;
         }
-        sc.op_word[j] = next;
+        sc.op_word[j] = place;
         sc.op_flag[j] = lead;
     }
     if (no_empty) ctl->serial[0] = 1u;
@@ -563,40 +566,62 @@ __global__ void __launch_bounds__(RBLOCK) k_rx_exec(TableView t, const uint8_t* 
     // after this pass; otherwise the host runs every op from round 0
     const bool to_pend = n0_arg == CMP_N0_CTL;
     const bool serial = *(volatile uint32_t*)&ctl->serial[0] != 0;
+    const uint32_t lane = threadIdx.x & 31u;
     uint32_t removed = 0;
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t iters = (n0 + stride - 1) / stride;
     for (uint32_t it = 0; it < iters; it++) {  // warp-uniform trip count
         const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x + it * stride;
         uint64_t E = NONE64;
-        uint32_t c = 0;
-        bool lead = false;
+        uint32_t cg = 0;  // the size of the group this op leads (0: none)
         if (j < n0 && serial && to_pend) sc.pend[1][atomicAdd(&ctl->npend[1], 1u)] = j;
         if (j < n0) {
             E = sc.op_slot[j];
             if (E != NONE64) {
                 if (serial) {  // registrations back to idle; the rounds run every op
-                    t.seg_min[E] = IDLE;
                     t.seg_cnt[E] = 0;
                     sc.op_word[j] = IDLE;
-                } else if (sc.op_flag[j]) {  // the leader of E runs its group
-                    c = t.seg_cnt[E];
+                } else {
+                    const uint32_t c = t.seg_cnt[E];
                     if (c == 1) {
                         RegKey<KB> key;
                         removed += rx_probe<KB>(t, key, home_of<KB>(t, keys, j, key));
-                        t.seg_min[E] = IDLE;
                         t.seg_cnt[E] = 0;
                         sc.op_word[j] = IDLE;
-                    } else {
-                        lead = true;
+                    } else if (sc.op_flag[j]) {
+                        cg = c;
                     }
                 }
             }
         }
-        // groups of two or more: their leaders to the group pass
-        append(sc.long_list, &ctl->nlong[0], j, lead);
+        // segments for the groups this warp leads: one atomic per warp
+        uint32_t incl = cg;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if ((int)lane >= o) incl += v;
+        }
+        const uint32_t tot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        uint32_t wbase = 0;
+        if (lane == 0 && tot) wbase = atomicAdd(&ctl->big_ops, tot);
+        wbase = __shfl_sync(0xFFFFFFFFu, wbase, 0);
+        if (cg) t.seg_min[E] = wbase + incl - cg;
+        append(sc.long_list, &ctl->nlong[0], j, cg != 0);
     }
     block_add_count(ctl, removed, s_tmp);
+}
+
+__global__ void __launch_bounds__(RBLOCK) k_rx_place(TableView t, uint32_t n0_arg, OpScratch sc, Ctl* ctl) {
+    const uint32_t n0 = n0_arg != CMP_N0_CTL ? n0_arg : *(volatile const uint32_t*)&ctl->n0;
+    if (*(volatile uint32_t*)&ctl->serial[0]) return;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n0; j += gridDim.x * blockDim.x) {
+        const uint32_t place = sc.op_word[j];
+        if (place == IDLE) continue;  // lone (already run) or no EMPTY slot
+        const uint32_t at = t.seg_min[sc.op_slot[j]] + place;
+        if (at < n0) sc.pend[0][at] = j;  // segments hold n0 words at most
+        else atomicOr(&ctl->err, ERR_SCRATCH);
+        sc.op_word[j] = IDLE;
+    }
 }
 
 // The group pass: a warp per group the exec pass listed, groups taken from a
@@ -609,17 +634,41 @@ __global__ void __launch_bounds__(RBLOCK) k_rx_warp(TableView t, const uint8_t* 
     __shared__ uint32_t s_grp[RBLOCK / 32][RX_GMAX];
     const uint32_t n0 = n0_arg != CMP_N0_CTL ? n0_arg : *(volatile const uint32_t*)&ctl->n0;
     const uint32_t n = *(volatile const uint32_t*)&ctl->nlong[0];
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t* grp = s_grp[threadIdx.x >> 5];
     uint32_t removed = 0;
     for (;;) {
         uint32_t i = 0;
-        if ((threadIdx.x & 31u) == 0) i = atomicAdd(&ctl->nlong[1], 1u);
+        if (lane == 0) i = atomicAdd(&ctl->nlong[1], 1u);
         i = __shfl_sync(0xFFFFFFFFu, i, 0);
         if (i >= n) break;
         const uint32_t j = sc.long_list[i];
         const uint64_t E = sc.op_slot[j];
         const uint32_t c = t.seg_cnt[E];
-        const uint32_t r = rx_group<KB>(t, keys, n0, sc, ctl, E, c, s_grp[threadIdx.x >> 5]);
-        if ((threadIdx.x & 31u) == 0) removed += r;
+        const uint32_t* seg = sc.pend[0] + t.seg_min[E];
+        bool bad = false;
+        for (uint32_t q = lane; q < c; q += 32) {
+            const uint32_t x = seg[q];
+            bad |= x >= n0 || sc.op_slot[x] != E;  // a place this call did not fill
+        }
+        bad = __any_sync(0xFFFFFFFFu, bad);
+        if (bad && lane == 0) atomicOr(&ctl->err, ERR_SCRATCH);  // the group is not run
+        const bool over = !bad && c > RX_GMAX;  // too many for a warp: to the rounds
+        uint32_t at = 0;
+        if (over && lane == 0) at = atomicAdd(&ctl->npend[1], c);
+        at = __shfl_sync(0xFFFFFFFFu, at, 0);
+        if (!bad)
+            for (uint32_t q = lane; q < c; q += 32) {
+                if (over) sc.pend[1][at + q] = seg[q];
+                else grp[q] = seg[q];
+            }
+        __syncwarp();
+        if (lane == 0) {
+            t.seg_min[E] = IDLE;
+            t.seg_cnt[E] = 0;
+        }
+        const uint32_t r = rx_group_run<KB>(t, keys, E, (bad || over) ? 0u : c, grp);
+        if (lane == 0) removed += r;
     }
     block_add_count(ctl, removed, s_tmp);
 }
@@ -635,10 +684,13 @@ void direct_shape(const TableView& t, const uint8_t* keys, uint32_t n0, uint32_t
     {
         KtScope kt(KC_REM_EXEC, s);
         k_rx_exec<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
-        // a warp per group, as many warps as can be resident
+    }
+    {
+        KtScope kt(KC_REM_GROUP, s);  // a warp per group, as many warps as can be resident
+        k_rx_place<<<g, RBLOCK, 0, s>>>(t, n0, sc, ctl);
         k_rx_warp<KB><<<grid_for((uint64_t)nmax * 32, 8), RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
     }
-    count_launches(3);
+    count_launches(4);
 }
 
 }  // namespace

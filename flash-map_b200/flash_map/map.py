@@ -253,7 +253,7 @@ class FlashMap:
     def kernel_times(self) -> dict:
         """{kernel class: (total device ms, launches)} since the last reset;
         waits for the recorded launches."""
-        n = 12
+        n = 13
         ms = (C.c_double * n)()
         cnt = (C.c_uint64 * n)()
         self._check(self._L.fm_kernel_times(self._h, ms, cnt, n))

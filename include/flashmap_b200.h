@@ -172,7 +172,7 @@ int fm_inject_fault(uint32_t site, uint32_t after);
  * class (index < FM_KERNEL_CLASSES, named by fm_kernel_class_name), the summed
  * device milliseconds and the launch count since the last reset.  Off by
  * default: no events are recorded then. */
-#define FM_KERNEL_CLASSES 12u
+#define FM_KERNEL_CLASSES 13u
 int fm_kernel_timing(fm_table* t, int on);
 int fm_kernel_times(fm_table* t, double* total_ms, uint64_t* launches, uint32_t n);
 int fm_kernel_times_reset(fm_table* t);
