@@ -309,8 +309,10 @@ __device__ __forceinline__ uint32_t rx_chunk32(const TableView& t, const uint8_t
     return __reduce_add_sync(0xFFFFFFFFu, removed);
 }
 
-// Ops of a group of removes (equal first EMPTY slot) a warp runs itself.
+// Ops of a group of removes (equal first EMPTY slot) a warp runs itself; up
+// to RX_THREAD of them one thread runs.
 constexpr uint32_t RX_GMAX = 256;
+constexpr uint32_t RX_THREAD = 8;
 
 template <int KB>
 __device__ __noinline__ uint32_t rx_group_run(const TableView& t, const uint8_t* keys, uint64_t E, uint32_t g,

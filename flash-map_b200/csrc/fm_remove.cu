@@ -526,8 +526,9 @@ void rounds_shape(const TableView& t, const uint8_t* keys, uint32_t n0, uint32_t
 //        and lists E for the group pass.
 //   place (a thread per op)  each op of a group writes its index at its place
 //        in its group's segment.
-//   group (a warp per listed E)  reads the segment, orders it by index and
-//        runs the ops in chunks of 32 (rx_group_run).
+//   group (a lane per listed E)  reads the segment, orders it by index and
+//        runs the ops one after another (up to RX_THREAD ops) or on the whole
+//        warp in chunks of 32 (rx_group_run).
 // A call where some op finds no EMPTY slot (its probe could go round the
 // table) leaves every op to the rounds (Ctl::serial[0]); a group of more than
 // RX_GMAX ops leaves its ops to them (pend[1], Ctl::npend[1]).  Every
@@ -624,9 +625,11 @@ __global__ void __launch_bounds__(RBLOCK) k_rx_place(TableView t, uint32_t n0_ar
     }
 }
 
-// The group pass: a warp per group the exec pass listed, groups taken from a
-// counter (Ctl::nlong[1], zero at the start of the call) so that a warp that
-// drew a large group does not hold up a static share of the list.
+// The group pass: groups taken 32 at a time by a warp from a counter
+// (Ctl::nlong[1], zero at the start of the call), one per lane.  A lane runs a
+// group of at most RX_THREAD ops itself, one op after another in index order
+// (each probe sees the ones before it); larger groups then run on the whole
+// warp, one after another (rx_group_run), or go to the rounds above RX_GMAX.
 template <int KB>
 __global__ void __launch_bounds__(RBLOCK) k_rx_warp(TableView t, const uint8_t* __restrict__ keys, uint32_t n0_arg,
                                                     OpScratch sc, Ctl* ctl) {
@@ -636,39 +639,66 @@ __global__ void __launch_bounds__(RBLOCK) k_rx_warp(TableView t, const uint8_t* 
     const uint32_t n = *(volatile const uint32_t*)&ctl->nlong[0];
     const uint32_t lane = threadIdx.x & 31u;
     uint32_t* grp = s_grp[threadIdx.x >> 5];
-    uint32_t removed = 0;
+    uint32_t removed = 0;  // this lane's
     for (;;) {
-        uint32_t i = 0;
-        if (lane == 0) i = atomicAdd(&ctl->nlong[1], 1u);
-        i = __shfl_sync(0xFFFFFFFFu, i, 0);
-        if (i >= n) break;
-        const uint32_t j = sc.long_list[i];
-        const uint64_t E = sc.op_slot[j];
-        const uint32_t c = t.seg_cnt[E];
-        const uint32_t* seg = sc.pend[0] + t.seg_min[E];
+        uint32_t i0 = 0;
+        if (lane == 0) i0 = atomicAdd(&ctl->nlong[1], 32u);
+        i0 = __shfl_sync(0xFFFFFFFFu, i0, 0);
+        if (i0 >= n) break;
+        const uint32_t i = i0 + lane;
+        uint64_t E = NONE64;
+        uint32_t c = 0, base = 0;
         bool bad = false;
-        for (uint32_t q = lane; q < c; q += 32) {
-            const uint32_t x = seg[q];
-            bad |= x >= n0 || sc.op_slot[x] != E;  // a place this call did not fill
+        if (i < n) {
+            E = sc.op_slot[sc.long_list[i]];
+            c = t.seg_cnt[E];
+            base = t.seg_min[E];
+            bad = (uint64_t)base + c > n0;  // segments hold n0 words at most
+            for (uint32_t q = 0; q < c && !bad; q++) {
+                const uint32_t x = sc.pend[0][base + q];
+                bad = x >= n0 || sc.op_slot[x] != E;  // a place this call did not fill
+            }
+            if (bad) atomicOr(&ctl->err, ERR_SCRATCH);  // the group is not run
         }
-        bad = __any_sync(0xFFFFFFFFu, bad);
-        if (bad && lane == 0) atomicOr(&ctl->err, ERR_SCRATCH);  // the group is not run
-        const bool over = !bad && c > RX_GMAX;  // too many for a warp: to the rounds
-        uint32_t at = 0;
-        if (over && lane == 0) at = atomicAdd(&ctl->npend[1], c);
-        at = __shfl_sync(0xFFFFFFFFu, at, 0);
-        if (!bad)
-            for (uint32_t q = lane; q < c; q += 32) {
+        if (!bad && c >= 2 && c <= RX_THREAD) {
+            uint32_t ops[RX_THREAD];
+            for (uint32_t q = 0; q < c; q++) {  // insertion sort: index order
+                const uint32_t x = sc.pend[0][base + q];
+                uint32_t k = q;
+                while (k > 0 && ops[k - 1] > x) {
+                    ops[k] = ops[k - 1];
+                    --k;
+                }
+                ops[k] = x;
+            }
+            for (uint32_t q = 0; q < c; q++) {
+                RegKey<KB> key;
+                removed += rx_probe<KB>(t, key, home_of<KB>(t, keys, ops[q], key));
+            }
+        }
+        // larger groups, one at a time on the whole warp
+        for (uint32_t bm = __ballot_sync(0xFFFFFFFFu, !bad && c > RX_THREAD); bm; bm &= bm - 1) {
+            const int L = __ffs(bm) - 1;
+            const uint64_t EL = __shfl_sync(0xFFFFFFFFu, E, L);
+            const uint32_t cL = __shfl_sync(0xFFFFFFFFu, c, L);
+            const uint32_t bL = __shfl_sync(0xFFFFFFFFu, base, L);
+            const uint32_t* seg = sc.pend[0] + bL;
+            const bool over = cL > RX_GMAX;  // too many for a warp: to the rounds
+            uint32_t at = 0;
+            if (over && lane == 0) at = atomicAdd(&ctl->npend[1], cL);
+            at = __shfl_sync(0xFFFFFFFFu, at, 0);
+            for (uint32_t q = lane; q < cL; q += 32) {
                 if (over) sc.pend[1][at + q] = seg[q];
                 else grp[q] = seg[q];
             }
-        __syncwarp();
-        if (lane == 0) {
+            __syncwarp();
+            const uint32_t r = rx_group_run<KB>(t, keys, EL, over ? 0u : cL, grp);
+            if (lane == 0) removed += r;
+        }
+        if (i < n) {
             t.seg_min[E] = IDLE;
             t.seg_cnt[E] = 0;
         }
-        const uint32_t r = rx_group_run<KB>(t, keys, E, (bad || over) ? 0u : c, grp);
-        if (lane == 0) removed += r;
     }
     block_add_count(ctl, removed, s_tmp);
 }
@@ -686,9 +716,9 @@ void direct_shape(const TableView& t, const uint8_t* keys, uint32_t n0, uint32_t
         k_rx_exec<KB><<<g, RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
     }
     {
-        KtScope kt(KC_REM_GROUP, s);  // a warp per group, as many warps as can be resident
+        KtScope kt(KC_REM_GROUP, s);  // a lane per group, as many warps as can be resident
         k_rx_place<<<g, RBLOCK, 0, s>>>(t, n0, sc, ctl);
-        k_rx_warp<KB><<<grid_for((uint64_t)nmax * 32, 8), RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
+        k_rx_warp<KB><<<grid_for(nmax, 8), RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
     }
     count_launches(4);
 }
