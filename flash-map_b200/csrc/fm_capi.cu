@@ -2097,12 +2097,18 @@ const double kBucketLoad[fm::LOAD_BUCKETS] = {0.5, 0.7, 0.88};
 int tune_load(const char* path) {
     FILE* f = fopen(path, "r");
     if (!f) return 0;
-    int sh, b, lanes, bps, n = 0;
-    while (fscanf(f, "%d %d %d %d", &sh, &b, &lanes, &bps) == 4) {
+    // one line per shape and load bucket: shape bucket lanes blocks_per_sm
+    // [queries per thread, 1 when absent]
+    int n = 0;
+    char line[128];
+    while (fgets(line, sizeof line, f)) {
+        int sh, b, lanes, bps, qpt = 1;
+        if (sscanf(line, "%d %d %d %d %d", &sh, &b, &lanes, &bps, &qpt) < 4) continue;
         if (sh < 0 || sh > fm::SHAPE_GENERIC || b < 0 || b >= fm::LOAD_BUCKETS) continue;
         fm::GetCfg c;
         c.lanes = lanes;
         c.blocks_per_sm = bps;
+        c.qpt = qpt;
         fm::set_tuned_get_cfg((fm::Shape)sh, b, c);
         ++n;
     }
@@ -2121,7 +2127,10 @@ int fm_autotune(int device, const char* cache_path) {
     if (e != cudaSuccess || device < 0 || device >= ndev) return fail(FM_ERR_CUDA_INIT, "no such CUDA device");
     DeviceGuard dg(device);
     const uint64_t cap = 1ull << 20, nq = 1ull << 20;
-    const int lanes[] = {1, 4, 8, 16, 32};
+    // candidates: lanes per query (with one lane, 1, 2 or 4 queries per
+    // thread in lockstep) x resident blocks per SM
+    const int lanes[] = {1, 1, 1, 4, 8, 16, 32};
+    const int qpts[] = {1, 2, 4, 1, 1, 1, 1};
     const int bpss[] = {8, 16, 32, 64};
     std::string out;
     cudaStream_t s = nullptr;
@@ -2156,10 +2165,11 @@ int fm_autotune(int device, const char* cache_path) {
             cudaMemcpy2DAsync(dq, 2 * sk.k, dk, sk.k * (filled / half), sk.k, half, cudaMemcpyDeviceToDevice, s);
             float best = 1e30f;
             fm::GetCfg bestc;
-            for (int l : lanes) {
+            for (int li = 0; li < (int)(sizeof(lanes) / sizeof(lanes[0])); li++) {
                 for (int bps : bpss) {
                     fm::GetCfg c;
-                    c.lanes = l;
+                    c.lanes = lanes[li];
+                    c.qpt = qpts[li];
                     c.blocks_per_sm = bps;
                     float ms = 1e30f;
                     for (int rep = 0; rep < 3; rep++) {
@@ -2181,7 +2191,7 @@ int fm_autotune(int device, const char* cache_path) {
             }
             fm::set_tuned_get_cfg(sk.sh, bk, bestc);
             out += std::to_string((int)sk.sh) + " " + std::to_string(bk) + " " + std::to_string(bestc.lanes) + " " +
-                   std::to_string(bestc.blocks_per_sm) + "\n";
+                   std::to_string(bestc.blocks_per_sm) + " " + std::to_string(bestc.qpt) + "\n";
         }
         fm_destroy(t);
         cudaFree(dk), cudaFree(dv), cudaFree(dq), cudaFree(dout), cudaFree(dfound);

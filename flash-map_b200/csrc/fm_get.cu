@@ -149,6 +149,18 @@ __global__ void __launch_bounds__(BLOCK) k_get_thread(TableView t, const uint8_t
                                  out_found ? out_found + q : nullptr);
 }
 
+// Q queries per thread probed in lockstep (get_queries_lockstep): thread g
+// takes queries g, g + G, ..., g + (Q-1)G of each span of Q*G (G threads in
+// the grid), so a warp's key loads stay coalesced.
+template <int KB, int VB, int Q>
+__global__ void __launch_bounds__(BLOCK) k_get_lockstep(TableView t, const uint8_t* __restrict__ qkeys, uint64_t n,
+                                                        uint8_t* __restrict__ out_vals,
+                                                        uint8_t* __restrict__ out_found) {
+    const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += G * Q)
+        get_queries_lockstep<KB, VB, Q>(t, qkeys, q, G, n, out_vals, out_found);
+}
+
 // Grouped lookups: the gets of a batch wave, one flat index space over their
 // queries (prefix[o] = first flat index of get o), T lanes per query (T == 1:
 // one thread per query).  Load-balanced over gets of any sizes.
@@ -206,7 +218,17 @@ cudaError_t get_shape(const TableView& t, const uint8_t* q, uint64_t n, uint8_t*
     if (lanes == 1 && !(KB != 0 && VB != 0 && t.mask >= 7)) lanes = 8;
     switch (lanes) {
         case 1:
-            if constexpr (KB != 0 && VB != 0) get_launch<KB, VB, 1>(t, q, n, ov, of, cfg.blocks_per_sm, s);
+            if constexpr (KB != 0 && VB != 0) {
+                if (cfg.qpt == 2 || cfg.qpt == 4) {
+                    KtScope kt(KC_GET, s);
+                    const unsigned g = grid_for((n + cfg.qpt - 1) / cfg.qpt, cfg.blocks_per_sm);
+                    if (cfg.qpt == 2) k_get_lockstep<KB, VB, 2><<<g, BLOCK, 0, s>>>(t, q, n, ov, of);
+                    else k_get_lockstep<KB, VB, 4><<<g, BLOCK, 0, s>>>(t, q, n, ov, of);
+                    g_launches += 1;
+                } else {
+                    get_launch<KB, VB, 1>(t, q, n, ov, of, cfg.blocks_per_sm, s);
+                }
+            }
             break;
         case 4: get_launch<KB, VB, 4>(t, q, n, ov, of, cfg.blocks_per_sm, s); break;
         case 16: get_launch<KB, VB, 16>(t, q, n, ov, of, cfg.blocks_per_sm, s); break;

@@ -193,8 +193,9 @@ struct GroupOp {
 // Lookup kernel configuration: lanes per query (1: one thread per query with
 // 8-slot windows; 4..32: a tile) and resident blocks per SM for the grid.
 struct GetCfg {
-    int lanes = 1;
+    int lanes = 1;          // lanes per query
     int blocks_per_sm = 64;
+    int qpt = 1;            // one lane per query: queries per thread probed in lockstep (1, 2 or 4)
 };
 cudaError_t launch_get_cfg(const TableView& t, Shape sh, const uint8_t* qkeys, uint64_t n, uint8_t* out_vals,
                            uint8_t* out_found, GetCfg cfg, cudaStream_t s);
