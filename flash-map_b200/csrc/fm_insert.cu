@@ -2310,11 +2310,16 @@ __global__ void __launch_bounds__(DX_THREADS, 2) k_dx_exec(TableView t, const ui
     const bool to_pend = n0_arg == CMP_N0_CTL;
     const bool serial = *(volatile uint32_t*)&ctl->serial[0] != 0;
     const bool lanes_ok = t.mask >= 7 && t.mask < (uint64_t)DIST_MASK;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t iters = (n0 + stride - 1) / stride;
     ExecAcc a;
-    for (uint32_t it = 0; it < iters; it++) {
-        const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x + it * stride;
+    // ops taken 32 at a time per warp from a counter (Ctl::exec_next, zero at
+    // the start of the call): the grid is the resident blocks, and a warp that
+    // drew long walks does not hold up a static share of the ops
+    for (;;) {
+        uint32_t j0 = 0;
+        if ((threadIdx.x & 31u) == 0) j0 = atomicAdd(&ctl->exec_next, 32u);
+        j0 = __shfl_sync(0xFFFFFFFFu, j0, 0);
+        if (j0 >= n0) break;
+        const uint32_t j = j0 + (threadIdx.x & 31u);
         uint32_t item = 0;
         bool defer = false;
         if (j < n0 && serial && to_pend) sc.pend[1][atomicAdd(&ctl->npend[1], 1u)] = j;
@@ -3444,7 +3449,8 @@ void direct_shape(const TableView& t, const uint8_t* keys, const uint8_t* vals, 
         }
         {
             KtScope kt(KC_INS_EXEC, s);
-            launch_dependent(k_dx_exec<KB, VB>, g, DX_THREADS, s, pdl, t, keys, vals, n0, sc, ctl);
+            const unsigned ge = grid_for(nmax, 2);  // the resident blocks at most (two per SM)
+            launch_dependent(k_dx_exec<KB, VB>, ge, DX_THREADS, s, pdl, t, keys, vals, n0, sc, ctl);
         }
         {
             KtScope kt(KC_INS_LONG, s);

@@ -33,6 +33,8 @@ struct Ctl {
     uint32_t nbig;           // batch queue inserts: components listed for the block pass (pend[0] pairs)
     uint32_t big_next;       //   the next of them to take
     uint32_t big_ops;        //   op indices they hold (pend[1])
+    uint32_t exec_next;      // direct insert exec pass: the next op a warp takes
+    uint32_t pad_[7];        // count_part on a 32-byte boundary
     unsigned long long count;  // new keys (insert) / removed keys (remove), single-block kernels
     unsigned long long count_part[COUNT_PARTS][4];  // the same from grid kernels, [i][0] used
     // Persistent table facts (survive across calls, reset by clear):
@@ -45,7 +47,8 @@ struct Ctl {
         return s;
     }
 };
-constexpr size_t CTL_CALL_BYTES = 64 + 32 * COUNT_PARTS;  // npend .. count_part
+constexpr size_t CTL_CALL_BYTES = 96 + 32 * COUNT_PARTS;  // npend .. count_part
+static_assert(offsetof(Ctl, count_part) % 32 == 0, "count parts in their own sectors");
 static_assert(offsetof(Ctl, dmax) == CTL_CALL_BYTES, "Ctl layout");
 
 // Op status codes written by device code (the FM_* values of the C ABI).
