@@ -2010,9 +2010,15 @@ __global__ void __launch_bounds__(RBLOCK) k_cmp_clean(TableView t, OpScratch sc)
 constexpr uint32_t DX_ABS = 0x80000000u;   // seg_cnt: the free slot is in an earlier slot's component
 constexpr uint32_t DX_CNT = 0x7FFFFFFFu;
 constexpr uint32_t DX_ROOT = 0x80000000u;  // warp-pass list entry: a component's leader
-constexpr int DX_LCH = 16;                 // evictions of a walk on the thread path
+#ifndef FM_DX_LCH
+#define FM_DX_LCH 4
+#endif
+#ifndef FM_DX_LTRIPS
+#define FM_DX_LTRIPS 4
+#endif
+constexpr int DX_LCH = FM_DX_LCH;          // evictions of a walk on the thread path
 constexpr int DX_LCMP = 6;                 // possible updates of a walk on the thread path
-constexpr int DX_LTRIPS = 4;               // 16-slot metadata reads of a walk on the thread path
+constexpr int DX_LTRIPS = FM_DX_LTRIPS;    // 16-slot metadata reads of a walk on the thread path
 constexpr int DX_GATHER = 64;              // ops of a component the warp pass runs itself
 constexpr int DX_THREADS = 256;            // threads of an exec block
 
@@ -3506,9 +3512,12 @@ cudaError_t launch_ins_direct_ctl(const TableView& t, Shape sh, const uint8_t* k
 // Tuned insert configurations, per shape and load bucket (tile 0: not measured).
 InsCfg g_ins_tuned[SHAPE_GENERIC + 1][LOAD_BUCKETS];
 
+#ifndef FM_INS_TILE
+#define FM_INS_TILE 32  // the warp pass's tile width where none was tuned
+#endif
 InsCfg tuned_ins_cfg(Shape sh, double load) {
     InsCfg c = g_ins_tuned[sh][load_bucket(load)];
-    if (c.tile != 8 && c.tile != 16 && c.tile != 32) c.tile = 32;
+    if (c.tile != 8 && c.tile != 16 && c.tile != 32) c.tile = FM_INS_TILE;
     return c;
 }
 
