@@ -654,7 +654,7 @@ def batched_leg(torch, F, native, dev, steps, warmup, scale=1, clip=False):
 # ---------------------------------------------------------------------------
 # Served form: Poisson request stream against a device-resident table
 # ---------------------------------------------------------------------------
-SERVE_RATE, SERVE_REQS, SERVE_SAT_REQS = 2000.0, 2000, 500
+SERVE_RATE, SERVE_REQS, SERVE_SAT_REQS = 2000.0, 10000, 2000
 SERVE_INSERT_POOL = 16_000_000  # fresh insert keys, taken in turn (later passes update)
 
 
@@ -664,10 +664,10 @@ def served_leg(torch, F, dev, scale=1):
     Poisson stream at 2,000/s, each insert / get / remove with probability
     0.3 / 0.6 / 0.1 and a size log-uniform in 64..1M keys, get and remove keys
     80% present (Zipf s=0.9 over a 4M-key sample of the present keys); 20 GB
-    staging budget (admitted against free HBM).  2,000 requests (one second
+    staging budget (admitted against free HBM).  10,000 requests (five seconds
     of arrivals) are served in real time with continuous batching and, from
     the same start state (a device copy), by the plain one-call-per-request
-    server through AsyncFlashMap; then the first 500 requests arrive all at
+    server through AsyncFlashMap; then the first 2,000 requests arrive all at
     once (saturation) for both, which gives each form's throughput.  Request
     inputs are slices of pinned host pools (inserts: a pool of 16M fresh keys
     taken in turn, so later passes update; gets/removes: the skewed mix); get

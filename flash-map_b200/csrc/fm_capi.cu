@@ -2099,10 +2099,19 @@ int tune_load(const char* path) {
     if (!f) return 0;
     // one line per shape and load bucket: shape bucket lanes blocks_per_sm
     // [queries per thread, 1 when absent]
+    // ("ins shape bucket tile": the insert warp pass's tile width)
     int n = 0;
     char line[128];
     while (fgets(line, sizeof line, f)) {
         int sh, b, lanes, bps, qpt = 1;
+        if (sscanf(line, "ins %d %d %d", &sh, &b, &lanes) == 3) {
+            if (sh < 0 || sh >= fm::SHAPE_GENERIC || b < 0 || b >= fm::LOAD_BUCKETS) continue;
+            fm::InsCfg c;
+            c.tile = lanes;
+            fm::set_tuned_ins_cfg((fm::Shape)sh, b, c);
+            ++n;
+            continue;
+        }
         if (sscanf(line, "%d %d %d %d %d", &sh, &b, &lanes, &bps, &qpt) < 4) continue;
         if (sh < 0 || sh > fm::SHAPE_GENERIC || b < 0 || b >= fm::LOAD_BUCKETS) continue;
         fm::GetCfg c;
@@ -2192,6 +2201,50 @@ int fm_autotune(int device, const char* cache_path) {
             fm::set_tuned_get_cfg(sk.sh, bk, bestc);
             out += std::to_string((int)sk.sh) + " " + std::to_string(bk) + " " + std::to_string(bestc.lanes) + " " +
                    std::to_string(bestc.blocks_per_sm) + " " + std::to_string(bestc.qpt) + "\n";
+            // the insert warp pass's tile width: a call of nins fresh keys
+            // (the queries' second half) from this state, restored from a
+            // device copy before every candidate
+            {
+                const uint64_t nins = nq / 2 < cap / 50 ? nq / 2 : cap / 50;
+                const uint8_t* ik = dq + (nq / 2) * sk.k;
+                fm_table* bk_t = nullptr;
+                if ((rc = fm_create(cap, sk.k, sk.v, FM_HASH_IDENTITY, device, &bk_t)) != FM_OK) break;
+                rc = fm_copy(bk_t, t, s);
+                const int tiles[] = {8, 16, 32};
+                float best_i = 1e30f;
+                int best_t = 32;
+                for (int tw : tiles) {
+                    fm::InsCfg ic;
+                    ic.tile = tw;
+                    fm::set_tuned_ins_cfg(sk.sh, bk, ic);
+                    float ms_i = 1e30f;
+                    for (int rep = 0; rep < 3 && rc == FM_OK; rep++) {
+                        if ((rc = fm_copy(t, bk_t, s)) != FM_OK) break;
+                        uint64_t added = 0;
+                        cudaEventRecord(a, s);
+                        rc = fm_bulk_insert_device(t, ik, dv, nins, &added, s);
+                        cudaEventRecord(b, s);
+                        if (rc != FM_OK || (e = cudaEventSynchronize(b)) != cudaSuccess) break;
+                        float x = 0.f;
+                        cudaEventElapsedTime(&x, a, b);
+                        if (rep > 0 && x < ms_i) ms_i = x;  // the first run warms up
+                    }
+                    if (rc != FM_OK || e != cudaSuccess) break;
+                    if (ms_i < best_i) best_i = ms_i, best_t = tw;
+                }
+                if (rc == FM_OK) rc = fm_copy(t, bk_t, s);  // the filled state for the next bucket
+                fm_destroy(bk_t);
+                if (rc != FM_OK) break;
+                if (e != cudaSuccess) {
+                    rc = cuda_fail(FM_ERR_KERNEL_LAUNCH, "autotune", e);
+                    break;
+                }
+                fm::InsCfg ic;
+                ic.tile = best_t;
+                fm::set_tuned_ins_cfg(sk.sh, bk, ic);
+                out += "ins " + std::to_string((int)sk.sh) + " " + std::to_string(bk) + " " + std::to_string(best_t) +
+                       "\n";
+            }
         }
         fm_destroy(t);
         cudaFree(dk), cudaFree(dv), cudaFree(dq), cudaFree(dout), cudaFree(dfound);

@@ -46,3 +46,29 @@ def test_every_lookup_configuration_matches_the_oracle(shape, tmp_path):
             assert np.array_equal(gv, ev), (lanes, bps, qpt)
     finally:
         _force(tmp_path, 1, 64, 1)  # the untuned default for the tests after this one
+
+
+def test_autotune_writes_lookup_and_insert_choices(tmp_path):
+    """fm_autotune times the lookup configurations and the insert warp pass's
+    tile width per record shape and load bucket and writes both to its cache;
+    inserts and lookups under the tuned choices still match the oracle."""
+    from flash_map import _native
+
+    path = tmp_path / "tune.txt"
+    _native.autotune(0, str(path))  # no cache yet: measures and writes it
+    lines = path.read_text().split("\n")
+    gets = [x for x in lines if x and not x.startswith("ins")]
+    ins = [x.split() for x in lines if x.startswith("ins")]
+    assert len(gets) == 5 * 3 and len(ins) == 5 * 3
+    assert all(int(x[3]) in (8, 16, 32) for x in ins)
+    _native.autotune(0, str(path))  # read back from the cache
+    rng = np.random.default_rng(71)
+    for ks, vs in ((8, 8), (32, 128)):
+        cap = 1 << 15
+        g, o = gpu_map(cap, ks, vs), OracleAdapter(cap, ks, vs)
+        for frac in (0.5, 0.3, 0.1):
+            k = rng.integers(0, 256, (int(cap * frac), ks), dtype=np.uint8)
+            v = rng.integers(0, 256, (len(k), vs), dtype=np.uint8)
+            assert g.bulk_insert(k, v) == o.bulk_insert(k, v)
+        for x, y in zip(g.snapshot(), o.snapshot()):
+            assert np.array_equal(x, y)
