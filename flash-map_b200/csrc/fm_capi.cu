@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -1265,7 +1266,9 @@ struct fm_batch {
     // segment; an insert that can take its table to FM_DIRECT_LOAD closes the
     // segment and runs on the component path between launches.
     bool qmode = false;
+    bool qlanes = false;  // queue mode: every op a device-driven step on its table's stream lane
     struct QStep {
+        uint32_t lane = 0;      // qlanes: the stream lane of its table
         bool external = false;  // an insert or remove run between persistent launches
         bool remove = false;    // external: a remove
         bool get = false;       // external: a lookup
@@ -1441,8 +1444,16 @@ int queue_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
     const auto* dph = reinterpret_cast<const fm::QPhase*>(b->d_desc + b->q_ph_off);
     const auto* dg = reinterpret_cast<const fm::GroupOp*>(b->d_desc + b->q_ext_off);
     const auto* hg = reinterpret_cast<const fm::GroupOp*>(b->h_desc + b->q_ext_off);
+    const cudaStream_t s0 = s;
+    const bool fork = b->qlanes && b->nlanes > 1;
+    if (fork) {  // the lanes start after the uploads on the caller's stream
+        e = cudaEventRecord(b->ev_fork, s0);
+        for (uint32_t l = 0; e == cudaSuccess && l < b->nlanes; l++) e = cudaStreamWaitEvent(b->lane_s[l], b->ev_fork, 0);
+        if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch lanes", e);
+    }
     for (size_t si = 0; si < b->qsteps.size(); si++) {
         fm_batch::QStep& st = b->qsteps[si];
+        s = fork ? b->lane_s[st.lane] : s0;
         if (!st.external) {
             fm::QProf* pr = b->d_prof ? b->d_prof + st.ph0 : nullptr;
             e = fm::launch_queue(st.shape, dph + st.ph0, st.nph, st.units, dq, b->d_done + st.ph0, b->d_qstate + si,
@@ -1497,6 +1508,14 @@ int queue_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
         }
         if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch queue", e);
     }
+    s = s0;
+    if (fork) {  // join the lanes back before the downloads
+        for (uint32_t l = 0; e == cudaSuccess && l < b->nlanes; l++) {
+            e = cudaEventRecord(b->ev_join[l], b->lane_s[l]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b->ev_join[l], 0);
+        }
+        if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch lanes", e);
+    }
     e = cudaMemcpyAsync(b->h_len(), b->d_len, b->tables.size() * 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_res(), b->d_res, b->ops.size() * 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_status(), b->d_status, b->ops.size() * 4, cudaMemcpyDeviceToHost, s);
@@ -1506,15 +1525,50 @@ int queue_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
     return FM_OK;
 }
 
+// Queue mode runs every op as device-driven kernels on its table's stream
+// lane (up to BATCH_LANES lanes forked from the caller's stream: the ops of
+// different tables overlap, each table's keep their order) when the batch has
+// tables on two lanes or more, and drains the ops through the persistent
+// kernel otherwise.  FLASHMAP_BATCH_MODE=queue or =lanes forces either.
+bool queue_lanes_wanted(uint32_t ntables) {
+    const char* m = getenv("FLASHMAP_BATCH_MODE");
+    if (m && !strcmp(m, "queue")) return false;
+    if (m && !strcmp(m, "lanes")) return true;
+    return ntables >= 2;
+}
+
 // Queue mode plan: segments of ops closed by the inserts that run between
 // persistent launches (large or able to fill their table); per segment
 // and record shape, the phases of every table's chain of ops listed level by
 // level (the first phase of every chain, then the second, ...), each waiting
 // for the one before it in its chain.
-void queue_plan(fm_batch* b) {
+void queue_plan(fm_batch* b, const std::vector<uint32_t>& lane_of) {
     const uint32_t nops = (uint32_t)b->ops.size();
     std::vector<double> est(b->tables.size());
     for (size_t i = 0; i < b->tables.size(); i++) est[i] = (double)b->tables[i]->len.load();
+    if (b->qlanes) {
+        // every op a device-driven step, in queue order on its table's lane
+        for (uint32_t i = 0; i < nops; i++) {
+            const fm_op& o = b->ops[i];
+            if (o.n == 0) continue;  // nothing to run; result 0, status OK
+            const uint32_t ti = b->table_of[i];
+            const double cap = (double)b->tables[ti]->cap;
+            fm_batch::QStep st;
+            st.external = true;
+            st.lane = lane_of[ti];
+            st.op = i;
+            st.shape = o.table->shape;
+            st.get = o.kind == FM_OP_GET;
+            st.remove = o.kind == FM_OP_REMOVE;
+            if (o.kind == FM_OP_INSERT) est[ti] = std::min(est[ti] + (double)o.n, cap);
+            st.direct = est[ti] < FM_DIRECT_LOAD * cap;
+            st.load = est[ti] / cap;
+            st.ext = (uint32_t)b->qext_ops.size();
+            b->qext_ops.push_back(i);
+            b->qsteps.push_back(st);
+        }
+        return;
+    }
     std::vector<uint32_t> seg;
     auto flush = [&]() {
         for (int shi = 0; shi < (int)fm::SHAPE_GENERIC; shi++) {
@@ -1784,7 +1838,29 @@ int fm_batch_create(const fm_op* ops, uint32_t nops, fm_batch** out) {
         if (o.table->shape == fm::SHAPE_GENERIC || !batch_aligned(o) || o.n >= (1ull << 31)) b->qmode = false;
     }
     if (b->qmode) {
-        queue_plan(b);
+        // lanes: tables by decreasing work (sum of op sizes, mutations
+        // weighted up), each to the lane with the least work so far
+        const uint32_t ntab = (uint32_t)b->tables.size();
+        std::vector<uint32_t> lane_of(ntab, 0);
+        b->qlanes = queue_lanes_wanted(ntab);
+        b->nlanes = b->qlanes ? (ntab < fm_batch::BATCH_LANES ? ntab : fm_batch::BATCH_LANES) : 1;
+        {
+            std::vector<double> work(ntab, 0.0);
+            for (uint32_t i = 0; i < nops; i++)
+                work[b->table_of[i]] += (double)ops[i].n * (ops[i].kind == FM_OP_GET ? 1.0 : 4.0);
+            std::vector<uint32_t> order(ntab);
+            for (uint32_t i = 0; i < ntab; i++) order[i] = i;
+            std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return work[x] > work[y]; });
+            std::vector<double> lane_work(b->nlanes, 0.0);
+            for (uint32_t ti : order) {
+                uint32_t best = 0;
+                for (uint32_t l = 1; l < b->nlanes; l++)
+                    if (lane_work[l] < lane_work[best]) best = l;
+                lane_of[ti] = best;
+                lane_work[best] += work[ti];
+            }
+        }
+        queue_plan(b, lane_of);
         size_t off = 0;
         auto take = [&](size_t bytes) {
             const size_t o = off;
@@ -1820,6 +1896,17 @@ int fm_batch_create(const fm_op* ops, uint32_t nops, fm_batch** out) {
         b->h_qstate = reinterpret_cast<fm::QState*>(b->arena.h + h_qs);
         memset(b->h_desc, 0, b->desc_bytes);
         memset(b->h_io, 0, b->io_bytes());
+        if (b->nlanes > 1) {
+            e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+            for (uint32_t l = 0; e == cudaSuccess && l < b->nlanes; l++) {
+                e = cudaStreamCreateWithFlags(&b->lane_s[l], cudaStreamNonBlocking);
+                if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join[l], cudaEventDisableTiming);
+            }
+            if (e != cudaSuccess) {
+                fm_batch_destroy(b);
+                return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch streams", e);
+            }
+        }
         *out = b;
         return FM_OK;
     }

@@ -13,6 +13,15 @@ pytestmark = pytest.mark.gpu
 SHAPES = [(8, 8), (32, 128), (32, 32), (8, 32)]
 
 
+@pytest.fixture(autouse=True, params=["queue", "lanes"])
+def batch_mode(request, monkeypatch):
+    """Every test under both queue-mode executions: the persistent kernel
+    draining the ops (with device-driven steps for the large ones), and
+    every op as device-driven kernels on its table's stream lane."""
+    monkeypatch.setenv("FLASHMAP_BATCH_MODE", request.param)
+    return request.param
+
+
 def _keys(rng, n, ks):
     return rng.integers(0, 256, (n, ks), dtype=np.uint8)
 
