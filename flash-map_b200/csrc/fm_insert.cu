@@ -2851,30 +2851,6 @@ __device__ __noinline__ void q_iwarp(const QOp& o, uint32_t c, uint32_t units, Q
     publish_rare(o.ctl, a.maxd, a.tomb, a.limit);
 }
 
-// Sorts a[0..n) (n <= QBIG_MAX) ascending in shared memory: bitonic network
-// over the next power of two, padded with 0xFFFFFFFF.  Block-uniform call.
-__device__ void block_sort_u32(uint32_t* a, uint32_t n) {
-    uint32_t P = 1;
-    while (P < n) P <<= 1;
-    for (uint32_t i = n + threadIdx.x; i < P; i += blockDim.x) a[i] = 0xFFFFFFFFu;
-    __syncthreads();
-    for (uint32_t k = 2; k <= P; k <<= 1) {
-        for (uint32_t d = k >> 1; d > 0; d >>= 1) {
-            for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
-                const uint32_t m = i ^ d;
-                if (m > i) {
-                    const uint32_t x = a[i], y = a[m];
-                    if ((x > y) == ((i & k) == 0)) {
-                        a[i] = y;
-                        a[m] = x;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
-}
-
 // The block pass: the components the warp pass listed (dx_gather_q), taken
 // one at a time; each is sorted into index order in shared memory and run by
 // warp 0 op after op.  A component of more than QBIG_MAX ops is marked for the

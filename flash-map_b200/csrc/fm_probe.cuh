@@ -174,6 +174,31 @@ __device__ __forceinline__ void get_queries_lockstep(const TableView& t, const u
     }
 }
 
+// Sorts a[0..n) ascending in shared memory (a holds the next power of two
+// >= n words): bitonic network over that power of two, padded with
+// 0xFFFFFFFF.  Block-uniform call.
+static __device__ __noinline__ void block_sort_u32(uint32_t* a, uint32_t n) {
+    uint32_t P = 1;
+    while (P < n) P <<= 1;
+    for (uint32_t i = n + threadIdx.x; i < P; i += blockDim.x) a[i] = 0xFFFFFFFFu;
+    __syncthreads();
+    for (uint32_t k = 2; k <= P; k <<= 1) {
+        for (uint32_t d = k >> 1; d > 0; d >>= 1) {
+            for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+                const uint32_t m = i ^ d;
+                if (m > i) {
+                    const uint32_t x = a[i], y = a[m];
+                    if ((x > y) == ((i & k) == 0)) {
+                        a[i] = y;
+                        a[m] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
 // First EMPTY slot at or after home h, NONE64 when the table has none (two
 // aligned 8-slot windows per round trip with capacity >= 8).
 __device__ __forceinline__ uint64_t rx_first_empty(const TableView& t, uint64_t h) {
@@ -313,6 +338,7 @@ __device__ __forceinline__ uint32_t rx_chunk32(const TableView& t, const uint8_t
 // to RX_THREAD of them one thread runs.
 constexpr uint32_t RX_GMAX = 256;
 constexpr uint32_t RX_THREAD = 8;
+constexpr uint32_t RX_BMAX = 8192;  // ops of a group one block sorts in shared memory
 
 template <int KB>
 __device__ __noinline__ uint32_t rx_group_run(const TableView& t, const uint8_t* keys, uint64_t E, uint32_t g,

@@ -528,11 +528,13 @@ void rounds_shape(const TableView& t, const uint8_t* keys, uint32_t n0, uint32_t
 //        in its group's segment.
 //   group (a lane per listed E)  reads the segment, orders it by index and
 //        runs the ops one after another (up to RX_THREAD ops) or on the whole
-//        warp in chunks of 32 (rx_group_run).
+//        warp in chunks of 32 (rx_group_run, up to RX_GMAX ops);
+//   block (a block per larger group, up to RX_BMAX ops)  sorts the segment in
+//        shared memory and runs it in chunks of 32 on warp 0 (rx_chunk32).
 // A call where some op finds no EMPTY slot (its probe could go round the
 // table) leaves every op to the rounds (Ctl::serial[0]); a group of more than
-// RX_GMAX ops leaves its ops to them (pend[1], Ctl::npend[1]).  Every
-// registration and list word is idle again when the four kernels end.
+// RX_BMAX ops leaves its ops to them (pend[1], Ctl::npend[1]).  Every
+// registration and list word is idle again when the five kernels end.
 
 template <int KB>
 __global__ void __launch_bounds__(RBLOCK) k_rx_find(TableView t, const uint8_t* __restrict__ keys, uint32_t n0_arg,
@@ -676,14 +678,18 @@ __global__ void __launch_bounds__(RBLOCK) k_rx_warp(TableView t, const uint8_t* 
                 removed += rx_probe<KB>(t, key, home_of<KB>(t, keys, ops[q], key));
             }
         }
+        // groups of up to RX_BMAX ops to the block pass (listed after the
+        // groups in long_list; their registrations stay for it)
+        const bool blk = !bad && c > RX_GMAX && c <= RX_BMAX;
+        if (blk) sc.long_list[n + atomicAdd(&ctl->nbig, 1u)] = sc.long_list[i];
         // larger groups, one at a time on the whole warp
-        for (uint32_t bm = __ballot_sync(0xFFFFFFFFu, !bad && c > RX_THREAD); bm; bm &= bm - 1) {
+        for (uint32_t bm = __ballot_sync(0xFFFFFFFFu, !bad && !blk && c > RX_THREAD); bm; bm &= bm - 1) {
             const int L = __ffs(bm) - 1;
             const uint64_t EL = __shfl_sync(0xFFFFFFFFu, E, L);
             const uint32_t cL = __shfl_sync(0xFFFFFFFFu, c, L);
             const uint32_t bL = __shfl_sync(0xFFFFFFFFu, base, L);
             const uint32_t* seg = sc.pend[0] + bL;
-            const bool over = cL > RX_GMAX;  // too many for a warp: to the rounds
+            const bool over = cL > RX_GMAX;  // too many for a block: to the rounds
             uint32_t at = 0;
             if (over && lane == 0) at = atomicAdd(&ctl->npend[1], cL);
             at = __shfl_sync(0xFFFFFFFFu, at, 0);
@@ -695,10 +701,67 @@ __global__ void __launch_bounds__(RBLOCK) k_rx_warp(TableView t, const uint8_t* 
             const uint32_t r = rx_group_run<KB>(t, keys, EL, over ? 0u : cL, grp);
             if (lane == 0) removed += r;
         }
-        if (i < n) {
+        if (i < n && !blk) {
             t.seg_min[E] = IDLE;
             t.seg_cnt[E] = 0;
         }
+    }
+    block_add_count(ctl, removed, s_tmp);
+}
+
+// The block pass: groups of RX_GMAX..RX_BMAX ops (listed by the group pass
+// after its own entries, Ctl::nbig of them), taken one at a time per block
+// from Ctl::big_next; each is sorted into index order in shared memory and
+// run by warp 0 in chunks of 32 (rx_chunk32).
+template <int KB>
+__global__ void __launch_bounds__(RBLOCK) k_rx_big(TableView t, const uint8_t* __restrict__ keys, uint32_t n0_arg,
+                                                   OpScratch sc, Ctl* ctl) {
+    __shared__ uint32_t s_list[RX_BMAX];
+    __shared__ uint32_t s_tmp[RBLOCK / 32];
+    __shared__ uint32_t s_k;
+    const uint32_t n0 = n0_arg != CMP_N0_CTL ? n0_arg : *(volatile const uint32_t*)&ctl->n0;
+    const uint32_t n = *(volatile const uint32_t*)&ctl->nlong[0];
+    const uint32_t nb = *(volatile const uint32_t*)&ctl->nbig;
+    uint32_t removed = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_k = atomicAdd(&ctl->big_next, 1u);
+        __syncthreads();
+        const uint32_t k = s_k;
+        __syncthreads();  // every thread has read s_k
+        if (k >= nb) break;
+        const uint64_t E = sc.op_slot[sc.long_list[n + k]];
+        const uint32_t c = t.seg_cnt[E];
+        const uint32_t base = t.seg_min[E];
+        if (c > RX_BMAX || (uint64_t)base + c > n0) {  // not a group the group pass listed
+            if (threadIdx.x == 0) atomicOr(&ctl->err, ERR_SCRATCH);
+            continue;
+        }
+        for (uint32_t q = threadIdx.x; q < c; q += blockDim.x) {
+            const uint32_t x = sc.pend[0][base + q];
+            s_list[q] = x < n0 ? x : 0xFFFFFFFFu;  // out of range: flagged below
+        }
+        __syncthreads();
+        block_sort_u32(s_list, c);
+        // every entry valid and of this group (a sorted list of distinct ops:
+        // the largest entry is in range)
+        if (threadIdx.x < 32) {
+            bool bad = s_list[c - 1] >= n0;
+            for (uint32_t q = threadIdx.x; q < c && !bad; q += 32) bad = sc.op_slot[s_list[q]] != E;
+            bad = __any_sync(0xFFFFFFFFu, bad);
+            if (bad) {
+                if (threadIdx.x == 0) atomicOr(&ctl->err, ERR_SCRATCH);
+            } else {
+                for (uint32_t q = 0; q < c; q += 32) {
+                    const uint32_t r = rx_chunk32<KB>(t, keys, s_list + q, min(32u, c - q));
+                    if (threadIdx.x == 0) removed += r;
+                }
+            }
+            if (threadIdx.x == 0) {
+                t.seg_min[E] = IDLE;
+                t.seg_cnt[E] = 0;
+            }
+        }
+        __syncthreads();
     }
     block_add_count(ctl, removed, s_tmp);
 }
@@ -719,8 +782,9 @@ void direct_shape(const TableView& t, const uint8_t* keys, uint32_t n0, uint32_t
         KtScope kt(KC_REM_GROUP, s);  // a lane per group, as many warps as can be resident
         k_rx_place<<<g, RBLOCK, 0, s>>>(t, n0, sc, ctl);
         k_rx_warp<KB><<<grid_for(nmax, 8), RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
+        k_rx_big<KB><<<grid_for((uint64_t)nmax * 256 / (RX_GMAX + 1), 2), RBLOCK, 0, s>>>(t, keys, n0, sc, ctl);
     }
-    count_launches(4);
+    count_launches(5);
 }
 
 }  // namespace

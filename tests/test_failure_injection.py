@@ -110,29 +110,29 @@ def _clustered(cap, n, first_home, span, ks):
 
 @pytest.mark.parametrize("shape", [(8, 8), (32, 128)])
 def test_failed_remove_with_chunk_summaries_then_remove(shape):
-    """A remove on a table whose largest stored distance is far above 256
-    (so the call builds per-chunk summaries and marks) fails after its first
-    pass of rounds; the next removes on the table must still make progress
-    and match the oracle from the state the failure left."""
+    """A remove on a full table (no EMPTY slot, so every op goes to the
+    rounds) whose largest stored distance is far above 256 (so the call builds
+    per-chunk summaries and marks) fails after its first pass of rounds; the
+    next removes on the table must still make progress and match the oracle
+    from the state the failure left."""
     import flash_map as F
     from flash_map import _native
 
     ks, vs = shape
-    cap = 1 << 14
+    cap = 1 << 13
     rng = np.random.default_rng(4 + ks)
     k = np.concatenate([_clustered(cap, 1500, 300, 40, ks),
-                        rng.integers(0, 256, (cap // 2, ks), dtype=np.uint8)])
+                        rng.integers(0, 256, (cap - 1500, ks), dtype=np.uint8)])
     v = rng.integers(0, 256, (len(k), vs), dtype=np.uint8)
     g = F.FlashMap(cap, ks, vs)
     o = OracleAdapter(cap, ks, vs)
-    assert g.bulk_insert(k, v) == o.bulk_insert(k, v)
+    assert g.bulk_insert(k, v) == o.bulk_insert(k, v) == cap
     flags = g.snapshot()[0]
-    assert (flags >> 4).max() >= 256
+    assert (flags >> 4).max() >= 256 and not ((flags & 0xF) == 0).any()
     rm = k[rng.choice(len(k), 4000, replace=False)]
-    # about 600 of the removes fall in the cluster's run between EMPTY slots:
-    # too many for the direct remove, so they go to the rounds; the fault
-    # fires at the readback after the first pass of those rounds (the direct
-    # remove's readback is the pass before it)
+    # no EMPTY slot: the direct remove leaves every op to the rounds; the
+    # fault fires at the readback after the first pass of those rounds (the
+    # direct remove's readback is the pass before it)
     _native.inject_fault(_native.FAULT_ROUND, 1)
     with pytest.raises(F.KernelLaunch):
         g.bulk_remove(rm)

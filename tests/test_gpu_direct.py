@@ -176,3 +176,34 @@ def test_direct_small_tables(cap, shape):
         rm = k[: n // 3]
         assert g.bulk_remove(rm) == o.bulk_remove(rm)
         _same(g, o)
+
+
+@pytest.mark.parametrize("shape", [(8, 8), (32, 128)])
+@pytest.mark.parametrize("ngroup", [300, 3000, 9000])
+def test_direct_remove_group_sizes(shape, ngroup):
+    """A remove whose ops share one run between EMPTY slots in groups too
+    large for a warp: 300 and 3,000 ops (the block pass) and 9,000 ops (the
+    rounds), with repeats of the same keys and absent keys among them, beside
+    lone removes and small groups elsewhere."""
+    ks, vs = shape
+    cap = 1 << 15
+    rng = np.random.default_rng(ngroup + ks)
+    g, o = gpu_map(cap, ks, vs), OracleAdapter(cap, ks, vs)
+    nclu = min(ngroup + ngroup // 4, 12000)
+    homes = 2000 + (np.arange(nclu, dtype=np.uint64) % np.uint64(200))
+    clu = _u64((np.arange(nclu, dtype=np.uint64) + 1) * np.uint64(cap) + homes, ks)
+    k0 = np.concatenate([clu, rng.integers(0, 256, (cap // 3, ks), dtype=np.uint8)])
+    v0 = rng.integers(0, 256, (len(k0), vs), dtype=np.uint8)
+    assert g.bulk_insert(k0, v0) == o.bulk_insert(k0, v0)
+    absent = _u64((np.arange(ngroup // 10, dtype=np.uint64) + 20000) * np.uint64(cap) + np.uint64(2050), ks)
+    grp = np.concatenate([clu[rng.choice(nclu, ngroup - ngroup // 10 - ngroup // 20, replace=False)],
+                          clu[rng.integers(0, nclu, ngroup // 20)], absent])
+    rest = k0[nclu + rng.choice(len(k0) - nclu, 2000, replace=False)]
+    rm = np.concatenate([grp, rest])
+    rm = rm[rng.permutation(len(rm))]
+    assert g.bulk_remove(rm) == o.bulk_remove(rm)
+    _same(g, o)
+    q = np.concatenate([clu, rest])
+    gv, gf = g.bulk_get(q)
+    ov, of = o.bulk_get(q)
+    assert np.array_equal(gf, of) and np.array_equal(gv, ov)
