@@ -1266,9 +1266,12 @@ struct fm_batch {
     // segment; an insert that can take its table to FM_DIRECT_LOAD closes the
     // segment and runs on the component path between launches.
     bool qmode = false;
-    bool qlanes = false;  // queue mode: every op a device-driven step on its table's stream lane
+    bool qlanes = false;  // queue mode: every op a device-driven step on a stream lane
+    std::vector<cudaEvent_t> step_ev;  // qlanes: recorded after each step another lane waits for
     struct QStep {
-        uint32_t lane = 0;      // qlanes: the stream lane of its table
+        uint32_t lane = 0;      // qlanes: its stream lane
+        std::vector<uint32_t> wait;  // qlanes: earlier steps on other lanes it waits for
+        bool signal = false;    // qlanes: a later step on another lane waits for it
         bool external = false;  // an insert or remove run between persistent launches
         bool remove = false;    // external: a remove
         bool get = false;       // external: a lookup
@@ -1451,9 +1454,20 @@ int queue_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
         for (uint32_t l = 0; e == cudaSuccess && l < b->nlanes; l++) e = cudaStreamWaitEvent(b->lane_s[l], b->ev_fork, 0);
         if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch lanes", e);
     }
+    // a step that a later step on another lane waits for records its event
+    // on its lane right after its work (before the next step is enqueued)
+    auto signal = [&](size_t k) -> cudaError_t {
+        if (!fork || !b->qsteps[k].signal) return cudaSuccess;
+        return cudaEventRecord(b->step_ev[k], b->lane_s[b->qsteps[k].lane]);
+    };
     for (size_t si = 0; si < b->qsteps.size(); si++) {
+        if (si > 0 && (e = signal(si - 1)) != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch lanes", e);
         fm_batch::QStep& st = b->qsteps[si];
         s = fork ? b->lane_s[st.lane] : s0;
+        if (fork)
+            for (uint32_t d : st.wait)
+                if ((e = cudaStreamWaitEvent(s, b->step_ev[d], 0)) != cudaSuccess)
+                    return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch lanes", e);
         if (!st.external) {
             fm::QProf* pr = b->d_prof ? b->d_prof + st.ph0 : nullptr;
             e = fm::launch_queue(st.shape, dph + st.ph0, st.nph, st.units, dq, b->d_done + st.ph0, b->d_qstate + si,
@@ -1508,6 +1522,8 @@ int queue_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
         }
         if (e != cudaSuccess) return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch queue", e);
     }
+    if (!b->qsteps.empty() && (e = signal(b->qsteps.size() - 1)) != cudaSuccess)
+        return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch lanes", e);
     s = s0;
     if (fork) {  // join the lanes back before the downloads
         for (uint32_t l = 0; e == cudaSuccess && l < b->nlanes; l++) {
@@ -1525,16 +1541,13 @@ int queue_enqueue(fm_batch* b, cudaStream_t s, bool adaptive) {
     return FM_OK;
 }
 
-// Queue mode runs every op as device-driven kernels on its table's stream
-// lane (up to BATCH_LANES lanes forked from the caller's stream: the ops of
-// different tables overlap, each table's keep their order) when the batch has
-// tables on two lanes or more, and drains the ops through the persistent
-// kernel otherwise.  FLASHMAP_BATCH_MODE=queue or =lanes forces either.
-bool queue_lanes_wanted(uint32_t ntables) {
+// Queue mode runs every op as device-driven kernels on BATCH_LANES stream
+// lanes forked from the caller's stream (queue_plan: a table's writes in
+// order on its lane, lookups spread over the lanes between them), or, with
+// FLASHMAP_BATCH_MODE=queue, drains the ops through the persistent kernel.
+bool queue_lanes_wanted() {
     const char* m = getenv("FLASHMAP_BATCH_MODE");
-    if (m && !strcmp(m, "queue")) return false;
-    if (m && !strcmp(m, "lanes")) return true;
-    return ntables >= 2;
+    return !(m && !strcmp(m, "queue"));
 }
 
 // Queue mode plan: segments of ops closed by the inserts that run between
@@ -1547,7 +1560,15 @@ void queue_plan(fm_batch* b, const std::vector<uint32_t>& lane_of) {
     std::vector<double> est(b->tables.size());
     for (size_t i = 0; i < b->tables.size(); i++) est[i] = (double)b->tables[i]->len.load();
     if (b->qlanes) {
-        // every op a device-driven step, in queue order on its table's lane
+        // every op a device-driven step: a table's inserts and removes on its
+        // lane in queue order; a lookup after the table's last write, on the
+        // table's lane or, with fewer tables than lanes, on the next lane in
+        // turn; a write after the table's lookups since its last write (on
+        // whatever lanes they ran)
+        const bool spread = b->tables.size() < b->nlanes;
+        std::vector<int32_t> last_w(b->tables.size(), -1);         // step of the table's last write
+        std::vector<std::vector<uint32_t>> gets(b->tables.size());  // its lookup steps since then
+        uint32_t rr = 0;
         for (uint32_t i = 0; i < nops; i++) {
             const fm_op& o = b->ops[i];
             if (o.n == 0) continue;  // nothing to run; result 0, status OK
@@ -1555,7 +1576,22 @@ void queue_plan(fm_batch* b, const std::vector<uint32_t>& lane_of) {
             const double cap = (double)b->tables[ti]->cap;
             fm_batch::QStep st;
             st.external = true;
-            st.lane = lane_of[ti];
+            // with fewer tables than lanes, lookups fill the idle lanes
+            st.lane = (o.kind == FM_OP_GET && spread) ? (rr++ % b->nlanes) : lane_of[ti];
+            const uint32_t me = (uint32_t)b->qsteps.size();
+            auto after = [&](uint32_t d) {
+                if (b->qsteps[d].lane == st.lane) return;  // stream order
+                st.wait.push_back(d);
+                b->qsteps[d].signal = true;
+            };
+            if (last_w[ti] >= 0) after((uint32_t)last_w[ti]);
+            if (o.kind == FM_OP_GET) {
+                gets[ti].push_back(me);
+            } else {
+                for (uint32_t d : gets[ti]) after(d);
+                gets[ti].clear();
+                last_w[ti] = (int32_t)me;
+            }
             st.op = i;
             st.shape = o.table->shape;
             st.get = o.kind == FM_OP_GET;
@@ -1842,8 +1878,8 @@ int fm_batch_create(const fm_op* ops, uint32_t nops, fm_batch** out) {
         // weighted up), each to the lane with the least work so far
         const uint32_t ntab = (uint32_t)b->tables.size();
         std::vector<uint32_t> lane_of(ntab, 0);
-        b->qlanes = queue_lanes_wanted(ntab);
-        b->nlanes = b->qlanes ? (ntab < fm_batch::BATCH_LANES ? ntab : fm_batch::BATCH_LANES) : 1;
+        b->qlanes = queue_lanes_wanted();
+        b->nlanes = b->qlanes ? fm_batch::BATCH_LANES : 1;
         {
             std::vector<double> work(ntab, 0.0);
             for (uint32_t i = 0; i < nops; i++)
@@ -1902,6 +1938,9 @@ int fm_batch_create(const fm_op* ops, uint32_t nops, fm_batch** out) {
                 e = cudaStreamCreateWithFlags(&b->lane_s[l], cudaStreamNonBlocking);
                 if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join[l], cudaEventDisableTiming);
             }
+            b->step_ev.assign(b->qsteps.size(), nullptr);
+            for (size_t k = 0; e == cudaSuccess && k < b->qsteps.size(); k++)
+                if (b->qsteps[k].signal) e = cudaEventCreateWithFlags(&b->step_ev[k], cudaEventDisableTiming);
             if (e != cudaSuccess) {
                 fm_batch_destroy(b);
                 return cuda_fail(FM_ERR_KERNEL_LAUNCH, "batch streams", e);
@@ -2099,6 +2138,8 @@ void fm_batch_destroy(fm_batch* b) {
         if (b->ev_join[l]) cudaEventDestroy(b->ev_join[l]);
     }
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    for (cudaEvent_t ev : b->step_ev)
+        if (ev) cudaEventDestroy(ev);
     if (b->d_prof) cudaFree(b->d_prof);
     arena_give(b->arena);
     delete b;
