@@ -144,6 +144,35 @@ template <int KB, int VB>
 __global__ void __launch_bounds__(BLOCK) k_get_thread(TableView t, const uint8_t* __restrict__ qkeys, uint64_t n,
                                                       uint8_t* __restrict__ out_vals,
                                                       uint8_t* __restrict__ out_found) {
+#if FM_GET_WCOPY
+    if constexpr (VB % 16 == 0) {
+        // a thread probes its query; then the warp moves its 32 values
+        // together, VB / 16 lanes per value, so each load and store
+        // instruction covers whole 128-byte lines of several values
+        constexpr uint32_t LPV = VB / 16, VPR = 32 / LPV;
+        const uint32_t lane = threadIdx.x & 31u, part = lane % LPV, vsel = lane / LPV;
+        const uint64_t G = (uint64_t)gridDim.x * blockDim.x;
+        for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += G) {
+            const uint64_t q = base + lane;
+            uint64_t hit = NONE64;
+            if (q < n) hit = get_probe_thread<KB>(t, qkeys + q * KB);
+            if (out_found && q < n) out_found[q] = hit != NONE64 ? 1 : 0;
+            if (!out_vals) continue;
+#pragma unroll
+            for (uint32_t r = 0; r < LPV; r++) {
+                const uint32_t src = r * VPR + vsel;
+                const uint64_t hs = __shfl_sync(0xFFFFFFFFu, hit, src);
+                const uint64_t qs = base + src;
+                if (qs < n) {
+                    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                    if (hs != NONE64) v = __ldg(reinterpret_cast<const uint4*>(t.vals + hs * VB) + part);
+                    reinterpret_cast<uint4*>(out_vals + qs * VB)[part] = v;
+                }
+            }
+        }
+        return;
+    }
+#endif
     for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (uint64_t)gridDim.x * blockDim.x)
         get_query_thread<KB, VB>(t, qkeys + q * KB, out_vals ? out_vals + q * VB : nullptr,
                                  out_found ? out_found + q : nullptr);

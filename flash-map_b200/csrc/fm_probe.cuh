@@ -13,6 +13,14 @@ __device__ __forceinline__ uint64_t home_of(const TableView& t, const uint8_t* k
     return key.hash(ksz, t.hash_mode) & t.mask;
 }
 
+#ifndef FM_GET_WCOPY
+#define FM_GET_WCOPY 1  // k_get_thread moves values a warp at a time
+#endif
+
+// The probe of one lookup on one thread: the slot holding the key, or NONE64.
+template <int KB>
+__device__ __forceinline__ uint64_t get_probe_thread(const TableView& t, const uint8_t* __restrict__ qk);
+
 // bulk_get with one thread per query (compile-time shapes, capacity >= 8).
 // Each step reads the 8-slot metadata window that holds the probe position as
 // two 16-byte loads (one 32-byte sector, aligned), walks it in registers, and
@@ -23,6 +31,18 @@ __device__ __forceinline__ uint64_t home_of(const TableView& t, const uint8_t* k
 template <int KB, int VB>
 __device__ __forceinline__ void get_query_thread(const TableView& t, const uint8_t* __restrict__ qk,
                                                  uint8_t* __restrict__ ov, uint8_t* __restrict__ of) {
+    const uint64_t hit = get_probe_thread<KB>(t, qk);
+    if (ov) {
+        RegVal<VB> v;
+        if (hit != NONE64) v.load_ro(t.vals + hit * VB);
+        else v.zero();
+        v.store(ov, VB);
+    }
+    if (of) *of = hit != NONE64 ? 1 : 0;
+}
+
+template <int KB>
+__device__ __forceinline__ uint64_t get_probe_thread(const TableView& t, const uint8_t* __restrict__ qk) {
     const uint64_t mask = t.mask;
     RegKey<KB> key;
     key.load(qk, KB);
@@ -62,13 +82,7 @@ __device__ __forceinline__ void get_query_thread(const TableView& t, const uint8
         }
         wb += 8;
     }
-    if (ov) {
-        RegVal<VB> v;
-        if (hit != NONE64) v.load_ro(t.vals + hit * VB);
-        else v.zero();
-        v.store(ov, VB);
-    }
-    if (of) *of = hit != NONE64 ? 1 : 0;
+    return hit;
 }
 
 // Q lookups per thread probed in lockstep (compile-time shapes, capacity >=
