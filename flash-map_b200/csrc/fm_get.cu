@@ -145,7 +145,11 @@ __global__ void __launch_bounds__(BLOCK) k_get_thread(TableView t, const uint8_t
                                                       uint8_t* __restrict__ out_vals,
                                                       uint8_t* __restrict__ out_found) {
 #if FM_GET_WCOPY
-    if constexpr (VB % 16 == 0) {
+    constexpr bool wcopy = VB % 16 == 0;
+#else
+    constexpr bool wcopy = false;
+#endif
+    if constexpr (wcopy) {
         // a thread probes its query; then the warp moves its 32 values
         // together, VB / 16 lanes per value, so each load and store
         // instruction covers whole 128-byte lines of several values
@@ -170,12 +174,12 @@ __global__ void __launch_bounds__(BLOCK) k_get_thread(TableView t, const uint8_t
                 }
             }
         }
-        return;
+    } else {
+        for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+             q += (uint64_t)gridDim.x * blockDim.x)
+            get_query_thread<KB, VB>(t, qkeys + q * KB, out_vals ? out_vals + q * VB : nullptr,
+                                     out_found ? out_found + q : nullptr);
     }
-#endif
-    for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (uint64_t)gridDim.x * blockDim.x)
-        get_query_thread<KB, VB>(t, qkeys + q * KB, out_vals ? out_vals + q * VB : nullptr,
-                                 out_found ? out_found + q : nullptr);
 }
 
 // Q queries per thread probed in lockstep (get_queries_lockstep): thread g
