@@ -1261,10 +1261,10 @@ struct fm_batch {
     uint8_t* h_io = nullptr;               // pinned: len[tables], res[ops], status[ops]
     uint32_t* d_pend = nullptr;            // pending counts (eager runs): GROUP_MAX + 1 words
     uint32_t* h_pend = nullptr;
-    // Queue mode (every op of a compile-time record shape): the ops run as
-    // chains of phases drained by one persistent launch per record shape and
-    // segment; an insert that can take its table to FM_DIRECT_LOAD closes the
-    // segment and runs on the component path between launches.
+    // Queue mode (every op of a compile-time record shape): every op as
+    // device-driven kernels on stream lanes (qlanes), or the ops as chains of
+    // phases drained by one persistent launch per record shape and segment,
+    // the large ops as device-driven steps between the launches.
     bool qmode = false;
     bool qlanes = false;  // queue mode: every op a device-driven step on a stream lane
     std::vector<cudaEvent_t> step_ev;  // qlanes: recorded after each step another lane waits for

@@ -5,10 +5,14 @@ A :class:`FlashMapBatch` holds a queue of device-resident bulk operations
 GPU).  Running it gives the result of calling ``bulk_get_device`` /
 ``bulk_insert_device`` / ``bulk_remove_device`` one by one in queue order --
 including each insert's ``TableFull`` precheck against the table's count at
-that point -- but the library plans the queue into waves of independent ops
-and serves every wave with grouped kernels, with no host round trip between
-waves.  :meth:`FlashMapBatch.capture` records the whole submission into a
-CUDA graph that later :meth:`run` calls replay.
+that point -- but the library runs every op as device-driven kernels on
+stream lanes (a table's writes in order, its lookups between them at the same
+time, different tables at once), with no host round trip between ops
+(``FLASHMAP_BATCH_MODE=queue``: one persistent kernel per record shape
+instead; batches with run-time record sizes: waves of grouped kernels).
+:meth:`FlashMapBatch.capture` records the whole submission into a CUDA graph
+that later :meth:`run` calls replay.  No op may read or write a buffer that
+another op of the batch writes.
 
 No counterpart in the reference (bajpainaman/flash-map 0.5.0); it is the
 batching form built around the same bulk semantics (src/lib.rs:123-162).

@@ -183,23 +183,30 @@ const char* fm_kernel_class_name(uint32_t cls);
  * device-resident keys, values and outputs, executed with the result of
  * calling fm_bulk_get_device / fm_bulk_insert_device / fm_bulk_remove_device
  * one by one in queue order (each insert's TableFull precheck sees the
- * table's count after the ops before it).  The ops are planned into waves of
- * independent ops (distinct tables; consecutive gets of one table share a
- * wave); each wave runs grouped kernels that serve all its ops of one kind
- * and record shape per launch.  Tables are spread over up to 8 stream lanes
- * forked from the caller's stream and joined back before the results are
- * copied out, so the waves of different tables overlap; a table's ops stay in
- * order on its lane.  Without a graph, fm_batch_run drives each
- * wave's insert/remove rounds from the host (a 4-byte readback per two
- * rounds, as the plain calls do) and records how many rounds each wave
- * needed.  fm_batch_capture records the whole batch into a CUDA graph with
- * those round counts (3 per wave before any eager run) and no host
- * synchronisation; later fm_batch_run calls replay it.  A replay whose data
- * needs more rounds than recorded still gives the same results, more slowly
- * (the remaining ops finish in a single block per op) -- run the batch
+ * table's count after the ops before it).  Batches whose tables all have
+ * compile-time record sizes and whose buffers are 16-byte aligned run every
+ * op as device-driven kernels (counts read from the device, no host step
+ * between ops) on 8 stream lanes forked from the caller's stream and joined
+ * back before the results are copied out: a table's inserts and removes in
+ * order on its lane, its lookups between two writes at once (on other lanes
+ * when the batch has fewer tables than lanes), each lane waiting for the
+ * steps of other lanes it depends on through events.  With the environment
+ * variable FLASHMAP_BATCH_MODE=queue set when the batch is created, they run
+ * instead through one persistent kernel per record shape that drains the
+ * ops' phases (large ops run as the same device-driven kernels between its
+ * launches).  Other batches run as waves of independent ops with grouped
+ * kernels, on the same lanes.  Without a graph, fm_batch_run drives any
+ * rounds (a remove's fallback, a wave's inserts and removes) from the host
+ * (a small readback per two rounds, as the plain calls do) and records how
+ * many each needed; fm_batch_capture records the whole batch into a CUDA
+ * graph with those round counts and no host synchronisation; later
+ * fm_batch_run calls replay it.  A replay whose data needs more rounds than
+ * recorded still gives the same results, more slowly -- run the batch
  * eagerly once on representative data before capturing.  Between
  * fm_batch_run and fm_batch_wait the batch's tables must not be used by other
- * calls.  Per-op results (new /
+ * calls, and no op of the batch may read or write a buffer that another op
+ * of it writes (lookups of one table may run at the same time).  Per-op
+ * results (new /
  * removed key counts) and status codes (FM_OK, FM_ERR_TABLE_FULL,
  * FM_ERR_PROBE_LIMIT, ...) are written back into the op array by
  * fm_batch_wait, which also updates each table's len. */
