@@ -351,7 +351,10 @@ __device__ __forceinline__ uint32_t rx_chunk32(const TableView& t, const uint8_t
 // Ops of a group of removes (equal first EMPTY slot) a warp runs itself; up
 // to RX_THREAD of them one thread runs.
 constexpr uint32_t RX_GMAX = 256;
-constexpr uint32_t RX_THREAD = 8;
+#ifndef FM_RX_THREAD
+#define FM_RX_THREAD 8
+#endif
+constexpr uint32_t RX_THREAD = FM_RX_THREAD;
 constexpr uint32_t RX_BMAX = 8192;  // ops of a group one block sorts in shared memory
 
 template <int KB>
