@@ -352,7 +352,7 @@ __device__ __forceinline__ uint32_t rx_chunk32(const TableView& t, const uint8_t
 // to RX_THREAD of them one thread runs.
 constexpr uint32_t RX_GMAX = 256;
 #ifndef FM_RX_THREAD
-#define FM_RX_THREAD 8
+#define FM_RX_THREAD 16
 #endif
 constexpr uint32_t RX_THREAD = FM_RX_THREAD;
 constexpr uint32_t RX_BMAX = 8192;  // ops of a group one block sorts in shared memory
