@@ -324,7 +324,7 @@ REMOVE_KERNELS = ("k_rem_p1", "k_rem_p2", "k_rem_p3", "k_rem_tail", "rem_group")
 # the same load factor and call size (the traffic summary under
 # profiles/ gives the command and the per-kernel figures); traffic grows with
 # the ops processed.
-NCU_TRAFFIC_PER_OP = {"insert": 2446.0, "get": 334.7, "remove": 516.1}
+NCU_TRAFFIC_PER_OP = {"insert": 2446.0, "get": 334.7, "remove": 515.2}
 
 
 class DeviceRun:
